@@ -1,0 +1,211 @@
+"""TEST INFRASTRUCTURE ONLY -- the CPU FP64 oracle for the DGSEM tendency + LSRK(5,4) path.
+
+This package wraps ``oracle/oracle.cpp`` (a C++ restatement of Raven.jl's brick grid,
+DGSEM tendency and LSRK(5,4) stepper, citations in that file).  Only ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` may import it; the
+product package (``raven.jl_b200``) never does.
+
+The oracle is pinned against the reference's own golden values
+(``tests/golden/reference_goldens.json``, produced by ``tests/golden/make_goldens.py``).
+"""
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+
+LAW_ADVECTION, LAW_EULER = 0, 1
+FORM_WEAK, FORM_FLUXDIFF = 0, 1
+FLUX_CENTRAL, FLUX_KG, FLUX_EC, FLUX_RUSANOV = 0, 1, 2, 3
+WARP_NONE, WARP_SINE, WARP_IDENTITY_CURVED = 0, 1, 2
+
+
+def build(force=False):
+    """Compile oracle.cpp into oracle/_build/liboracle.so (g++, -ffp-contract=off, OpenMP)."""
+    src = os.path.join(HERE, "oracle.cpp")
+    hdr = os.path.join(HERE, "oracle.h")
+    os.makedirs(os.path.dirname(LIB_PATH), exist_ok=True)
+    if (
+        not force
+        and os.path.exists(LIB_PATH)
+        and os.path.getmtime(LIB_PATH) >= max(os.path.getmtime(src), os.path.getmtime(hdr))
+    ):
+        return LIB_PATH
+    cmd = [
+        "g++", "-O2", "-std=gnu++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
+        "-fno-fast-math", "-o", LIB_PATH, src, "-lquadmath",
+    ]
+    subprocess.check_call(cmd)
+    return LIB_PATH
+
+
+class _Law(ctypes.Structure):
+    _fields_ = [
+        ("law", ctypes.c_int),
+        ("form", ctypes.c_int),
+        ("volume_flux", ctypes.c_int),
+        ("surface_flux", ctypes.c_int),
+        ("gamma", ctypes.c_double),
+        ("adv", ctypes.c_double * 3),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.c_void_p
+        L.og_grid_create.restype = P
+        L.og_grid_create.argtypes = [ctypes.c_int, ctypes.c_int, P, P, P, P, ctypes.c_int, ctypes.c_double]
+        L.og_grid_destroy.argtypes = [P]
+        for name in ("og_grid_sizes", "og_grid_points", "og_grid_vmet", "og_grid_smet", "og_grid_vmapM",
+                     "og_grid_vmapP", "og_grid_boundary", "og_grid_tree_coords"):
+            getattr(L, name).argtypes = [P, P]
+        L.og_grid_lgl.argtypes = [P, P, P, P]
+        L.og_lgl.argtypes = [ctypes.c_int, P, P, P]
+        L.og_initial_condition.argtypes = [P, P, ctypes.c_int, P, ctypes.c_double, P]
+        L.og_tendency.argtypes = [P, P, P, P, ctypes.c_double, ctypes.c_int, ctypes.c_int64, ctypes.c_int64]
+        L.og_lsrk54_step.argtypes = [P, P, P, P, ctypes.c_double, ctypes.c_double]
+        L.og_solve.restype = ctypes.c_int64
+        L.og_solve.argtypes = [P, P, P, ctypes.c_double, ctypes.c_double]
+        L.og_weightednorm.restype = ctypes.c_double
+        L.og_weightednorm.argtypes = [P, P, ctypes.c_int, P]
+        L.og_integrals.argtypes = [P, P, ctypes.c_int, P]
+        L.og_num_threads.restype = ctypes.c_int
+        L.og_set_num_threads.argtypes = [ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def lgl(nq):
+    r = np.zeros(nq)
+    w = np.zeros(nq)
+    D = np.zeros((nq, nq), order="F")
+    lib().og_lgl(nq, _ptr(r), _ptr(w), _ptr(D))
+    return r, w, D
+
+
+class Law:
+    """Law/scheme selection for the oracle (mirrors Raven's DGSEM keyword arguments)."""
+
+    def __init__(self, law, dim, form=FORM_WEAK, volume_flux=FLUX_CENTRAL, surface_flux=FLUX_RUSANOV,
+                 gamma=1.4, adv=None):
+        self.dim = dim
+        self.c = _Law()
+        self.c.law = law
+        self.c.form = form
+        self.c.volume_flux = volume_flux
+        self.c.surface_flux = surface_flux
+        self.c.gamma = gamma
+        a = adv if adv is not None else [1.0] * dim
+        for i in range(3):
+            self.c.adv[i] = a[i] if i < len(a) else 0.0
+        self.ns = 1 if law == LAW_ADVECTION else dim + 2
+
+
+class Grid:
+    """A brick grid built by the oracle (element order, points, metrics, face maps)."""
+
+    def __init__(self, dim, nq, K, lo, hi, periodic, warp=WARP_NONE, warp_amp=0.0):
+        K3 = np.array(list(K) + [1] * (3 - len(K)), dtype=np.int32)
+        lo3 = np.array(list(lo) + [0.0] * (3 - len(lo)), dtype=np.float64)
+        hi3 = np.array(list(hi) + [1.0] * (3 - len(hi)), dtype=np.float64)
+        p3 = np.array([int(bool(p)) for p in periodic] + [0] * (3 - len(periodic)), dtype=np.int32)
+        self._keep = (K3, lo3, hi3, p3)
+        self.h = lib().og_grid_create(dim, nq, _ptr(K3), _ptr(lo3), _ptr(hi3), _ptr(p3), warp, warp_amp)
+        s = np.zeros(8, dtype=np.int64)
+        lib().og_grid_sizes(self.h, _ptr(s))
+        self.dim, self.nq, self.np, self.nfp, self.nfaces, self.E, self.nvmet, self.nsmet = (int(v) for v in s)
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.og_grid_destroy(self.h)
+            self.h = None
+
+    def _get(self, name, shape, dtype):
+        a = np.zeros(shape, dtype=dtype, order="F")
+        getattr(lib(), name)(self.h, _ptr(a))
+        return a
+
+    def lgl(self):
+        r = np.zeros(self.nq)
+        w = np.zeros(self.nq)
+        D = np.zeros((self.nq, self.nq), order="F")
+        lib().og_grid_lgl(self.h, _ptr(r), _ptr(w), _ptr(D))
+        return r, w, D
+
+    def points(self):
+        return self._get("og_grid_points", (self.np, self.dim, self.E), np.float64)
+
+    def volume_metrics(self):
+        return self._get("og_grid_vmet", (self.np, self.nvmet, self.E), np.float64)
+
+    def surface_metrics(self):
+        return self._get("og_grid_smet", (self.nsmet, self.nfaces * self.nfp, self.E), np.float64)
+
+    def vmapM(self):
+        return self._get("og_grid_vmapM", (self.nfaces * self.nfp, self.E), np.int64)
+
+    def vmapP(self):
+        return self._get("og_grid_vmapP", (self.nfaces * self.nfp, self.E), np.int64)
+
+    def boundary(self):
+        return self._get("og_grid_boundary", (self.nfaces, self.E), np.int64)
+
+    def tree_coords(self):
+        return self._get("og_grid_tree_coords", (3, self.E), np.int32)
+
+    # ---- state ----
+    def state(self, law):
+        return np.zeros((self.np, law.ns, self.E), order="F")
+
+    def initial_condition(self, law, kind, params=(), t=0.0):
+        q = self.state(law)
+        prm = np.array(list(params) + [0.0] * 8, dtype=np.float64)
+        lib().og_initial_condition(self.h, ctypes.byref(law.c), kind, _ptr(prm), t, _ptr(q))
+        return q
+
+    def tendency(self, law, q, dq=None, t=0.0, increment=False, e0=0, e1=None):
+        q = np.asfortranarray(q, dtype=np.float64)
+        if dq is None:
+            dq = self.state(law)
+        lib().og_tendency(self.h, ctypes.byref(law.c), _ptr(dq), _ptr(q), t, int(increment), e0,
+                          self.E if e1 is None else e1)
+        return dq
+
+    def lsrk54_step(self, law, q, dq, time, dt):
+        lib().og_lsrk54_step(self.h, ctypes.byref(law.c), _ptr(q), _ptr(dq), time, dt)
+
+    def solve(self, law, q, dt, timeend):
+        return lib().og_solve(self.h, ctypes.byref(law.c), _ptr(q), dt, timeend)
+
+    def weightednorm(self, q, ns):
+        comp = np.zeros(ns)
+        v = lib().og_weightednorm(self.h, _ptr(np.asfortranarray(q)), ns, _ptr(comp))
+        return v, comp
+
+    def integrals(self, q, ns):
+        out = np.zeros(ns)
+        lib().og_integrals(self.h, _ptr(np.asfortranarray(q)), ns, _ptr(out))
+        return out
+
+
+def num_threads():
+    return lib().og_num_threads()
+
+
+def set_num_threads(n):
+    lib().og_set_num_threads(int(n))
