@@ -1,0 +1,443 @@
+#!/usr/bin/env python
+"""DOF-updates/s of the fused DGSEM tendency + LSRK(5,4) path on B200.
+
+Workload (default): 3-D compressible Euler, periodic 32^3 brick of hex elements on
+[0,10]^3, N = 7 (512 nodes/element, 16.8 M nodes, 83.9 M DOF), Kennedy-Gruber
+flux-differencing volume term, Rusanov surface flux, isentropic vortex (strength 5,
+background Mach 0.5, z-invariant), LSRK(5,4) at CFL 0.4, FP64.  One bench step is one
+LSRK(5,4) time step (5 fused stage kernels).  The 1.3 GB state is larger than L2
+(126 MB), so no L2 flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+
+Multi-GPU (torchrun): every rank runs an independent replica of the workload (the
+single-grid path has no cross-rank exchange on one rank); time is the max over ranks.
+"""
+
+import argparse
+import importlib.util
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: dim, N, elements per side, domain side, law, volume flux, precision, warp
+    "euler3d_kg_n7_32_fp64": dict(dim=3, N=7, K=32, L=10.0, law="euler", vflux="kg", precision="fp64", warp=False),
+    "euler3d_kg_n7_32_fp32bulk_warped": dict(dim=3, N=7, K=32, L=10.0, law="euler", vflux="kg",
+                                             precision="fp32_bulk", warp=True),
+    "euler3d_kg_n7_32_fp64_warped": dict(dim=3, N=7, K=32, L=10.0, law="euler", vflux="kg", precision="fp64",
+                                         warp=True),
+    "adv2d_weak_n4_16_fp64": dict(dim=2, N=4, K=16, L=1.0, law="advection", vflux="weak", precision="fp64",
+                                  warp=False),
+}
+DEFAULT = "euler3d_kg_n7_32_fp64"
+METRIC = "DOF-updates/s per RHS"
+UNIT = "DOF-updates/s"
+
+
+def load_product():
+    if "raven_b200" in sys.modules:
+        return sys.modules["raven_b200"]
+    pkg = os.path.join(ROOT, "raven.jl_b200")
+    spec = importlib.util.spec_from_file_location("raven_b200", os.path.join(pkg, "__init__.py"),
+                                                  submodule_search_locations=[pkg])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["raven_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def config_json(name, w):
+    return {
+        "workload": name,
+        "equation": "euler" if w["law"] == "euler" else "advection",
+        "dim": w["dim"],
+        "polynomial_order": w["N"],
+        "elements": w["K"] ** w["dim"],
+        "nodes": w["K"] ** w["dim"] * (w["N"] + 1) ** w["dim"],
+        "volume_form": "flux_differencing_kennedy_gruber" if w["vflux"] == "kg" else "weak",
+        "surface_flux": "rusanov",
+        "precision": w["precision"],
+        "geometry": "warped" if w["warp"] else "brick",
+        "time_stepper": "LSRK54",
+        "initial_data": "isentropic_vortex" if w["law"] == "euler" else "sine_plus_gaussian",
+        "l2_flush": "not needed: state larger than L2" if w["K"] >= 32 else "state is L2-resident",
+        "parallelism": "replicas",
+    }
+
+
+def sine_warp(L, dim):
+    import numpy as np
+
+    def warp(*x):
+        s = 1.0
+        for d in range(dim):
+            s = s * np.sin(np.pi * (x[d] / L))
+        return [x[d] + (0.1 * L) * s for d in range(dim)]
+
+    return warp
+
+
+def setup(rb, w, device):
+    import numpy as np
+
+    from raven_b200 import initial_conditions as ic
+
+    dim, N, K, L = w["dim"], w["N"], w["K"], w["L"]
+    cell = rb.LobattoCell(*([N + 1] * dim))
+    cg = rb.brick(tuple(rb.jl_range(0.0, L, K + 1) for _ in range(dim)), (True,) * dim)
+    gm = rb.GridManager(cell, cg)
+    grid = rb.generate(sine_warp(L, dim), gm) if w["warp"] else rb.generate(gm)
+    if w["law"] == "euler":
+        law = rb.EulerLaw(dim)
+        u0 = 0.5 * math.sqrt(law.gamma)
+        q0 = ic.isentropic_vortex(grid, law, beta=5.0, u0=u0, center=(L / 2, L / 2))
+        form = rb.FluxDifferencingForm(rb.KennedyGruberFlux())
+        dt = 0.4 * (L / K) / N / ic.max_wavespeed(grid, law, q0)
+    else:
+        law = rb.AdvectionLaw(dim, (1.0, 0.5))
+        q0 = ic.sine_plus_gaussian(grid, law, sigma=0.05)
+        form = rb.WeakForm()
+        dt = 0.5 * (L / K) / N / math.hypot(*law.u)
+    dg = rb.DGSEM(law=law, grid=grid, volume_form=form, surface_numericalflux=rb.RusanovFlux(),
+                  precision=w["precision"], device=device)
+    return grid, law, dg, q0, dt
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(name):
+    """dram bytes per launch of the stage kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"stage_kernel_{name}.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def stage_bytes_per_launch(w, nodes, ns):
+    """Algorithmic HBM bytes of one stage launch, averaged over the 5 stages of a step:
+    q read + q write (FP64) + dq write every stage + dq read in stages 2-5 (stage 1 has
+    rka = 0), plus the per-node metrics of a curved grid (wJ*dRdX rows + MJI, and n,
+    wsJ on 0.75 face slots per node at N = 7)."""
+    dqb = 4 if w["precision"] == "fp32_bulk" else 8
+    per_step = nodes * ns * (5 * 16 + 5 * dqb + 4 * dqb)
+    if w["warp"]:
+        dim, nq = w["dim"], w["N"] + 1
+        per_node_geo = (dim * dim + 1) * 8 + (2 * dim * nq ** (dim - 1)) * (dim + 1) * 8 / nq**dim
+        per_step += 5 * nodes * per_node_geo
+    return per_step / 5.0
+
+
+def cpu_sample(w, max_seconds=20.0):
+    """The oracle (C++ FP64 restatement) on the host cores: LSRK(5,4) steps of the same
+    element type, law and flux on a small brick, repeated for up to ~max_seconds."""
+    import oracle as O
+
+    dim, N = w["dim"], w["N"]
+    K = 8 if dim == 3 else 16
+    warp = O.WARP_SINE if w["warp"] else O.WARP_NONE
+    og = O.Grid(dim, N + 1, [K] * dim, [0.0] * dim, [w["L"]] * dim, [True] * dim, warp, 0.1)
+    if w["law"] == "euler":
+        law = O.Law(O.LAW_EULER, dim, form=O.FORM_FLUXDIFF, volume_flux=O.FLUX_KG)
+        q = og.initial_condition(law, 4, [5.0, 0.5 * math.sqrt(1.4), w["L"] / 2, w["L"] / 2])
+    else:
+        law = O.Law(O.LAW_ADVECTION, dim, adv=[1.0, 0.5])
+        q = og.initial_condition(law, 3, [0.05, 0.5, 0.5, 0.5])
+    dq = og.state(law)
+    dt = 1e-4
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        og.lsrk54_step(law, q, dq, steps * dt, dt)
+        steps += 1
+        if time.perf_counter() - t0 >= max_seconds or steps >= 1000:
+            break
+    el = time.perf_counter() - t0
+    nodes = og.np * og.E
+    return {
+        "value": nodes * law.ns * 5 * steps / el,
+        "unit": UNIT,
+        "cores": O.num_threads(),
+        "kind": "port",
+        "sample": f"{steps} LSRK(5,4) steps of the same scheme (dim {dim}, N {N}, {w['vflux']}, "
+                  f"{'warped' if w['warp'] else 'brick'}) on a {K}^{dim}-element periodic brick, FP64, "
+                  f"OpenMP over elements, {el:.1f} s",
+    }
+
+
+def run_reference(args, w):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import oracle as O
+
+    O.build()
+    dim, N = w["dim"], w["N"]
+    # per-step sample size: keep (warmup + steps) * step time within ~2 minutes
+    K = {3: 4, 2: 8}[dim]
+    warp = O.WARP_SINE if w["warp"] else O.WARP_NONE
+    og = O.Grid(dim, N + 1, [K] * dim, [0.0] * dim, [w["L"]] * dim, [True] * dim, warp, 0.1)
+    if w["law"] == "euler":
+        law = O.Law(O.LAW_EULER, dim, form=O.FORM_FLUXDIFF, volume_flux=O.FLUX_KG)
+        q = og.initial_condition(law, 4, [5.0, 0.5 * math.sqrt(1.4), w["L"] / 2, w["L"] / 2])
+    else:
+        law = O.Law(O.LAW_ADVECTION, dim, adv=[1.0, 0.5])
+        q = og.initial_condition(law, 3, [0.05, 0.5, 0.5, 0.5])
+    dq = og.state(law)
+    dt = 1e-4
+    for i in range(args.warmup):
+        og.lsrk54_step(law, q, dq, i * dt, dt)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        og.lsrk54_step(law, q, dq, i * dt, dt)
+    el = time.perf_counter() - t0
+    nodes = og.np * og.E
+    value = nodes * law.ns * 5 * args.steps / el
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": el / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": config_json(args.workload, w),
+        "cpu_baseline": {
+            "value": value,
+            "unit": UNIT,
+            "cores": O.num_threads(),
+            "kind": "port",
+            "sample": f"each step: one LSRK(5,4) step of the same scheme on a {K}^{dim}-element periodic brick "
+                      f"(N {N}), FP64 C++ restatement of Raven's CPU path, OpenMP over elements",
+        },
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main(argv=None):
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    args = p.parse_args(argv)
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference(args, w)
+
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    rb = load_product()
+    grid, law, dg, q0, dt = setup(rb, w, local)
+    nodes, ns = grid.np * grid.E, law.ns
+    q = rb.GridArray.from_numpy(q0)
+    dq = q.similar()
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+            torch.cuda.synchronize()
+
+    dg.lsrk54_steps(q, dq, 0.0, dt, args.warmup)
+    barrier()
+    sampler = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local)
+    sampler.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    dg.lsrk54_steps(q, dq, args.warmup * dt, dt, args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    sampler.stop()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * nodes * ns * 5 * args.steps / (ms / 1e3)
+    launches = 5 * args.steps
+
+    # accuracy of the run: L2 distance to the exactly advected vortex, and conservation
+    l2_err = None
+    if w["law"] == "euler":
+        from raven_b200 import initial_conditions as ic
+
+        T = (args.warmup + args.steps) * dt
+        qe = rb.GridArray.from_numpy(ic.isentropic_vortex(grid, law, beta=5.0, u0=0.5 * math.sqrt(law.gamma),
+                                                          center=(w["L"] / 2, w["L"] / 2), t=T))
+        qe.data.sub_(q.data)
+        l2_err = rb.weightednorm(dg, qe)
+        del qe
+
+    # end to end through the C ABI with host buffers: every step copies the state in from
+    # pinned host memory, runs one LSRK(5,4) step and copies the state back
+    qh_t = torch.empty((grid.E, ns, grid.np), dtype=torch.float64, pin_memory=True)
+    qh = qh_t.numpy().transpose(2, 1, 0)
+    qh[...] = q0
+    dg.lsrk54_steps_host(qh, 0.0, dt, 1)  # warm-up
+    barrier()
+    t0 = time.perf_counter()
+    for i in range(args.e2e_steps):
+        dg.lsrk54_steps_host(qh, i * dt, dt, 1)
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {
+        "value": world * nodes * ns * 5 * args.e2e_steps / e2e_s,
+        "unit": UNIT,
+        "h2d_bytes_per_step": nodes * ns * 8,
+        "d2h_bytes_per_step": nodes * ns * 8,
+    }
+
+    peak, peak_kind = measured_peaks()
+    bytes_launch = stage_bytes_per_launch(w, nodes, ns)
+    achieved = bytes_launch / (ms / 1e3 / launches) / 1e9
+    traffic = profiled_traffic(args.workload)
+    roofline = {
+        "bound": "hbm",
+        "achieved": achieved,
+        "peak": peak,
+        "unit": "GB/s",
+        "frac": achieved / peak,
+        "traffic": traffic,
+        "peak_source": peak_kind,
+        "kernel": "stage_kernel (fused volume + surface + LSRK stage)",
+        "algorithmic_bytes_per_launch": bytes_launch,
+    }
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_sample(w)
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32+f64" if w["precision"] == "fp32_bulk" else "f64",
+            "data": "synthetic",
+            "config": config_json(args.workload, w),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": sampler.summary(),
+            "l2_error_vs_exact": l2_err,
+            "dt": dt,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

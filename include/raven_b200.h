@@ -1,0 +1,132 @@
+/*
+ * raven_b200.h -- C ABI of the B200 (sm_100a) DGSEM tendency + LSRK(5,4) library.
+ *
+ * The library replaces, for one GPU and one rank, the device work behind Raven.jl's
+ *   (dg::DGSEM)(dq, q, time; increment)       src/balancelaws/dgsem.jl:84-126
+ *   dostep!(q, ::LSRK, after_stage)           src/balancelaws/odesolvers.jl:51-61
+ *   weightednorm(dg, q)                       src/balancelaws/measures.jl:6-21
+ * The grid data it consumes are exactly the arrays a Raven `Grid` holds
+ * (`volumemetrics`, `surfacemetrics`, `facemaps`, `boundarycodes`,
+ * `derivatives_1d`, `weights_1d`), in the GridArray parent layouts of
+ * src/gridarrays.jl:50-108.  State arrays are Raven's GridArray parent layout
+ * (Nq^dim, Ns, E), column-major, FP64, on the device.
+ *
+ * All functions return an rb200_status and never abort.  Device-pointer arguments
+ * are borrowed for the duration of the call; work is enqueued on the caller's stream
+ * (a cudaStream_t passed as void*; NULL = legacy default stream).  A handle is not
+ * thread-safe.
+ */
+#ifndef RAVEN_B200_H
+#define RAVEN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RB200_ABI_VERSION 1
+
+typedef enum rb200_status {
+    RB200_OK = 0,
+    RB200_ERR_BAD_ARG = 1,     /* null pointer, out-of-range enum or size */
+    RB200_ERR_SHAPE = 2,       /* array sizes inconsistent (DimensionMismatch in Raven) */
+    RB200_ERR_OOM = 3,         /* device allocation failed */
+    RB200_ERR_CUDA = 4,        /* a CUDA runtime call failed */
+    RB200_ERR_TIMEOUT = 5,     /* a bounded wait expired */
+    RB200_ERR_UNSUPPORTED = 6  /* valid input this build does not implement */
+} rb200_status;
+
+/* Balance laws: AdvectionLaw{FT,D}(u) (balancelaws/advection.jl:8-16),
+ * EulerLaw{FT,D}(; gamma) (balancelaws/euler.jl:9-19). */
+enum { RB200_LAW_ADVECTION = 0, RB200_LAW_EULER = 1 };
+/* Volume forms: WeakForm(), FluxDifferencingForm(flux) (dgsem.jl:5-17). */
+enum { RB200_FORM_WEAK = 0, RB200_FORM_FLUXDIFF = 1 };
+/* Numerical fluxes (numericalfluxes.jl:39-55, euler.jl:150-216). */
+enum {
+    RB200_FLUX_CENTRAL = 0,
+    RB200_FLUX_KENNEDY_GRUBER = 1,
+    RB200_FLUX_ENTROPY_CONSERVATIVE = 2,
+    RB200_FLUX_RUSANOV = 3
+};
+/* Arithmetic of the volume/surface bulk.  FP32_BULK keeps the state q, the
+ * geometry and all reductions in FP64 and the LSRK register dq in FP32. */
+enum { RB200_PRECISION_FP64 = 0, RB200_PRECISION_FP32_BULK = 1 };
+
+typedef struct rb200_desc {
+    int32_t abi_version;      /* RB200_ABI_VERSION */
+    int32_t dim;              /* 2 or 3 */
+    int32_t nq;               /* nodes per direction, 2..8 (N = nq-1) */
+    int32_t law;              /* RB200_LAW_* */
+    int64_t num_elements;     /* E (local elements; no ghosts on one rank) */
+    int32_t volume_form;      /* RB200_FORM_* */
+    int32_t volume_flux;      /* two-point flux of FluxDifferencingForm */
+    int32_t surface_flux;     /* RB200_FLUX_RUSANOV or RB200_FLUX_CENTRAL */
+    int32_t precision;        /* RB200_PRECISION_* */
+    double gamma;             /* Euler ratio of specific heats (Raven default 7//5) */
+    double advection_velocity[3];
+    /* Host arrays, read during rb200_create only: */
+    const double* D;               /* (nq, nq) col-major, derivatives_1d(cell)[1] (lobattocells.jl:263) */
+    const double* w;               /* (nq), weights_1d */
+    const double* volume_metrics;  /* (nq^dim, dim*dim+2, E): dRdX (col-major), J, wJ
+                                      = parent(first(volumemetrics(grid))) */
+    const double* surface_metrics; /* (dim+2, 2*dim*nq^(dim-1), E): n, sJ, wsJ
+                                      = parent(first(surfacemetrics(grid))) */
+    const int64_t* vmapM;          /* (2*dim*nq^(dim-1), E), 1-based (facemaps(grid).vmapM) */
+    const int64_t* vmapP;          /* same shape (facemaps(grid).vmapP) */
+    const int64_t* boundary_codes; /* (2*dim, E) boundarycodes(grid); NULL = all 0 */
+    int32_t device;                /* CUDA device ordinal */
+} rb200_desc;
+
+typedef struct rb200_handle rb200_handle;
+
+/* DGSEM(; law, grid, surface_numericalflux, volume_form)  (dgsem.jl:46-81).
+ * Uploads the grid once; compresses vmapM/vmapP into a per-face neighbour table
+ * after checking, node by node, that it reproduces them. */
+rb200_status rb200_create(const rb200_desc* desc, rb200_handle** out);
+rb200_status rb200_destroy(rb200_handle* h);
+
+/* (dg::DGSEM)(dq, q, time; increment)  (dgsem.jl:84-126).
+ * dq = (increment ? dq : 0) + RHS(q).  dq, q: device, (nq^dim, Ns, E) FP64. */
+rb200_status rb200_tendency(rb200_handle* h, double* dq, const double* q, double time, int32_t increment,
+                            void* stream);
+
+/* nsteps of dostep!(q, LSRK54(dg, q, dt))  (odesolvers.jl:51-66): for each of the 5
+ * stages  dq = rka*dq + RHS(q);  q = q + rkb*dt*dq,  fused into one kernel per stage.
+ * q, dq: device FP64 (dq is the LSRK register, ignored in FP32_BULK mode where the
+ * handle keeps an FP32 register).  `time` is the time at the start of the first step. */
+rb200_status rb200_lsrk54_step(rb200_handle* h, double* q, double* dq, double time, double dt, int32_t nsteps,
+                               void* stream);
+
+/* Same as rb200_lsrk54_step for a state held in HOST memory: copies q in, runs the
+ * steps, copies q back, synchronously.  The LSRK register lives on the device. */
+rb200_status rb200_lsrk54_step_host(rb200_handle* h, double* q_host, double time, double dt, int32_t nsteps,
+                                    void* stream);
+
+/* weightednorm(dg, q, 2; componentwise=true)  (measures.jl:6-21): out[s] =
+ * sqrt(sum(MJ .* q_s.^2)) for s < Ns, out[Ns] = 2-norm of those.  FP64, synchronous,
+ * deterministic (fixed reduction order).  out: host, Ns+1 doubles. */
+rb200_status rb200_weightednorm(rb200_handle* h, const double* q, double* out, void* stream);
+
+/* Conservation integrals out[s] = sum(MJ .* q_s)  (FP64, synchronous).  out: host, Ns. */
+rb200_status rb200_integrals(rb200_handle* h, const double* q, double* out, void* stream);
+
+/* Rebuilds vmapP (1-based, (2*dim*nq^(dim-1), E) int64) on the device from the
+ * neighbour table the kernels use, for bit-exact comparison with facemaps(grid).vmapP. */
+rb200_status rb200_face_vmapP(rb200_handle* h, int64_t* vmapP_out, void* stream);
+
+/* Handle properties: info[0]=dim, [1]=nq, [2]=Ns, [3]=E, [4]=geometry kind
+ * (0 affine brick, 1 curved), [5]=precision, [6]=kernel launches per LSRK step,
+ * [7]=algorithmic HBM bytes per node per stage. */
+rb200_status rb200_get_info(const rb200_handle* h, int64_t* info, int32_t n);
+
+/* Last error message of a handle (empty if none); static text for NULL. */
+const char* rb200_last_error(const rb200_handle* h);
+const char* rb200_status_string(rb200_status s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RAVEN_B200_H */

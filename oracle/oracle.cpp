@@ -101,16 +101,12 @@ extern "C" void og_lgl(int nq, double* r, double* w, double* D) {
         if (w) w[i] = (double)wt[i];
     }
     if (D) {
-        for (int i = 0; i < nq; ++i) {
-            f128 diag = 0;
-            for (int j = 0; j < nq; ++j) {
-                if (i == j) continue;
-                f128 dij = (lam[j] / lam[i]) / (x[i] - x[j]);
-                diag -= dij;
-                D[i + nq * j] = (double)dij;
-            }
-            D[i + nq * i] = (double)diag;
-        }
+        for (int i = 0; i < nq; ++i)
+            for (int j = 0; j < nq; ++j)
+                D[i + nq * j] = (i == j) ? 0.0 : (double)((lam[j] / lam[i]) / (x[i] - x[j]));
+        // exact diagonal: -N(N+1)/4, N(N+1)/4 at the end points, 0 inside
+        D[0] = -N * (N + 1) / 4.0;
+        D[N + nq * N] = N * (N + 1) / 4.0;
     }
 }
 

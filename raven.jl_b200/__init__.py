@@ -1,0 +1,397 @@
+"""raven.jl_b200 -- Raven.jl's DGSEM tendency + LSRK(5,4) path on one B200 (sm_100a).
+
+The names, argument meanings and error behaviour follow Raven.jl's balance-law API
+(src/balancelaws/{dgsem,odesolvers,measures}.jl, src/lobattocells.jl,
+src/coarsegrids.jl, src/gridmanager.jl) so that a Raven driver script maps line by
+line:
+
+    Raven.jl                                        raven_b200
+    cell = LobattoCell{FT,A}(Nq, Nq, Nq)            cell = LobattoCell(Nq, Nq, Nq)
+    cg = brick((vx, vy, vz), (true, true, true))    cg = brick((vx, vy, vz), (True, True, True))
+    grid = generate(GridManager(cell, cg))          grid = generate(GridManager(cell, cg))
+    dg = DGSEM(; law, grid, volume_form,            dg = DGSEM(law=law, grid=grid, volume_form=...,
+               surface_numericalflux)                          surface_numericalflux=RusanovFlux())
+    q = GridArray(undef, law, grid)                 q = GridArray.zeros(law, grid)
+    dg(dq, q, t; increment = true)                  dg(dq, q, t, increment=True)
+    solve!(q, timeend, LSRK54(dg, q, dt))           solve(q, timeend, LSRK54(dg, q, dt))
+    weightednorm(dg, q)                             weightednorm(dg, q)
+
+Every operation on a GridArray runs the CUDA kernels of libravenb200.so through its C
+ABI (include/raven_b200.h).  There is no CPU fallback: without a CUDA device or
+without the built library the calls raise.
+
+Layout: a GridArray's data is a torch CUDA tensor of shape (E, Ns, Np), row-major,
+which is byte for byte Raven's GridArray parent array (Np, Ns, E) in column-major
+order.
+"""
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import RB200Error
+from .grids import Grid, brick_tree_order, jl_range, lobatto_operators
+
+__all__ = [
+    "LobattoCell", "brick", "BrickGrid", "GridManager", "generate", "Grid", "AdvectionLaw", "EulerLaw",
+    "RusanovFlux", "CentralFlux", "KennedyGruberFlux", "EntropyConservativeFlux", "WeakForm",
+    "FluxDifferencingForm", "GridArray", "DGSEM", "LSRK54", "solve", "weightednorm", "integrals",
+    "jl_range", "RB200Error", "brick_tree_order",
+]
+
+# --------------------------------------------------------------------------- cells and grids
+
+
+class LobattoCell:
+    """LobattoCell{Float64}(Nq...) (src/lobattocells.jl:89-250); all directions equal."""
+
+    def __init__(self, *sizes):
+        if len(sizes) not in (2, 3) or len(set(sizes)) != 1:
+            raise ValueError("LobattoCell needs 2 or 3 equal sizes (cubic cells, dgsem.jl:92)")
+        self.dim = len(sizes)
+        self.nq = int(sizes[0])
+        if not 2 <= self.nq <= 8:
+            raise ValueError("Nq must be in 2..8")
+        self.r, self.w, self.D = lobatto_operators(self.nq)
+
+    def size(self):
+        return (self.nq,) * self.dim
+
+    def derivatives_1d(self):
+        return (self.D,) * self.dim
+
+    def weights_1d(self):
+        return (self.w,) * self.dim
+
+    def points_1d(self):
+        return (self.r,) * self.dim
+
+
+class BrickGrid:
+    def __init__(self, coordinates, periodic):
+        self.coordinates = tuple(np.asarray(c, dtype=np.float64) for c in coordinates)
+        self.periodic = tuple(bool(p) for p in periodic)
+
+
+def brick(coordinates, periodic=None):
+    """brick(coordinates, periodic) (src/coarsegrids.jl:306-405).  `coordinates` is a
+    tuple of vertex arrays (use jl_range for Julia's `range(a, stop=b, length=n)`) or a
+    tuple of element counts (vertices 0:n)."""
+    coords = []
+    for c in coordinates:
+        if np.isscalar(c):
+            coords.append(np.arange(int(c) + 1, dtype=np.float64))
+        else:
+            coords.append(np.asarray(c, dtype=np.float64))
+    if periodic is None:
+        periodic = (False,) * len(coords)
+    if len(periodic) != len(coords):
+        raise ValueError("periodic must have one flag per dimension")
+    return BrickGrid(coords, periodic)
+
+
+class GridManager:
+    def __init__(self, cell, coarsegrid, min_level=0):
+        if min_level != 0:
+            raise NotImplementedError("only level-0 bricks (one element per tree) are generated")
+        if len(coarsegrid.coordinates) != cell.dim:
+            raise ValueError("cell and coarse grid dimensions differ")
+        self.cell = cell
+        self.coarsegrid = coarsegrid
+
+
+def generate(arg, gm=None):
+    """generate(gm) or generate(warp, gm) (src/gridmanager.jl:1084-1208).  `warp` maps
+    the coordinate arrays (x, y[, z]) to new ones; a warped grid gets curved metrics."""
+    if gm is None:
+        gm, warp = arg, None
+    else:
+        warp = arg
+    return Grid(gm.cell, gm.coarsegrid, warp=warp)
+
+
+# ------------------------------------------------------------------------ laws and fluxes
+
+
+class AdvectionLaw:
+    """AdvectionLaw{Float64,D}(u) (balancelaws/advection.jl:8-16)."""
+
+    code = _lib.LAW_ADVECTION
+
+    def __init__(self, dim, u=None):
+        self.dim = dim
+        self.u = tuple(float(x) for x in (u if u is not None else (1.0,) * dim))
+        if len(self.u) != dim:
+            raise ValueError("advection velocity must have `dim` components")
+        self.ns = 1
+        self.gamma = 1.4
+
+
+class EulerLaw:
+    """EulerLaw{Float64,D}(; gamma = 7//5) (balancelaws/euler.jl:9-19)."""
+
+    code = _lib.LAW_EULER
+
+    def __init__(self, dim, gamma=1.4):
+        self.dim = dim
+        self.gamma = float(gamma)
+        self.u = (0.0,) * dim
+        self.ns = dim + 2
+
+    def pressure(self, rho, rhou, rhoe):
+        return (self.gamma - 1) * (rhoe - sum(m * m for m in rhou) / (2 * rho))
+
+    def energy(self, rho, rhou, p):
+        return p / (self.gamma - 1) + sum(m * m for m in rhou) / (2 * rho)
+
+    def soundspeed(self, rho, p):
+        return np.sqrt(self.gamma * p / rho)
+
+
+class RusanovFlux:
+    code = _lib.FLUX_RUSANOV
+
+
+class CentralFlux:
+    code = _lib.FLUX_CENTRAL
+
+
+class KennedyGruberFlux:
+    code = _lib.FLUX_KENNEDY_GRUBER
+
+
+class EntropyConservativeFlux:
+    code = _lib.FLUX_ENTROPY_CONSERVATIVE
+
+
+class WeakForm:
+    code = _lib.FORM_WEAK
+    volume_numericalflux = CentralFlux()
+
+
+class FluxDifferencingForm:
+    code = _lib.FORM_FLUXDIFF
+
+    def __init__(self, volume_numericalflux, kernel_type="per_dir"):
+        self.volume_numericalflux = volume_numericalflux
+        self.kernel_type = kernel_type
+
+
+# ------------------------------------------------------------------------------ GridArray
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+class GridArray:
+    """State array in Raven's GridArray parent layout, resident on a CUDA device."""
+
+    def __init__(self, data, ns, np_, E):
+        self.data = data
+        self.ns, self.np, self.E = ns, np_, E
+
+    @classmethod
+    def zeros(cls, law, grid, device="cuda", dtype=None):
+        torch = _torch()
+        t = torch.zeros((grid.E, law.ns, grid.np), dtype=dtype or torch.float64, device=device)
+        return cls(t, law.ns, grid.np, grid.E)
+
+    @classmethod
+    def from_numpy(cls, arr, device="cuda"):
+        """arr: (Np, Ns, E) column-major (Raven parent layout)."""
+        torch = _torch()
+        a = np.asarray(arr, dtype=np.float64)
+        np_, ns, E = a.shape
+        t = torch.from_numpy(np.ascontiguousarray(a.transpose(2, 1, 0))).to(device)
+        return cls(t, ns, np_, E)
+
+    def numpy(self):
+        """(Np, Ns, E) column-major copy on the host."""
+        return np.asfortranarray(self.data.detach().cpu().numpy().transpose(2, 1, 0))
+
+    def similar(self):
+        return GridArray(_torch().zeros_like(self.data), self.ns, self.np, self.E)
+
+    def copy(self):
+        return GridArray(self.data.clone(), self.ns, self.np, self.E)
+
+    def ptr(self):
+        if not self.data.is_cuda or not self.data.is_contiguous() or self.data.dtype != _torch().float64:
+            raise ValueError("GridArray data must be a contiguous float64 CUDA tensor")
+        return ctypes.c_void_p(self.data.data_ptr())
+
+
+def _stream_ptr():
+    torch = _torch()
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+# ----------------------------------------------------------------------------------- DGSEM
+
+
+class DGSEM:
+    """DGSEM(; law, grid, surface_numericalflux, volume_form) (src/balancelaws/dgsem.jl:46-81).
+
+    precision: "fp64" (plain FP64) or "fp32_bulk" (FP32 volume/surface arithmetic, FP64
+    geometry, state accumulation and reductions)."""
+
+    def __init__(self, *, law, grid, surface_numericalflux, volume_form=None, precision="fp64", device=None):
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise RuntimeError("raven_b200.DGSEM needs a CUDA device (no CPU fallback)")
+        volume_form = volume_form or WeakForm()
+        if law.dim != grid.dim:
+            raise ValueError("law and grid dimensions differ")
+        if precision not in ("fp64", "fp32_bulk"):
+            raise ValueError("precision must be 'fp64' or 'fp32_bulk'")
+        self.law, self.grid, self.volume_form = law, grid, volume_form
+        self.surface_numericalflux = surface_numericalflux
+        self.precision = precision
+        self.device = torch.cuda.current_device() if device is None else int(device)
+        L = _lib.lib()
+        d = _lib.Desc()
+        d.abi_version = _lib.RB200_ABI_VERSION
+        d.dim, d.nq, d.law = grid.dim, grid.nq, law.code
+        d.num_elements = grid.E
+        d.volume_form = volume_form.code
+        d.volume_flux = getattr(volume_form, "volume_numericalflux", CentralFlux()).code
+        d.surface_flux = surface_numericalflux.code
+        d.precision = _lib.PRECISION_FP64 if precision == "fp64" else _lib.PRECISION_FP32_BULK
+        d.gamma = law.gamma
+        for i in range(3):
+            d.advection_velocity[i] = law.u[i] if i < len(law.u) else 0.0
+        keep = [
+            np.asfortranarray(grid.cell.D, dtype=np.float64),
+            np.ascontiguousarray(grid.cell.w, dtype=np.float64),
+            np.asfortranarray(grid.volume_metrics, dtype=np.float64),
+            np.asfortranarray(grid.surface_metrics, dtype=np.float64),
+            np.asfortranarray(grid.vmapM, dtype=np.int64),
+            np.asfortranarray(grid.vmapP, dtype=np.int64),
+            np.asfortranarray(grid.boundarycodes, dtype=np.int64),
+        ]
+        (d.D, d.w, d.volume_metrics, d.surface_metrics, d.vmapM, d.vmapP, d.boundary_codes) = [
+            k.ctypes.data_as(ctypes.c_void_p) for k in keep
+        ]
+        d.device = self.device
+        h = ctypes.c_void_p()
+        st = L.rb200_create(ctypes.byref(d), ctypes.byref(h))
+        self._h = h
+        if st != 0:
+            msg = L.rb200_last_error(h).decode() if h else ""
+            if h:
+                L.rb200_destroy(h)
+            self._h = None
+            raise RB200Error(st, msg)
+        info = (ctypes.c_int64 * 8)()
+        L.rb200_get_info(h, info, 8)
+        self.info = list(info)
+        self.geometry = "affine" if info[4] == 0 else "curved"
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                _lib.lib().rb200_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @property
+    def MJ(self):
+        return self.grid.volume_weights()
+
+    def __call__(self, dq, q, time=0.0, increment=True):
+        """(dg::DGSEM)(dq, q, time; increment) (dgsem.jl:84-126)."""
+        _lib.check(_lib.lib().rb200_tendency(self._h, dq.ptr(), q.ptr(), float(time), int(bool(increment)),
+                                             _stream_ptr()), self._h)
+        return dq
+
+    def lsrk54_steps(self, q, dq, time, dt, nsteps):
+        _lib.check(_lib.lib().rb200_lsrk54_step(self._h, q.ptr(), dq.ptr() if dq is not None else None,
+                                                float(time), float(dt), int(nsteps), _stream_ptr()), self._h)
+
+    def lsrk54_steps_host(self, q_host, time, dt, nsteps):
+        """nsteps LSRK(5,4) steps on a host array (Np, Ns, E) column-major, in place."""
+        if not (q_host.flags["F_CONTIGUOUS"] and q_host.dtype == np.float64):
+            raise ValueError("q_host must be a column-major float64 array")
+        _lib.check(_lib.lib().rb200_lsrk54_step_host(self._h, q_host.ctypes.data_as(ctypes.c_void_p), float(time),
+                                                     float(dt), int(nsteps), _stream_ptr()), self._h)
+
+    def face_vmapP(self):
+        torch = _torch()
+        out = torch.empty((self.grid.E, 2 * self.grid.dim * self.grid.nfp), dtype=torch.int64, device="cuda")
+        _lib.check(_lib.lib().rb200_face_vmapP(self._h, ctypes.c_void_p(out.data_ptr()), _stream_ptr()), self._h)
+        return np.asfortranarray(out.cpu().numpy().T)
+
+
+# ------------------------------------------------------------------------------- LSRK(5,4)
+
+
+class LSRK54:
+    """LSRK54(rhs!, q, dt; t0 = 0) (src/balancelaws/odesolvers.jl:63-66, 32-49)."""
+
+    def __init__(self, dg, q, dt, t0=0.0):
+        self.dg = dg
+        self.dt = float(dt)
+        self.time = float(t0)
+        self.dq = q.similar()  # fill!(dq, 0)
+
+    def dostep(self, q, nsteps=1):
+        """dostep!(q, lsrk) (odesolvers.jl:51-61), `nsteps` times with the same dt."""
+        self.dg.lsrk54_steps(q, self.dq, self.time, self.dt, nsteps)
+        for _ in range(nsteps):
+            self.time += self.dt
+
+
+def solve(q, timeend, solver, after_step=None, adjust_final=True):
+    """solve!(q, timeend, solver; after_step, adjust_final) (odesolvers.jl:9-30).
+
+    The reference loop is `time = solver.time; if time + dt >= timeend (dt = timeend -
+    time; final); dostep!; after_step(step, time, q)`.  Here the number of non-final
+    steps is found by replaying the same floating-point time accumulation on the host,
+    and (without an after_step callback) those steps go to the device in one call."""
+    step = 0
+    while True:
+        if after_step is None:
+            n, t = 0, solver.time
+            while not (t + solver.dt >= timeend):
+                t += solver.dt
+                n += 1
+            if n:
+                solver.dostep(q, n)
+                step += n
+        time = solver.time
+        final = time + solver.dt >= timeend
+        if final and adjust_final:
+            solver.dt = timeend - time
+        solver.dostep(q, 1)
+        step += 1
+        if after_step is not None:
+            after_step(step, time, q)
+        if final:
+            return step
+
+
+# ------------------------------------------------------------------------------- measures
+
+
+def weightednorm(dg, q, p=2, componentwise=False):
+    """weightednorm(dg, q, p=2; componentwise) (src/balancelaws/measures.jl:6-21)."""
+    if p != 2:
+        raise NotImplementedError("only p = 2 is implemented on the device")
+    out = (ctypes.c_double * (q.ns + 1))()
+    _lib.check(_lib.lib().rb200_weightednorm(dg._h, q.ptr(), out, _stream_ptr()), dg._h)
+    vals = list(out)
+    return vals[: q.ns] if componentwise else vals[q.ns]
+
+
+def integrals(dg, q):
+    """sum(MJ .* q_s) for every field (FP64): the conservation monitor."""
+    out = (ctypes.c_double * q.ns)()
+    _lib.check(_lib.lib().rb200_integrals(dg._h, q.ptr(), out, _stream_ptr()), dg._h)
+    return list(out)

@@ -1,0 +1,111 @@
+"""ctypes binding of libravenb200.so (the C ABI declared in include/raven_b200.h).
+
+The shared library is built in-tree by ``raven.jl_b200/build.py``.  There is no
+fallback: if the library is missing or fails to load, every entry point raises.
+"""
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libravenb200.so")
+
+RB200_ABI_VERSION = 1
+STATUS = {
+    0: "RB200_OK",
+    1: "RB200_ERR_BAD_ARG",
+    2: "RB200_ERR_SHAPE",
+    3: "RB200_ERR_OOM",
+    4: "RB200_ERR_CUDA",
+    5: "RB200_ERR_TIMEOUT",
+    6: "RB200_ERR_UNSUPPORTED",
+}
+LAW_ADVECTION, LAW_EULER = 0, 1
+FORM_WEAK, FORM_FLUXDIFF = 0, 1
+FLUX_CENTRAL, FLUX_KENNEDY_GRUBER, FLUX_ENTROPY_CONSERVATIVE, FLUX_RUSANOV = 0, 1, 2, 3
+PRECISION_FP64, PRECISION_FP32_BULK = 0, 1
+
+EXPORTED = [
+    "rb200_create",
+    "rb200_destroy",
+    "rb200_tendency",
+    "rb200_lsrk54_step",
+    "rb200_lsrk54_step_host",
+    "rb200_weightednorm",
+    "rb200_integrals",
+    "rb200_face_vmapP",
+    "rb200_get_info",
+    "rb200_last_error",
+    "rb200_status_string",
+]
+
+
+class Desc(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", ctypes.c_int32),
+        ("dim", ctypes.c_int32),
+        ("nq", ctypes.c_int32),
+        ("law", ctypes.c_int32),
+        ("num_elements", ctypes.c_int64),
+        ("volume_form", ctypes.c_int32),
+        ("volume_flux", ctypes.c_int32),
+        ("surface_flux", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("gamma", ctypes.c_double),
+        ("advection_velocity", ctypes.c_double * 3),
+        ("D", ctypes.c_void_p),
+        ("w", ctypes.c_void_p),
+        ("volume_metrics", ctypes.c_void_p),
+        ("surface_metrics", ctypes.c_void_p),
+        ("vmapM", ctypes.c_void_p),
+        ("vmapP", ctypes.c_void_p),
+        ("boundary_codes", ctypes.c_void_p),
+        ("device", ctypes.c_int32),
+    ]
+
+
+class RB200Error(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"CUDA extension {LIB_PATH} is missing; build it with `python raven.jl_b200/build.py` "
+            "(there is no CPU fallback)"
+        )
+    L = ctypes.CDLL(LIB_PATH)
+    P, I32, I64, D = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+    L.rb200_create.argtypes = [ctypes.POINTER(Desc), ctypes.POINTER(P)]
+    L.rb200_destroy.argtypes = [P]
+    L.rb200_tendency.argtypes = [P, P, P, D, I32, P]
+    L.rb200_lsrk54_step.argtypes = [P, P, P, D, D, I32, P]
+    L.rb200_lsrk54_step_host.argtypes = [P, P, D, D, I32, P]
+    L.rb200_weightednorm.argtypes = [P, P, P, P]
+    L.rb200_integrals.argtypes = [P, P, P, P]
+    L.rb200_face_vmapP.argtypes = [P, P, P]
+    L.rb200_get_info.argtypes = [P, P, I32]
+    L.rb200_last_error.argtypes = [P]
+    L.rb200_last_error.restype = ctypes.c_char_p
+    L.rb200_status_string.argtypes = [ctypes.c_int]
+    L.rb200_status_string.restype = ctypes.c_char_p
+    for name in EXPORTED:
+        if name not in ("rb200_last_error", "rb200_status_string"):
+            getattr(L, name).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def check(status, handle=None):
+    if status != 0:
+        msg = lib().rb200_last_error(handle).decode() if handle else lib().rb200_status_string(status).decode()
+        raise RB200Error(status, msg)

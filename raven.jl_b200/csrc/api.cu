@@ -1,0 +1,485 @@
+// Host runtime behind the C ABI (include/raven_b200.h).
+//
+// rb200_create turns the arrays of a Raven `Grid` into the compact device form the
+// kernels read:
+//  * geometry: an unwarped brick (what Raven's `isunwarpedbrick` path produces,
+//    gridmanager.jl:1166) is detected node by node and stored as 4 doubles per
+//    element (dRdX diagonal, J); anything else keeps per-node metric rows
+//    wJ*dRdX[dir,:] plus MJI and MJ, and per-face-node (n, wsJ);
+//  * connectivity: vmapM/vmapP (lobattocells.jl:2278-2291) become one int32
+//    neighbour per element face.  Every node of every face is checked against the
+//    given vmapP before the table is accepted, so the kernels' implied indexing is
+//    the reference's indexing bit for bit (rb200_face_vmapP rebuilds it on the GPU).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/raven_b200.h"
+#include "rb200_internal.h"
+
+using namespace rb200;
+
+struct rb200_handle {
+    int dim = 0, nq = 0, np = 0, nfp = 0, nf = 0, ns = 0;
+    int64_t E = 0;
+    int law = 0, form = 0, vflux = 0, sflux = 0, prec = 0, combo = 0, geom = 0;
+    double gamma = 1.4, adv[3] = {0, 0, 0};
+    double D[kMaxNq * kMaxNq] = {0}, w[kMaxNq] = {0};
+    int device = 0;
+    double* d_elem_geo = nullptr;
+    double* d_vgeo = nullptr;
+    double* d_sgeo = nullptr;
+    double* d_w = nullptr;
+    int32_t* d_nbr = nullptr;
+    double* d_qtmp = nullptr;
+    float* d_dq32 = nullptr;
+    double* d_hq = nullptr;   // device copy of a host state (rb200_lsrk54_step_host)
+    double* d_hdq = nullptr;  // its LSRK register
+    double* d_partial = nullptr;
+    double* d_sums = nullptr;
+    int red_blocks = 0;
+    std::string err;
+};
+
+namespace {
+
+// LSRK(5,4) coefficients (odesolvers.jl:163-189): exact rationals, each rounded once.
+const double RKA[5] = {0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
+                       -3550918686646.0 / 2091501179385.0, -1275806237668.0 / 842570457699.0};
+const double RKB[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+                       1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+                       2277821191437.0 / 14882151754819.0};
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+rb200_status fail(rb200_handle* h, rb200_status st, const std::string& msg) {
+    if (h) h->err = msg;
+    return st;
+}
+
+rb200_status cuda_fail(rb200_handle* h, cudaError_t e, const char* where) {
+    return fail(h, RB200_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+// 0-based volume node of face f at in-face index j (cellfaceindices, lobattocells.jl:2012-2053)
+int face_node(int dim, int nq, int f, int j) {
+    const int dir = f / 2, c = (f % 2) ? nq - 1 : 0;
+    if (dim == 2) return dir == 0 ? c + nq * j : j + nq * c;
+    const int j1 = j % nq, j2 = j / nq;
+    if (dir == 0) return c + nq * (j1 + nq * j2);
+    if (dir == 1) return j1 + nq * (c + nq * j2);
+    return j1 + nq * (j2 + nq * c);
+}
+
+template <typename T>
+rb200_status dev_alloc(rb200_handle* h, T** p, size_t count) {
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(h, RB200_ERR_OOM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+    }
+    return RB200_OK;
+}
+
+void free_all(rb200_handle* h) {
+    void* ptrs[] = {h->d_elem_geo, h->d_vgeo, h->d_sgeo, h->d_w, h->d_nbr, h->d_qtmp,
+                    h->d_dq32,     h->d_hq,   h->d_hdq,  h->d_partial, h->d_sums};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    h->d_elem_geo = h->d_vgeo = h->d_sgeo = h->d_w = h->d_qtmp = h->d_hq = h->d_hdq = h->d_partial = h->d_sums =
+        nullptr;
+    h->d_nbr = nullptr;
+    h->d_dq32 = nullptr;
+}
+
+StageArgs base_args(const rb200_handle* h) {
+    StageArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.elem_geo = h->d_elem_geo;
+    a.vgeo = h->d_vgeo;
+    a.sgeo = h->d_sgeo;
+    a.nbr = h->d_nbr;
+    a.E = h->E;
+    a.surface_rusanov = h->sflux == RB200_FLUX_RUSANOV ? 1 : 0;
+    a.gamma = h->gamma;
+    for (int d = 0; d < 3; ++d) a.adv[d] = h->adv[d];
+    std::memcpy(a.D, h->D, sizeof(a.D));
+    std::memcpy(a.w, h->w, sizeof(a.w));
+    return a;
+}
+
+rb200_status run_steps(rb200_handle* h, double* q, void* dq, double dt, int32_t nsteps, cudaStream_t st) {
+    const size_t nstate = (size_t)h->np * h->ns * h->E;
+    if (!h->d_qtmp) {
+        rb200_status s = dev_alloc(h, &h->d_qtmp, nstate);
+        if (s != RB200_OK) return s;
+    }
+    StageArgs a = base_args(h);
+    a.dq = h->prec == RB200_PRECISION_FP32_BULK ? (void*)h->d_dq32 : dq;
+    double* cur = q;
+    double* oth = h->d_qtmp;
+    for (int32_t step = 0; step < nsteps; ++step) {
+        for (int stg = 0; stg < 5; ++stg) {
+            a.q_in = cur;
+            a.q_out = oth;
+            a.mode = RKA[stg] == 0.0 ? MODE_STAGE_FIRST : MODE_STAGE;
+            a.rka = RKA[stg];
+            a.rkb_dt = RKB[stg] * dt;
+            cudaError_t e = launch_stage(h->dim, h->nq, h->combo, h->geom, h->prec, a, st);
+            if (e != cudaSuccess) return cuda_fail(h, e, "stage kernel launch");
+            double* t = cur;
+            cur = oth;
+            oth = t;
+        }
+    }
+    if (cur != q) {
+        cudaError_t e = cudaMemcpyAsync(q, cur, nstate * sizeof(double), cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return cuda_fail(h, e, "state copy-back");
+    }
+    return RB200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* rb200_status_string(rb200_status s) {
+    switch (s) {
+        case RB200_OK: return "ok";
+        case RB200_ERR_BAD_ARG: return "bad argument";
+        case RB200_ERR_SHAPE: return "shape mismatch";
+        case RB200_ERR_OOM: return "out of device memory";
+        case RB200_ERR_CUDA: return "CUDA error";
+        case RB200_ERR_TIMEOUT: return "timeout";
+        case RB200_ERR_UNSUPPORTED: return "unsupported";
+    }
+    return "unknown status";
+}
+
+const char* rb200_last_error(const rb200_handle* h) {
+    if (!h) return "null handle";
+    return h->err.c_str();
+}
+
+rb200_status rb200_create(const rb200_desc* d, rb200_handle** out) {
+    if (!out) return RB200_ERR_BAD_ARG;
+    *out = nullptr;
+    if (!d) return RB200_ERR_BAD_ARG;
+    if (d->abi_version != RB200_ABI_VERSION) return RB200_ERR_BAD_ARG;
+    rb200_handle* h = new (std::nothrow) rb200_handle();
+    if (!h) return RB200_ERR_OOM;
+    auto bail = [&](rb200_status s) {
+        // the handle is returned even on failure so that rb200_last_error can explain;
+        // the caller must still rb200_destroy it
+        *out = h;
+        return s;
+    };
+    if (d->dim != 2 && d->dim != 3)
+        return bail(fail(h, RB200_ERR_UNSUPPORTED, "dim must be 2 or 3 (1-D grids are not implemented)"));
+    if (d->nq < 2 || d->nq > kMaxNq) return bail(fail(h, RB200_ERR_UNSUPPORTED, "nq must be in 2..8"));
+    if (d->num_elements < 0 || d->num_elements > (int64_t)INT32_MAX)
+        return bail(fail(h, RB200_ERR_BAD_ARG, "num_elements out of range"));
+    if (!d->D || !d->w || !d->volume_metrics || !d->surface_metrics || !d->vmapM || !d->vmapP)
+        return bail(fail(h, RB200_ERR_BAD_ARG, "null host array in descriptor"));
+    h->dim = d->dim;
+    h->nq = d->nq;
+    h->np = d->dim == 2 ? d->nq * d->nq : d->nq * d->nq * d->nq;
+    h->nfp = h->np / d->nq;
+    h->nf = 2 * d->dim;
+    h->E = d->num_elements;
+    h->law = d->law;
+    h->form = d->volume_form;
+    h->vflux = d->volume_flux;
+    h->sflux = d->surface_flux;
+    h->prec = d->precision;
+    h->gamma = d->gamma;
+    h->device = d->device;
+    for (int i = 0; i < 3; ++i) h->adv[i] = d->advection_velocity[i];
+    if (h->prec != RB200_PRECISION_FP64 && h->prec != RB200_PRECISION_FP32_BULK)
+        return bail(fail(h, RB200_ERR_BAD_ARG, "unknown precision"));
+    if (h->sflux != RB200_FLUX_RUSANOV && h->sflux != RB200_FLUX_CENTRAL)
+        return bail(fail(h, RB200_ERR_UNSUPPORTED, "surface flux must be Rusanov or Central"));
+    if (h->law == RB200_LAW_ADVECTION) {
+        h->ns = 1;
+        if (h->form == RB200_FORM_WEAK) h->combo = ADV_WEAK;
+        else if (h->form == RB200_FORM_FLUXDIFF && h->vflux == RB200_FLUX_CENTRAL) h->combo = ADV_FDC;
+        else return bail(fail(h, RB200_ERR_UNSUPPORTED, "advection supports WeakForm and FluxDifferencing(Central)"));
+    } else if (h->law == RB200_LAW_EULER) {
+        h->ns = h->dim + 2;
+        if (!(h->gamma > 1.0)) return bail(fail(h, RB200_ERR_BAD_ARG, "gamma must be > 1"));
+        if (h->form == RB200_FORM_WEAK) h->combo = EUL_WEAK;
+        else if (h->form == RB200_FORM_FLUXDIFF) {
+            if (h->vflux == RB200_FLUX_CENTRAL) h->combo = EUL_FDC;
+            else if (h->vflux == RB200_FLUX_KENNEDY_GRUBER) h->combo = EUL_KG;
+            else if (h->vflux == RB200_FLUX_ENTROPY_CONSERVATIVE) h->combo = EUL_EC;
+            else return bail(fail(h, RB200_ERR_UNSUPPORTED, "unknown volume flux"));
+        } else return bail(fail(h, RB200_ERR_BAD_ARG, "unknown volume form"));
+    } else {
+        return bail(fail(h, RB200_ERR_BAD_ARG, "unknown law"));
+    }
+    const int dim = h->dim, nq = h->nq, np = h->np, nfp = h->nfp, nf = h->nf;
+    const int64_t E = h->E;
+    for (int i = 0; i < nq * nq; ++i) h->D[i] = d->D[i];
+    for (int i = 0; i < nq; ++i) h->w[i] = d->w[i];
+
+    // ---------------------------------------------------------------- geometry
+    const int nvm = dim * dim + 2;  // dRdX, J, wJ
+    const int nsm = dim + 2;        // n, sJ, wsJ
+    const double* vm = d->volume_metrics;
+    const double* sm = d->surface_metrics;
+    bool affine = true;
+    std::vector<double> eg(4 * (size_t)E, 0.0);
+    for (int64_t e = 0; e < E && affine; ++e) {
+        const double* m = vm + (size_t)np * nvm * e;
+        double diag[3], J = m[(size_t)np * (dim * dim)];
+        for (int a = 0; a < dim; ++a) diag[a] = m[(size_t)np * (a + dim * a)];
+        for (int n = 0; n < np && affine; ++n) {
+            for (int a = 0; a < dim; ++a)
+                for (int b = 0; b < dim; ++b) {
+                    const double v = m[n + (size_t)np * (a + dim * b)];
+                    if (a == b ? v != diag[a] : v != 0.0) affine = false;
+                }
+            if (m[n + (size_t)np * (dim * dim)] != J) affine = false;
+            const int idx[3] = {n % nq, (n / nq) % nq, n / (nq * nq)};
+            double wJ = h->w[idx[0]];
+            for (int k = 1; k < dim; ++k) wJ = wJ * h->w[idx[k]];
+            wJ = wJ * J;
+            if (m[n + (size_t)np * (dim * dim + 1)] != wJ) affine = false;
+        }
+        for (int f = 0; f < nf && affine; ++f) {
+            const int dir = f / 2;
+            const double sJ = std::fabs(J * diag[dir]);
+            for (int j = 0; j < nfp && affine; ++j) {
+                const double* s = sm + (size_t)nsm * ((size_t)nf * nfp * e + (size_t)f * nfp + j);
+                for (int k = 0; k < dim; ++k) {
+                    const double want = k == dir ? (f % 2 ? 1.0 : -1.0) : 0.0;
+                    if (s[k] != want) affine = false;
+                }
+                double wsJ;
+                if (dim == 2) wsJ = sJ * h->w[j];
+                else wsJ = (sJ * h->w[j % nq]) * h->w[j / nq];
+                if (s[dim + 1] != wsJ) affine = false;
+            }
+        }
+        for (int a = 0; a < dim; ++a) eg[4 * e + a] = diag[a];
+        eg[4 * e + 3] = J;
+    }
+    h->geom = affine ? GEOM_AFFINE : GEOM_CURVED;
+
+    // ------------------------------------------------------------- connectivity
+    std::vector<int32_t> nbr((size_t)nf * E, -1);
+    for (int64_t e = 0; e < E; ++e)
+        for (int f = 0; f < nf; ++f) {
+            const size_t base = (size_t)nf * nfp * e + (size_t)f * nfp;
+            const int64_t bcode = d->boundary_codes ? d->boundary_codes[(size_t)nf * e + f] : 0;
+            for (int j = 0; j < nfp; ++j)
+                if (d->vmapM[base + j] != (int64_t)np * e + face_node(dim, nq, f, j) + 1)
+                    return bail(fail(h, RB200_ERR_SHAPE, "vmapM is not Raven's face-node numbering"));
+            if (bcode != 0) {
+                nbr[(size_t)nf * e + f] = -1;
+                continue;
+            }
+            const int64_t p0 = d->vmapP[base] - 1;
+            const int64_t ne = p0 / np;
+            bool ok = ne >= 0 && ne < E;
+            for (int j = 0; j < nfp && ok; ++j)
+                ok = d->vmapP[base + j] == ne * np + face_node(dim, nq, f ^ 1, j) + 1;
+            if (!ok) {
+                bool self = true;  // non-conforming / unconnected faces keep vmapP = vmapM
+                for (int j = 0; j < nfp && self; ++j) self = d->vmapP[base + j] == d->vmapM[base + j];
+                if (self) {
+                    nbr[(size_t)nf * e + f] = -1;
+                    continue;
+                }
+                return bail(fail(h, RB200_ERR_UNSUPPORTED,
+                                 "face connectivity is not an aligned conforming neighbour (rotated faces are not "
+                                 "implemented)"));
+            }
+            nbr[(size_t)nf * e + f] = (int32_t)ne;
+        }
+
+    // ----------------------------------------------------------------- upload
+    DeviceGuard guard(h->device);
+    rb200_status st;
+    if ((st = dev_alloc(h, &h->d_nbr, nbr.size())) != RB200_OK) return bail(st);
+    if ((st = dev_alloc(h, &h->d_w, (size_t)nq)) != RB200_OK) return bail(st);
+    cudaError_t ce = cudaMemcpy(h->d_nbr, nbr.data(), nbr.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    if (ce == cudaSuccess) ce = cudaMemcpy(h->d_w, h->w, nq * sizeof(double), cudaMemcpyHostToDevice);
+    if (ce != cudaSuccess) return bail(cuda_fail(h, ce, "upload"));
+    if (affine) {
+        if ((st = dev_alloc(h, &h->d_elem_geo, eg.size())) != RB200_OK) return bail(st);
+        ce = cudaMemcpy(h->d_elem_geo, eg.data(), eg.size() * sizeof(double), cudaMemcpyHostToDevice);
+        if (ce != cudaSuccess) return bail(cuda_fail(h, ce, "upload"));
+    } else {
+        const int nvg = dim * dim + 2;  // wJ*dRdX[dir,d] (dir-major), MJI, MJ
+        std::vector<double> vg((size_t)np * nvg * E);
+        for (int64_t e = 0; e < E; ++e) {
+            const double* m = vm + (size_t)np * nvm * e;
+            double* g = vg.data() + (size_t)np * nvg * e;
+            for (int n = 0; n < np; ++n) {
+                const double wJ = m[n + (size_t)np * (dim * dim + 1)];
+                for (int dir = 0; dir < dim; ++dir)
+                    for (int k = 0; k < dim; ++k)
+                        g[n + (size_t)np * (dir * dim + k)] = wJ * m[n + (size_t)np * (dir + dim * k)];
+                g[n + (size_t)np * (dim * dim)] = 1.0 / wJ;
+                g[n + (size_t)np * (dim * dim + 1)] = wJ;
+            }
+        }
+        std::vector<double> sg((size_t)(dim + 1) * nf * nfp * E);
+        for (size_t k = 0; k < (size_t)nf * nfp * E; ++k) {
+            for (int c = 0; c < dim; ++c) sg[(dim + 1) * k + c] = sm[nsm * k + c];
+            sg[(dim + 1) * k + dim] = sm[nsm * k + dim + 1];
+        }
+        if ((st = dev_alloc(h, &h->d_vgeo, vg.size())) != RB200_OK) return bail(st);
+        if ((st = dev_alloc(h, &h->d_sgeo, sg.size())) != RB200_OK) return bail(st);
+        ce = cudaMemcpy(h->d_vgeo, vg.data(), vg.size() * sizeof(double), cudaMemcpyHostToDevice);
+        if (ce == cudaSuccess) ce = cudaMemcpy(h->d_sgeo, sg.data(), sg.size() * sizeof(double), cudaMemcpyHostToDevice);
+        if (ce != cudaSuccess) return bail(cuda_fail(h, ce, "upload"));
+    }
+    if (h->prec == RB200_PRECISION_FP32_BULK) {
+        const size_t n = (size_t)np * h->ns * E;
+        if ((st = dev_alloc(h, &h->d_dq32, n)) != RB200_OK) return bail(st);
+        ce = cudaMemset(h->d_dq32, 0, n * sizeof(float));
+        if (ce != cudaSuccess) return bail(cuda_fail(h, ce, "memset"));
+    }
+    h->red_blocks = 296;
+    if ((st = dev_alloc(h, &h->d_partial, (size_t)h->red_blocks * 2 * h->ns)) != RB200_OK) return bail(st);
+    if ((st = dev_alloc(h, &h->d_sums, (size_t)2 * h->ns)) != RB200_OK) return bail(st);
+    if (stage_smem_bytes(dim, nq, h->combo, h->geom, h->prec) == 0)
+        return bail(fail(h, RB200_ERR_UNSUPPORTED, "no kernel instantiation for this configuration"));
+    *out = h;
+    return RB200_OK;
+}
+
+rb200_status rb200_destroy(rb200_handle* h) {
+    if (!h) return RB200_ERR_BAD_ARG;
+    {
+        DeviceGuard guard(h->device);
+        free_all(h);
+    }
+    delete h;
+    return RB200_OK;
+}
+
+rb200_status rb200_tendency(rb200_handle* h, double* dq, const double* q, double time, int32_t increment,
+                            void* stream) {
+    (void)time;  // the advection and Euler laws have no time-dependent sources
+    if (!h) return RB200_ERR_BAD_ARG;
+    if (!dq || !q) return fail(h, RB200_ERR_BAD_ARG, "null state pointer");
+    if (h->E == 0) return RB200_OK;
+    DeviceGuard guard(h->device);
+    StageArgs a = base_args(h);
+    a.q_in = q;
+    a.dq = dq;
+    a.mode = increment ? MODE_TENDENCY_INC : MODE_TENDENCY_SET;
+    cudaError_t e = launch_stage(h->dim, h->nq, h->combo, h->geom, h->prec, a, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "tendency kernel launch");
+    return RB200_OK;
+}
+
+rb200_status rb200_lsrk54_step(rb200_handle* h, double* q, double* dq, double time, double dt, int32_t nsteps,
+                               void* stream) {
+    (void)time;
+    if (!h) return RB200_ERR_BAD_ARG;
+    if (!q || (!dq && h->prec == RB200_PRECISION_FP64)) return fail(h, RB200_ERR_BAD_ARG, "null state pointer");
+    if (nsteps < 0 || !std::isfinite(dt)) return fail(h, RB200_ERR_BAD_ARG, "bad nsteps or dt");
+    if (h->E == 0 || nsteps == 0) return RB200_OK;
+    DeviceGuard guard(h->device);
+    return run_steps(h, q, dq, dt, nsteps, (cudaStream_t)stream);
+}
+
+rb200_status rb200_lsrk54_step_host(rb200_handle* h, double* q_host, double time, double dt, int32_t nsteps,
+                                    void* stream) {
+    (void)time;
+    if (!h) return RB200_ERR_BAD_ARG;
+    if (!q_host) return fail(h, RB200_ERR_BAD_ARG, "null state pointer");
+    if (nsteps < 0 || !std::isfinite(dt)) return fail(h, RB200_ERR_BAD_ARG, "bad nsteps or dt");
+    if (h->E == 0) return RB200_OK;
+    DeviceGuard guard(h->device);
+    const size_t n = (size_t)h->np * h->ns * h->E;
+    rb200_status st;
+    if (!h->d_hq && (st = dev_alloc(h, &h->d_hq, n)) != RB200_OK) return st;
+    if (!h->d_hdq && (st = dev_alloc(h, &h->d_hdq, n)) != RB200_OK) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMemcpyAsync(h->d_hq, q_host, n * sizeof(double), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "host-to-device copy");
+    if ((st = run_steps(h, h->d_hq, h->d_hdq, dt, nsteps, s)) != RB200_OK) return st;
+    e = cudaMemcpyAsync(q_host, h->d_hq, n * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "device-to-host copy");
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "stream synchronize");
+    return RB200_OK;
+}
+
+static rb200_status sums(rb200_handle* h, const double* q, double* host, cudaStream_t s) {
+    if (!h) return RB200_ERR_BAD_ARG;
+    if (!q || !host) return fail(h, RB200_ERR_BAD_ARG, "null pointer");
+    DeviceGuard guard(h->device);
+    cudaError_t e = launch_weighted_sums(q, h->d_elem_geo, h->d_vgeo, h->d_w, h->dim, h->nq, h->ns, h->E, h->geom,
+                                         h->d_partial, h->red_blocks, h->d_sums, s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "reduction launch");
+    e = cudaMemcpyAsync(host, h->d_sums, 2 * h->ns * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "reduction readback");
+    return RB200_OK;
+}
+
+rb200_status rb200_weightednorm(rb200_handle* h, const double* q, double* out, void* stream) {
+    double buf[2 * 5];
+    rb200_status st = sums(h, q, buf, (cudaStream_t)stream);
+    if (st != RB200_OK) return st;
+    double tot = 0.0;
+    for (int s = 0; s < h->ns; ++s) {
+        out[s] = std::sqrt(buf[s]);
+        tot += out[s] * out[s];
+    }
+    out[h->ns] = std::sqrt(tot);
+    return RB200_OK;
+}
+
+rb200_status rb200_integrals(rb200_handle* h, const double* q, double* out, void* stream) {
+    double buf[2 * 5];
+    rb200_status st = sums(h, q, buf, (cudaStream_t)stream);
+    if (st != RB200_OK) return st;
+    for (int s = 0; s < h->ns; ++s) out[s] = buf[h->ns + s];
+    return RB200_OK;
+}
+
+rb200_status rb200_face_vmapP(rb200_handle* h, int64_t* vmapP_out, void* stream) {
+    if (!h) return RB200_ERR_BAD_ARG;
+    if (!vmapP_out) return fail(h, RB200_ERR_BAD_ARG, "null pointer");
+    DeviceGuard guard(h->device);
+    cudaError_t e = launch_face_vmapP(h->d_nbr, h->dim, h->nq, h->E, vmapP_out, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "vmapP kernel launch");
+    return RB200_OK;
+}
+
+rb200_status rb200_get_info(const rb200_handle* h, int64_t* info, int32_t n) {
+    if (!h || !info) return RB200_ERR_BAD_ARG;
+    const int64_t bytes_q = 8, bytes_dq = h->prec == RB200_PRECISION_FP32_BULK ? 4 : 8;
+    int64_t per_node = h->ns * (2 * bytes_q + 2 * bytes_dq);
+    if (h->geom == GEOM_CURVED)
+        per_node += (h->dim * h->dim + 1) * 8 + (int64_t)h->nf * h->nfp * (h->dim + 1) * 8 / h->np;
+    const int64_t v[8] = {h->dim, h->nq, h->ns, h->E, h->geom, h->prec, 5, per_node};
+    for (int i = 0; i < n && i < 8; ++i) info[i] = v[i];
+    return RB200_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,65 @@
+// Internal declarations shared by the host runtime (api.cu) and the kernel
+// instantiation units (stage_*.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+namespace rb200 {
+
+// Physics + volume-form combination (template parameter of the stage kernel).
+enum Combo : int {
+    ADV_WEAK = 0,  // AdvectionLaw, WeakForm
+    ADV_FDC = 1,   // AdvectionLaw, FluxDifferencingForm(CentralFlux())
+    EUL_WEAK = 2,  // EulerLaw, WeakForm
+    EUL_FDC = 3,   // EulerLaw, FluxDifferencingForm(CentralFlux())
+    EUL_KG = 4,    // EulerLaw, FluxDifferencingForm(KennedyGruberFlux())
+    EUL_EC = 5,    // EulerLaw, FluxDifferencingForm(EntropyConservativeFlux())
+    NUM_COMBOS = 6
+};
+
+enum Geom : int { GEOM_AFFINE = 0, GEOM_CURVED = 1 };
+
+// What a launch of the stage kernel does with dq and q.
+enum Mode : int {
+    MODE_TENDENCY_SET = 0,  // dq = RHS(q)
+    MODE_TENDENCY_INC = 1,  // dq = dq + RHS(q)
+    MODE_STAGE = 2,         // dq = rka*dq + RHS(q); q_out = q_in + rkb_dt*dq
+    MODE_STAGE_FIRST = 3    // rka == 0: dq = RHS(q) without reading dq; q_out = q_in + rkb_dt*dq
+};
+
+constexpr int kMaxNq = 8;
+
+struct StageArgs {
+    const double* q_in;   // (Np, Ns, E)
+    double* q_out;        // stage modes only (may alias nothing that q_in aliases)
+    void* dq;             // double* (FP64) or float* (FP32 bulk), read-modify-write in place
+    const double* elem_geo;  // affine: (4, E): drdx, dsdy, dtdz, J
+    const double* vgeo;      // curved: (Np, dim*dim+1, E): wJ*dRdX[dir,d] (dir-major), MJI
+    const double* sgeo;      // curved: (dim+1, 2*dim*Nfp, E): n, wsJ
+    const int32_t* nbr;      // (2*dim, E): neighbour element across each face, -1 = boundary
+    int64_t E;
+    int32_t mode;
+    int32_t surface_rusanov;  // 1 Rusanov, 0 central
+    double rka;
+    double rkb_dt;
+    double gamma;
+    double adv[3];
+    double D[kMaxNq * kMaxNq];  // D[i + nq*j] = l_j'(r_i)
+    double w[kMaxNq];
+};
+
+// Launches one stage kernel; returns cudaSuccess or the launch error.
+cudaError_t launch_stage(int dim, int nq, int combo, int geom, int fp32, const StageArgs& a, cudaStream_t s);
+// Dynamic shared memory the kernel needs (bytes) and threads per block; 0 if not built.
+size_t stage_smem_bytes(int dim, int nq, int combo, int geom, int fp32);
+
+// Reductions and face-map expansion (reduce.cu).
+cudaError_t launch_weighted_sums(const double* q, const double* elem_geo, const double* vgeo, const double* w,
+                                 int dim, int nq, int ns, int64_t E, int geom, double* partial, int nblocks,
+                                 double* out_dev, cudaStream_t s);
+cudaError_t launch_face_vmapP(const int32_t* nbr, int dim, int nq, int64_t E, int64_t* out, cudaStream_t s);
+
+}  // namespace rb200

@@ -1,0 +1,112 @@
+// FP64 reductions behind weightednorm / conservation integrals (measures.jl:6-33) and
+// the device-side rebuild of vmapP from the neighbour table.
+//
+// The reductions are deterministic: a fixed number of CTAs each own a fixed,
+// strided set of elements, partial sums are combined in a fixed tree, and a single
+// CTA adds the per-CTA partials in index order.
+#include "rb200_internal.h"
+
+namespace rb200 {
+
+namespace {
+
+constexpr int kRedThreads = 256;
+
+// partial[(blockIdx.x * 2*ns) + s]       = sum MJ q_s^2
+// partial[(blockIdx.x * 2*ns) + ns + s]  = sum MJ q_s
+__global__ void __launch_bounds__(kRedThreads) weighted_sums_kernel(const double* __restrict__ q,
+                                                                    const double* __restrict__ elem_geo,
+                                                                    const double* __restrict__ vgeo,
+                                                                    const double* __restrict__ wgt, int dim, int nq,
+                                                                    int ns, int64_t E, int geom,
+                                                                    double* __restrict__ partial) {
+    __shared__ double red[kRedThreads];
+    const int np = dim == 2 ? nq * nq : nq * nq * nq;
+    const int nvg = dim * dim + 2;
+    for (int s = 0; s < ns; ++s) {
+        double a2 = 0.0, a1 = 0.0;
+        for (int64_t e = blockIdx.x; e < E; e += gridDim.x) {
+            for (int n = threadIdx.x; n < np; n += blockDim.x) {
+                double mj;
+                if (geom == GEOM_AFFINE) {
+                    const int i = n % nq, j = (n / nq) % nq, k = n / (nq * nq);
+                    mj = wgt[i] * wgt[j];
+                    if (dim == 3) mj = mj * wgt[k];
+                    mj = mj * elem_geo[4 * e + 3];
+                } else {
+                    mj = vgeo[((size_t)e * nvg + dim * dim + 1) * np + n];
+                }
+                const double v = q[((size_t)e * ns + s) * np + n];
+                a2 += mj * (v * v);
+                a1 += mj * v;
+            }
+        }
+        for (int pass = 0; pass < 2; ++pass) {
+            red[threadIdx.x] = pass == 0 ? a2 : a1;
+            __syncthreads();
+            for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+                if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) partial[(size_t)blockIdx.x * 2 * ns + pass * ns + s] = red[0];
+            __syncthreads();
+        }
+    }
+}
+
+__global__ void finish_sums_kernel(const double* __restrict__ partial, int nblocks, int nvals, double* out) {
+    const int v = threadIdx.x;
+    if (v >= nvals) return;
+    double acc = 0.0;
+    for (int b = 0; b < nblocks; ++b) acc += partial[(size_t)b * nvals + v];
+    out[v] = acc;
+}
+
+__global__ void face_vmapP_kernel(const int32_t* __restrict__ nbr, int dim, int nq, int64_t E,
+                                  int64_t* __restrict__ out) {
+    const int np = dim == 2 ? nq * nq : nq * nq * nq;
+    const int nfp = dim == 2 ? nq : nq * nq;
+    const int nf = 2 * dim;
+    const int64_t total = E * nf * nfp;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int j = (int)(t % nfp);
+        const int f = (int)((t / nfp) % nf);
+        const int64_t e = t / ((int64_t)nfp * nf);
+        const int dir = f / 2, side = f % 2;
+        const int ne = nbr[(size_t)nf * e + f];
+        // node of face f (side) or of the opposite face (1-side) at in-face index j
+        auto facenode = [&](int sd) {
+            const int c = sd ? nq - 1 : 0;
+            if (dim == 2) return dir == 0 ? c + nq * j : j + nq * c;
+            const int j1 = j % nq, j2 = j / nq;
+            if (dir == 0) return c + nq * (j1 + nq * j2);
+            if (dir == 1) return j1 + nq * (c + nq * j2);
+            return j1 + nq * (j2 + nq * c);
+        };
+        out[t] = ne < 0 ? e * np + facenode(side) + 1 : (int64_t)ne * np + facenode(1 - side) + 1;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_weighted_sums(const double* q, const double* elem_geo, const double* vgeo, const double* w, int dim,
+                                 int nq, int ns, int64_t E, int geom, double* partial, int nblocks, double* out_dev,
+                                 cudaStream_t s) {
+    weighted_sums_kernel<<<nblocks, kRedThreads, 0, s>>>(q, elem_geo, vgeo, w, dim, nq, ns, E, geom, partial);
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    finish_sums_kernel<<<1, 32, 0, s>>>(partial, nblocks, 2 * ns, out_dev);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_face_vmapP(const int32_t* nbr, int dim, int nq, int64_t E, int64_t* out, cudaStream_t s) {
+    const int nfp = dim == 2 ? nq : nq * nq;
+    const int64_t total = E * 2 * dim * nfp;
+    if (total == 0) return cudaSuccess;
+    int64_t blocks = (total + 255) / 256;
+    if (blocks > 4096) blocks = 4096;
+    face_vmapP_kernel<<<(unsigned)blocks, 256, 0, s>>>(nbr, dim, nq, E, out);
+    return cudaGetLastError();
+}
+
+}  // namespace rb200

@@ -1,0 +1,490 @@
+// Fused DGSEM stage kernel: volume term + surface term + LSRK(5,4) stage update.
+//
+// One thread owns one volume node; EPB elements share a CTA (EPB*Np threads).  The
+// thread keeps its own state, accumulators and metric in registers; the per-node
+// quantities its line partners need (primitive half-values, fluxes, metric rows) are
+// staged once in shared memory.  The surface term is evaluated by the thread that
+// owns the face node, face by face in Raven's order (x-, x+, y-, y+, z-, z+), so no
+// atomics or extra barriers are needed and corner nodes accumulate in the same order
+// as surfaceterm! (src/balancelaws/dgsem.jl:756-782).  The neighbour's trace is read
+// straight from the previous stage's state (ping-pong buffers: q_in is never written).
+//
+// Reference kernels restated: volumeterm! (dgsem.jl:257-348), esvolumeterm_dir!
+// (dgsem.jl:514-608), surfaceterm! (dgsem.jl:733-784), the LSRK stage broadcasts
+// (odesolvers.jl:55-57); fluxes from balancelaws/euler.jl:34-68,150-216,
+// balancelaws/advection.jl:18-19 and numericalfluxes.jl:9-50.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "rb200_internal.h"
+
+namespace rb200 {
+
+template <int N, int D>
+struct IPow {
+    static constexpr int v = N * IPow<N, D - 1>::v;
+};
+template <int N>
+struct IPow<N, 0> {
+    static constexpr int v = 1;
+};
+
+template <int DIM, int NQ>
+struct Shape {
+    static constexpr int NP = IPow<NQ, DIM>::v;
+    static constexpr int NFP = IPow<NQ, DIM - 1>::v;
+    static constexpr int NF = 2 * DIM;
+    static constexpr int EPB = NP >= 256 ? 1 : 256 / NP;  // elements per CTA
+    static constexpr int THREADS = EPB * NP;
+};
+
+template <int COMBO, int DIM>
+struct CSize {
+    static constexpr bool ADV = (COMBO == ADV_WEAK || COMBO == ADV_FDC);
+    static constexpr int NS = ADV ? 1 : DIM + 2;
+    // per-node values staged in shared memory for the line partners
+    static constexpr int NAUX = COMBO == ADV_WEAK   ? DIM              // l_F[dir]
+                                : COMBO == ADV_FDC  ? 1                // q/2
+                                : COMBO == EUL_WEAK ? DIM * (DIM + 2)  // l_F[dir][s]
+                                : COMBO == EUL_FDC  ? DIM * (DIM + 2)  // F[d][s]/2
+                                : COMBO == EUL_KG   ? DIM + 3          // rho/2, u/2, e/2, p/2
+                                                    : DIM + 3;         // EC: rho, u, b, |u|^2
+};
+
+template <int DIM, int NQ, int COMBO, int GEOM, typename T>
+struct KernelCfg {
+    using S = Shape<DIM, NQ>;
+    using C = CSize<COMBO, DIM>;
+    static constexpr int NLG = GEOM == GEOM_AFFINE ? DIM : DIM * DIM;
+    static constexpr size_t smem = (size_t)S::EPB * (C::NAUX + NLG) * S::NP * sizeof(T);
+};
+
+// Products and differences that must not be contracted into an FMA (they make the
+// diagonal pair term cancel exactly).
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double dev_log(double x) { return log(x); }
+__device__ __forceinline__ float dev_log(float x) { return logf(x); }
+__device__ __forceinline__ double dev_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float dev_sqrt(float x) { return sqrtf(x); }
+
+// logavg (numericalfluxes.jl:9-22)
+template <typename T>
+__device__ __forceinline__ T logavg(T a, T b) {
+    const T zeta = a / b;
+    const T f = (zeta - T(1)) / (zeta + T(1));
+    const T u = f * f;
+    const T eps = sizeof(T) == 8 ? T(2.220446049250313e-16) : T(1.1920929e-07f);
+    T F;
+    if (u < eps) {
+        F = fma(u, fma(u, fma(u, fma(u, T(1) / T(9), T(1) / T(7)), T(1) / T(5)), T(1) / T(3)), T(1));
+    } else {
+        F = dev_log(zeta) / (T(2) * f);
+    }
+    return (a + b) / (T(2) * F);
+}
+
+template <int DIM, int NQ, int COMBO, int GEOM, typename T>
+__global__ void __launch_bounds__(Shape<DIM, NQ>::THREADS, 1)
+    stage_kernel(const __grid_constant__ StageArgs A) {
+    using S = Shape<DIM, NQ>;
+    using C = CSize<COMBO, DIM>;
+    using K = KernelCfg<DIM, NQ, COMBO, GEOM, T>;
+    constexpr int NP = S::NP, NFP = S::NFP, NF = S::NF, EPB = S::EPB;
+    constexpr int NS = C::NS, NAUX = C::NAUX, NLG = K::NLG;
+    constexpr bool AFF = GEOM == GEOM_AFFINE;
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* s_aux = reinterpret_cast<T*>(smem_raw);
+    T* s_lg = s_aux + EPB * NAUX * NP;
+
+    const int tid = threadIdx.x;
+    const int el = tid / NP;
+    const int n = tid - el * NP;
+    const int64_t e = (int64_t)blockIdx.x * EPB + el;
+    const bool active = e < A.E;
+    int id[3];
+    id[0] = n % NQ;
+    id[1] = DIM > 1 ? (n / NQ) % NQ : 0;
+    id[2] = DIM > 2 ? n / (NQ * NQ) : 0;
+    T* aux = s_aux + el * NAUX * NP;
+    T* lgs = s_lg + el * NLG * NP;
+
+    double qd[NS];
+    T q[NS];
+    T lg[NLG];
+    T own[NAUX > 0 ? NAUX : 1];
+    double mji = 0.0, J = 0.0, wJ = 0.0;
+    double drdx[3] = {0.0, 0.0, 0.0};
+
+    if (active) {
+        const double* qe = A.q_in + (size_t)e * NS * NP;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            qd[s] = __ldg(qe + s * NP + n);
+            q[s] = (T)qd[s];
+        }
+        if constexpr (AFF) {
+            const double* eg = A.elem_geo + 4 * e;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) drdx[d] = __ldg(eg + d);
+            J = __ldg(eg + 3);
+            // wJ = wr[i]*ws[j]*wt[k]*J (lobattocells.jl:3231), MJI = 1 ./ MJ (dgsem.jl:56)
+            wJ = A.w[id[0]];
+#pragma unroll
+            for (int d = 1; d < DIM; ++d) wJ = wJ * A.w[id[d]];
+            wJ = wJ * J;
+            mji = 1.0 / wJ;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) lg[d] = (T)(wJ * drdx[d]);
+        } else {
+            const double* vg = A.vgeo + (size_t)e * (DIM * DIM + 1) * NP;
+#pragma unroll
+            for (int c = 0; c < DIM * DIM; ++c) lg[c] = (T)__ldg(vg + c * NP + n);
+            mji = __ldg(vg + DIM * DIM * NP + n);
+        }
+#pragma unroll
+        for (int c = 0; c < NLG; ++c) lgs[c * NP + n] = lg[c];
+
+        // ---- per-node values for the partners ----
+        if constexpr (COMBO == ADV_WEAK) {
+#pragma unroll
+            for (int dir = 0; dir < DIM; ++dir) {
+                T v;
+                if constexpr (AFF) {
+                    // l_F = (dRdX[dir,dir] * f[dir]) * MJ  (dgsem.jl:299-308)
+                    v = ((T)drdx[dir] * ((T)A.adv[dir] * q[0])) * (T)wJ;
+                } else {
+                    T acc = T(0);
+#pragma unroll
+                    for (int dd = 0; dd < DIM; ++dd) acc += lg[dir * DIM + dd] * ((T)A.adv[dd] * q[0]);
+                    v = acc;
+                }
+                own[dir] = v;
+            }
+        } else if constexpr (COMBO == ADV_FDC) {
+            own[0] = q[0] * T(0.5);
+        } else {
+            const T rho = q[0];
+            const T rhoe = q[DIM + 1];
+            T u[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) u[d] = q[1 + d] / rho;
+            T rr = q[1] * q[1];
+#pragma unroll
+            for (int d = 1; d < DIM; ++d) rr = rr + q[1 + d] * q[1 + d];
+            const T gm1 = (T)(A.gamma - 1.0);
+            const T p = gm1 * (rhoe - rr / (T(2) * rho));
+            if constexpr (COMBO == EUL_KG) {
+                own[0] = rho * T(0.5);
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) own[1 + d] = u[d] * T(0.5);
+                own[DIM + 1] = (rhoe / rho) * T(0.5);
+                own[DIM + 2] = p * T(0.5);
+            } else if constexpr (COMBO == EUL_EC) {
+                own[0] = rho;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) own[1 + d] = u[d];
+                own[DIM + 1] = rho / (T(2) * p);
+                T uu = u[0] * u[0];
+#pragma unroll
+                for (int d = 1; d < DIM; ++d) uu = uu + u[d] * u[d];
+                own[DIM + 2] = uu;
+            } else {
+                // physical flux F[d][s] (euler.jl:50-61)
+                T F[DIM][NS];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    F[d][0] = q[1 + d];
+#pragma unroll
+                    for (int b = 0; b < DIM; ++b) F[d][1 + b] = (d == b) ? q[1 + d] * u[b] + p : q[1 + d] * u[b];
+                    F[d][DIM + 1] = u[d] * (rhoe + p);
+                }
+                if constexpr (COMBO == EUL_FDC) {
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d)
+#pragma unroll
+                        for (int s = 0; s < NS; ++s) own[d * NS + s] = F[d][s] * T(0.5);
+                } else {  // EUL_WEAK: l_F[dir][s] = MJ * sum_dd dRdX[dir,dd] F[dd,s]
+#pragma unroll
+                    for (int dir = 0; dir < DIM; ++dir)
+#pragma unroll
+                        for (int s = 0; s < NS; ++s) {
+                            if constexpr (AFF) {
+                                own[dir * NS + s] = ((T)drdx[dir] * F[dir][s]) * (T)wJ;
+                            } else {
+                                T acc = T(0);
+#pragma unroll
+                                for (int dd = 0; dd < DIM; ++dd) acc += lg[dir * DIM + dd] * F[dd][s];
+                                own[dir * NS + s] = acc;
+                            }
+                        }
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < NAUX; ++k) aux[k * NP + n] = own[k];
+    }
+    __syncthreads();
+    if (!active) return;
+
+    // ------------------------------------------------------------------ volume term
+    T acc[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) acc[s] = T(0);
+
+#pragma unroll
+    for (int dir = 0; dir < DIM; ++dir) {
+        const int stride = dir == 0 ? 1 : (dir == 1 ? NQ : NQ * NQ);
+        const int idd = id[dir];
+        const int base = n - idd * stride;
+#pragma unroll
+        for (int a = 0; a < NQ; ++a) {
+            const int na = base + a * stride;
+            const T Dai = (T)A.D[a + NQ * idd];  // D[a, id]
+            if constexpr (COMBO == ADV_WEAK) {
+                acc[0] += Dai * aux[dir * NP + na];
+            } else if constexpr (COMBO == EUL_WEAK) {
+#pragma unroll
+                for (int s = 0; s < NS; ++s) acc[s] += Dai * aux[(dir * NS + s) * NP + na];
+            } else {
+                const T Dia = (T)A.D[idd + NQ * a];  // D[id, a]
+                // metric combination G_d = D[a,id] l_g[a][d] - D[id,a] l_g[i][d]
+                T G[DIM];
+                if constexpr (AFF) {
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) G[d] = T(0);
+                    G[dir] = sub_rn(mul_rn(Dai, lgs[dir * NP + na]), mul_rn(Dia, lg[dir]));
+                } else {
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d)
+                        G[d] = sub_rn(mul_rn(Dai, lgs[(dir * DIM + d) * NP + na]), mul_rn(Dia, lg[dir * DIM + d]));
+                }
+                if constexpr (COMBO == ADV_FDC) {
+                    T aG = (T)A.adv[0] * G[0];
+#pragma unroll
+                    for (int d = 1; d < DIM; ++d) aG += (T)A.adv[d] * G[d];
+                    acc[0] += (own[0] + aux[na]) * aG;
+                } else if constexpr (COMBO == EUL_FDC) {
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) {
+                        T v = T(0);
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) v += (own[d * NS + s] + aux[(d * NS + s) * NP + na]) * G[d];
+                        acc[s] += v;
+                    }
+                } else if constexpr (COMBO == EUL_KG) {
+                    const T rb = own[0] + aux[na];
+                    T ub[DIM];
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) ub[d] = own[1 + d] + aux[(1 + d) * NP + na];
+                    const T eb = own[DIM + 1] + aux[(DIM + 1) * NP + na];
+                    const T pb = own[DIM + 2] + aux[(DIM + 2) * NP + na];
+                    T un;
+                    if constexpr (AFF) {
+                        un = ub[dir] * G[dir];
+                    } else {
+                        un = ub[0] * G[0];
+#pragma unroll
+                        for (int d = 1; d < DIM; ++d) un += ub[d] * G[d];
+                    }
+                    const T f1 = rb * un;
+                    acc[0] += f1;
+#pragma unroll
+                    for (int b = 0; b < DIM; ++b) {
+                        if (AFF && b != dir) acc[1 + b] += f1 * ub[b];
+                        else acc[1 + b] += f1 * ub[b] + pb * G[b];
+                    }
+                    acc[DIM + 1] += un * (rb * eb + pb);
+                } else {  // EUL_EC
+                    const T r2 = aux[na];
+                    T u2[DIM], ua[DIM];
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) {
+                        u2[d] = aux[(1 + d) * NP + na];
+                        ua[d] = (own[1 + d] + u2[d]) * T(0.5);
+                    }
+                    const T b2 = aux[(DIM + 1) * NP + na];
+                    const T uu2 = aux[(DIM + 2) * NP + na];
+                    const T ra = (own[0] + r2) * T(0.5);
+                    const T ba = (own[DIM + 1] + b2) * T(0.5);
+                    const T u2a = (own[DIM + 2] + uu2) * T(0.5);
+                    const T rlog = logavg(own[0], r2);
+                    const T blog = logavg(own[DIM + 1], b2);
+                    const T pt = ra / (T(2) * ba);
+                    const T c = T(1) / ((T(2) * (T)(A.gamma - 1.0)) * blog) - u2a * T(0.5);
+                    T un = ua[0] * G[0], uaa = ua[0] * ua[0];
+#pragma unroll
+                    for (int d = 1; d < DIM; ++d) {
+                        un += ua[d] * G[d];
+                        uaa += ua[d] * ua[d];
+                    }
+                    const T f0 = rlog * un;
+                    acc[0] += f0;
+#pragma unroll
+                    for (int b = 0; b < DIM; ++b) acc[1 + b] += f0 * ua[b] + pt * G[b];
+                    acc[DIM + 1] += un * (c * rlog + rlog * uaa + pt);
+                }
+            }
+        }
+    }
+
+    // ------------------------------------------------------------- combine with dq
+    const T mjiT = (T)mji;
+    const bool stage = A.mode >= MODE_STAGE;
+    const size_t node0 = (size_t)e * NS * NP + n;
+    T t[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        T v = acc[s] * mjiT;
+        if (A.mode == MODE_STAGE) {
+            T old;
+            if (sizeof(T) == 4) old = (T) reinterpret_cast<const float*>(A.dq)[node0 + s * NP];
+            else old = (T) reinterpret_cast<const double*>(A.dq)[node0 + s * NP];
+            v = (T)A.rka * old + v;
+        } else if (A.mode == MODE_TENDENCY_INC) {
+            v = (T)(reinterpret_cast<const double*>(A.dq)[node0 + s * NP] + (double)v);
+        }
+        t[s] = v;
+    }
+
+    // ---------------------------------------------------------------- surface term
+#pragma unroll
+    for (int dir = 0; dir < DIM; ++dir) {
+        const int idd = id[dir];
+        if (idd != 0 && idd != NQ - 1) continue;
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            if ((side == 0 && idd != 0) || (side == 1 && idd != NQ - 1)) continue;
+            const int f = 2 * dir + side;
+            const int stride = dir == 0 ? 1 : (dir == 1 ? NQ : NQ * NQ);
+            const int ne = __ldg(A.nbr + (size_t)NF * e + f);
+            T qp[NS];
+            if (ne >= 0) {
+                const int nn = n + (side == 0 ? (NQ - 1) * stride : -(NQ - 1) * stride);
+                const double* qn = A.q_in + (size_t)ne * NS * NP + nn;
+#pragma unroll
+                for (int s = 0; s < NS; ++s) qp[s] = (T)__ldg(qn + s * NP);
+            } else {
+#pragma unroll
+                for (int s = 0; s < NS; ++s) qp[s] = q[s];  // default boundarystate (balancelaw.jl:77)
+            }
+            // in-face index of this node (column-major over the face dims)
+            int j;
+            if (DIM == 2) j = (dir == 0) ? id[1] : id[0];
+            else j = (dir == 0) ? id[1] + NQ * id[2] : (dir == 1 ? id[0] + NQ * id[2] : id[0] + NQ * id[1]);
+            T nv[DIM];
+            double wsJ;
+            if constexpr (AFF) {
+                // hexsurfacemetrics! on an unwarped brick (lobattocells.jl:3278-3291)
+                const double sJ = fabs(J * drdx[dir]);
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) nv[d] = T(0);
+                nv[dir] = side == 0 ? T(-1) : T(1);
+                if (DIM == 2) wsJ = sJ * A.w[dir == 0 ? id[1] : id[0]];
+                else {
+                    const int i1 = dir == 0 ? id[1] : id[0];
+                    const int i2 = dir == 2 ? id[1] : id[2];
+                    wsJ = (sJ * A.w[i1]) * A.w[i2];
+                }
+            } else {
+                const double* sg = A.sgeo + ((size_t)e * NF * NFP + (size_t)f * NFP + j) * (DIM + 1);
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) nv[d] = (T)__ldg(sg + d);
+                wsJ = __ldg(sg + DIM);
+            }
+            T nf[NS];
+            if constexpr (C::ADV) {
+                T an;
+                if constexpr (AFF) an = (T)A.adv[dir] * nv[dir];
+                else {
+                    an = (T)A.adv[0] * nv[0];
+#pragma unroll
+                    for (int d = 1; d < DIM; ++d) an += (T)A.adv[d] * nv[d];
+                }
+                const T fc = (an * q[0] + an * qp[0]) * T(0.5);
+                nf[0] = A.surface_rusanov ? fc - (fabs(an) * (qp[0] - q[0])) * T(0.5) : fc;
+            } else {
+                // Rusanov: central flux of the physical fluxes, minus the max wave speed jump
+                // (numericalfluxes.jl:44-50, euler.jl:50-68)
+                const T gm1 = (T)(A.gamma - 1.0);
+                T Fn[2][NS], ws[2];
+#pragma unroll
+                for (int side2 = 0; side2 < 2; ++side2) {
+                    const T* qq = side2 == 0 ? q : qp;
+                    const T rho = qq[0], rhoe = qq[DIM + 1];
+                    T u[DIM];
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) u[d] = qq[1 + d] / rho;
+                    T rr = qq[1] * qq[1];
+#pragma unroll
+                    for (int d = 1; d < DIM; ++d) rr = rr + qq[1 + d] * qq[1 + d];
+                    const T p = gm1 * (rhoe - rr / (T(2) * rho));
+                    T un, mn;
+                    if constexpr (AFF) {
+                        un = u[dir] * nv[dir];
+                        mn = qq[1 + dir] * nv[dir];
+                    } else {
+                        un = u[0] * nv[0];
+                        mn = qq[1] * nv[0];
+#pragma unroll
+                        for (int d = 1; d < DIM; ++d) {
+                            un += u[d] * nv[d];
+                            mn += qq[1 + d] * nv[d];
+                        }
+                    }
+                    Fn[side2][0] = mn;
+#pragma unroll
+                    for (int b = 0; b < DIM; ++b) Fn[side2][1 + b] = mn * u[b] + p * nv[b];
+                    Fn[side2][DIM + 1] = un * (rhoe + p);
+                    ws[side2] = fabs(un) + dev_sqrt((T)A.gamma * p / rho);
+                }
+                const T mx = fmax(ws[0], ws[1]);
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    const T fc = (Fn[0][s] + Fn[1][s]) * T(0.5);
+                    nf[s] = A.surface_rusanov ? fc - (mx * (qp[s] - q[s])) * T(0.5) : fc;
+                }
+            }
+            const T wsJT = (T)wsJ;
+#pragma unroll
+            for (int s = 0; s < NS; ++s) t[s] = t[s] - (wsJT * nf[s]) * mjiT;
+        }
+    }
+
+    // ----------------------------------------------------------------- write back
+    if (stage) {
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            if (sizeof(T) == 4) reinterpret_cast<float*>(A.dq)[node0 + s * NP] = (float)t[s];
+            else reinterpret_cast<double*>(A.dq)[node0 + s * NP] = (double)t[s];
+            A.q_out[node0 + s * NP] = qd[s] + A.rkb_dt * (double)t[s];
+        }
+    } else {
+#pragma unroll
+        for (int s = 0; s < NS; ++s) reinterpret_cast<double*>(A.dq)[node0 + s * NP] = (double)t[s];
+    }
+}
+
+template <int DIM, int NQ, int COMBO, int GEOM, typename T>
+cudaError_t launch_one(const StageArgs& a, cudaStream_t st) {
+    using S = Shape<DIM, NQ>;
+    using K = KernelCfg<DIM, NQ, COMBO, GEOM, T>;
+    auto kern = stage_kernel<DIM, NQ, COMBO, GEOM, T>;
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::smem);
+        if (err != cudaSuccess) return err;
+        configured = true;
+    }
+    const int64_t blocks = (a.E + S::EPB - 1) / S::EPB;
+    if (blocks <= 0) return cudaSuccess;
+    kern<<<(unsigned)blocks, S::THREADS, K::smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace rb200
