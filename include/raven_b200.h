@@ -116,9 +116,19 @@ rb200_status rb200_integrals(rb200_handle* h, const double* q, double* out, void
  * neighbour table the kernels use, for bit-exact comparison with facemaps(grid).vmapP. */
 rb200_status rb200_face_vmapP(rb200_handle* h, int64_t* vmapP_out, void* stream);
 
+/* Kernel selection: 0 = automatic (the persistent TMA-pipelined kernel for 3-D, nq = 8,
+ * unwarped-brick flux differencing when the state pointers are 16-byte aligned, the
+ * generic stage kernel otherwise), 1 = generic stage kernel only. */
+rb200_status rb200_set_kernel_path(rb200_handle* h, int32_t path);
+
+/* Synchronizes `stream` and returns RB200_ERR_TIMEOUT if a kernel of this handle gave
+ * up a bounded wait since the handle was created, RB200_OK otherwise. */
+rb200_status rb200_sync_status(rb200_handle* h, void* stream);
+
 /* Handle properties: info[0]=dim, [1]=nq, [2]=Ns, [3]=E, [4]=geometry kind
  * (0 affine brick, 1 curved), [5]=precision, [6]=kernel launches per LSRK step,
- * [7]=algorithmic HBM bytes per node per stage. */
+ * [7]=algorithmic HBM bytes per node per stage, [8]=CTAs of the pipelined kernel
+ * (0 when the handle's configuration does not use it). */
 rb200_status rb200_get_info(const rb200_handle* h, int64_t* info, int32_t n);
 
 /* Last error message of a handle (empty if none); static text for NULL. */

@@ -287,10 +287,19 @@ class DGSEM:
                 L.rb200_destroy(h)
             self._h = None
             raise RB200Error(st, msg)
-        info = (ctypes.c_int64 * 8)()
-        L.rb200_get_info(h, info, 8)
+        info = (ctypes.c_int64 * 9)()
+        L.rb200_get_info(h, info, 9)
         self.info = list(info)
         self.geometry = "affine" if info[4] == 0 else "curved"
+        self.pipelined_ctas = int(info[8])
+
+    def set_kernel_path(self, path):
+        """'auto' (pipelined kernel where eligible) or 'generic' (generic stage kernel only)."""
+        _lib.check(_lib.lib().rb200_set_kernel_path(self._h, {"auto": 0, "generic": 1}[path]), self._h)
+
+    def sync_status(self):
+        """Synchronizes and raises RB200Error(TIMEOUT) if a kernel gave up a bounded wait."""
+        _lib.check(_lib.lib().rb200_sync_status(self._h, _stream_ptr()), self._h)
 
     def __del__(self):
         h = getattr(self, "_h", None)

@@ -35,6 +35,8 @@ EXPORTED = [
     "rb200_integrals",
     "rb200_face_vmapP",
     "rb200_get_info",
+    "rb200_set_kernel_path",
+    "rb200_sync_status",
     "rb200_last_error",
     "rb200_status_string",
 ]
@@ -94,6 +96,8 @@ def lib():
     L.rb200_integrals.argtypes = [P, P, P, P]
     L.rb200_face_vmapP.argtypes = [P, P, P]
     L.rb200_get_info.argtypes = [P, P, I32]
+    L.rb200_set_kernel_path.argtypes = [P, I32]
+    L.rb200_sync_status.argtypes = [P, P]
     L.rb200_last_error.argtypes = [P]
     L.rb200_last_error.restype = ctypes.c_char_p
     L.rb200_status_string.argtypes = [ctypes.c_int]

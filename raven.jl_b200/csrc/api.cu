@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/raven_b200.h"
+#include "pipelined_kernel.cuh"
 #include "rb200_internal.h"
 
 using namespace rb200;
@@ -42,7 +43,11 @@ struct rb200_handle {
     double* d_hdq = nullptr;  // its LSRK register
     double* d_partial = nullptr;
     double* d_sums = nullptr;
+    int32_t* d_status = nullptr;  // bounded-wait error word written by the kernels
     int red_blocks = 0;
+    int kernel_path = 0;          // 0 automatic, 1 generic stage kernel only
+    int pipe_grid = 0;            // CTAs of the pipelined kernel (0: not eligible)
+    double pipe_S[64] = {0};      // D[a,id] w[a] / w[id] - D[id,a]
     std::string err;
 };
 
@@ -99,14 +104,45 @@ rb200_status dev_alloc(rb200_handle* h, T** p, size_t count) {
 }
 
 void free_all(rb200_handle* h) {
-    void* ptrs[] = {h->d_elem_geo, h->d_vgeo, h->d_sgeo, h->d_w, h->d_nbr, h->d_qtmp,
-                    h->d_dq32,     h->d_hq,   h->d_hdq,  h->d_partial, h->d_sums};
+    void* ptrs[] = {h->d_elem_geo, h->d_vgeo, h->d_sgeo,    h->d_w,    h->d_nbr,   h->d_qtmp,
+                    h->d_dq32,     h->d_hq,   h->d_hdq,     h->d_partial, h->d_sums, h->d_status};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     h->d_elem_geo = h->d_vgeo = h->d_sgeo = h->d_w = h->d_qtmp = h->d_hq = h->d_hdq = h->d_partial = h->d_sums =
         nullptr;
     h->d_nbr = nullptr;
     h->d_dq32 = nullptr;
+    h->d_status = nullptr;
+}
+
+bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+// One stage (or tendency) launch: the pipelined kernel when the configuration and the
+// pointers allow it, the generic stage kernel otherwise.
+cudaError_t launch_any(rb200_handle* h, const StageArgs& a, cudaStream_t st) {
+    const bool stage_mode = a.mode >= MODE_STAGE;
+    const bool eligible = h->kernel_path == 0 && h->pipe_grid > 0 && aligned16(a.q_in) && aligned16(a.dq) &&
+                          (!stage_mode || aligned16(a.q_out)) &&
+                          (h->prec == RB200_PRECISION_FP64 || stage_mode);
+    if (!eligible) return launch_stage(h->dim, h->nq, h->combo, h->geom, h->prec, a, st);
+    PipeArgs p;
+    std::memset(&p, 0, sizeof(p));
+    p.q_in = a.q_in;
+    p.q_out = a.q_out;
+    p.dq = a.dq;
+    p.elem_geo = a.elem_geo;
+    p.nbr = a.nbr;
+    p.status = h->d_status;
+    p.E = a.E;
+    p.mode = a.mode;
+    p.surface_rusanov = a.surface_rusanov;
+    p.rka = a.rka;
+    p.rkb_dt = a.rkb_dt;
+    p.gamma = a.gamma;
+    std::memcpy(p.S, h->pipe_S, sizeof(p.S));
+    std::memcpy(p.w, h->w, sizeof(p.w));
+    const int grid = (int)std::min<int64_t>(h->pipe_grid, a.E);
+    return launch_pipelined(h->combo, h->prec, p, grid, st);
 }
 
 StageArgs base_args(const rb200_handle* h) {
@@ -142,7 +178,7 @@ rb200_status run_steps(rb200_handle* h, double* q, void* dq, double dt, int32_t 
             a.mode = RKA[stg] == 0.0 ? MODE_STAGE_FIRST : MODE_STAGE;
             a.rka = RKA[stg];
             a.rkb_dt = RKB[stg] * dt;
-            cudaError_t e = launch_stage(h->dim, h->nq, h->combo, h->geom, h->prec, a, st);
+            cudaError_t e = launch_any(h, a, st);
             if (e != cudaSuccess) return cuda_fail(h, e, "stage kernel launch");
             double* t = cur;
             cur = oth;
@@ -359,6 +395,20 @@ rb200_status rb200_create(const rb200_desc* d, rb200_handle** out) {
         ce = cudaMemset(h->d_dq32, 0, n * sizeof(float));
         if (ce != cudaSuccess) return bail(cuda_fail(h, ce, "memset"));
     }
+    if ((st = dev_alloc(h, &h->d_status, 1)) != RB200_OK) return bail(st);
+    ce = cudaMemset(h->d_status, 0, sizeof(int32_t));
+    if (ce != cudaSuccess) return bail(cuda_fail(h, ce, "memset"));
+    if (dim == 3 && nq == 8 && affine && (h->combo == EUL_KG || h->combo == EUL_EC)) {
+        for (int a = 0; a < 8; ++a)
+            for (int id = 0; id < 8; ++id)
+                h->pipe_S[a * 8 + id] = h->D[a + 8 * id] * (h->w[a] / h->w[id]) - h->D[id + 8 * a];
+        int dev = 0, nsm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        const int per_sm = pipelined_blocks_per_sm(h->combo, h->prec);
+        h->pipe_grid = per_sm > 0 ? per_sm * nsm : 0;
+        cudaGetLastError();
+    }
     h->red_blocks = 296;
     if ((st = dev_alloc(h, &h->d_partial, (size_t)h->red_blocks * 2 * h->ns)) != RB200_OK) return bail(st);
     if ((st = dev_alloc(h, &h->d_sums, (size_t)2 * h->ns)) != RB200_OK) return bail(st);
@@ -389,7 +439,7 @@ rb200_status rb200_tendency(rb200_handle* h, double* dq, const double* q, double
     a.q_in = q;
     a.dq = dq;
     a.mode = increment ? MODE_TENDENCY_INC : MODE_TENDENCY_SET;
-    cudaError_t e = launch_stage(h->dim, h->nq, h->combo, h->geom, h->prec, a, (cudaStream_t)stream);
+    cudaError_t e = launch_any(h, a, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "tendency kernel launch");
     return RB200_OK;
 }
@@ -471,14 +521,31 @@ rb200_status rb200_face_vmapP(rb200_handle* h, int64_t* vmapP_out, void* stream)
     return RB200_OK;
 }
 
+rb200_status rb200_set_kernel_path(rb200_handle* h, int32_t path) {
+    if (!h || path < 0 || path > 1) return RB200_ERR_BAD_ARG;
+    h->kernel_path = path;
+    return RB200_OK;
+}
+
+rb200_status rb200_sync_status(rb200_handle* h, void* stream) {
+    if (!h) return RB200_ERR_BAD_ARG;
+    DeviceGuard guard(h->device);
+    int32_t v = 0;
+    cudaError_t e = cudaMemcpyAsync(&v, h->d_status, sizeof(v), cudaMemcpyDeviceToHost, (cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "status readback");
+    if (v != 0) return fail(h, (rb200_status)v, "a kernel wait exceeded its iteration limit");
+    return RB200_OK;
+}
+
 rb200_status rb200_get_info(const rb200_handle* h, int64_t* info, int32_t n) {
     if (!h || !info) return RB200_ERR_BAD_ARG;
     const int64_t bytes_q = 8, bytes_dq = h->prec == RB200_PRECISION_FP32_BULK ? 4 : 8;
     int64_t per_node = h->ns * (2 * bytes_q + 2 * bytes_dq);
     if (h->geom == GEOM_CURVED)
         per_node += (h->dim * h->dim + 1) * 8 + (int64_t)h->nf * h->nfp * (h->dim + 1) * 8 / h->np;
-    const int64_t v[8] = {h->dim, h->nq, h->ns, h->E, h->geom, h->prec, 5, per_node};
-    for (int i = 0; i < n && i < 8; ++i) info[i] = v[i];
+    const int64_t v[9] = {h->dim, h->nq, h->ns, h->E, h->geom, h->prec, 5, per_node, h->pipe_grid};
+    for (int i = 0; i < n && i < 9; ++i) info[i] = v[i];
     return RB200_OK;
 }
 

@@ -1,0 +1,44 @@
+// Instantiations and launch helpers of the pipelined 3-D Nq = 8 stage kernel.
+#include "pipelined_kernel.cuh"
+
+namespace rb200 {
+
+template <int COMBO, typename T>
+static cudaError_t launch_p(const PipeArgs& a, int grid, cudaStream_t s) {
+    auto kern = pipelined_stage_kernel<COMBO, T>;
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)sizeof(pipe::Smem<T>));
+        if (err != cudaSuccess) return err;
+        configured = true;
+    }
+    kern<<<grid, pipe::NT, sizeof(pipe::Smem<T>), s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pipelined(int combo, int fp32, const PipeArgs& a, int grid, cudaStream_t s) {
+    if (combo == EUL_KG) return fp32 ? launch_p<EUL_KG, float>(a, grid, s) : launch_p<EUL_KG, double>(a, grid, s);
+    if (combo == EUL_EC) return fp32 ? launch_p<EUL_EC, float>(a, grid, s) : launch_p<EUL_EC, double>(a, grid, s);
+    return cudaErrorInvalidValue;
+}
+
+template <int COMBO, typename T>
+static int occupancy_p() {
+    auto kern = pipelined_stage_kernel<COMBO, T>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(pipe::Smem<T>)) !=
+        cudaSuccess)
+        return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, pipe::NT, sizeof(pipe::Smem<T>)) != cudaSuccess)
+        return 0;
+    return n;
+}
+
+int pipelined_blocks_per_sm(int combo, int fp32) {
+    if (combo == EUL_KG) return fp32 ? occupancy_p<EUL_KG, float>() : occupancy_p<EUL_KG, double>();
+    if (combo == EUL_EC) return fp32 ? occupancy_p<EUL_EC, float>() : occupancy_p<EUL_EC, double>();
+    return 0;
+}
+
+}  // namespace rb200

@@ -31,13 +31,14 @@ enum Mode : int {
 };
 
 constexpr int kMaxNq = 8;
+constexpr int32_t kStatusTimeout = 5;  // RB200_ERR_TIMEOUT
 
 struct StageArgs {
     const double* q_in;   // (Np, Ns, E)
     double* q_out;        // stage modes only (may alias nothing that q_in aliases)
     void* dq;             // double* (FP64) or float* (FP32 bulk), read-modify-write in place
     const double* elem_geo;  // affine: (4, E): drdx, dsdy, dtdz, J
-    const double* vgeo;      // curved: (Np, dim*dim+1, E): wJ*dRdX[dir,d] (dir-major), MJI
+    const double* vgeo;      // curved: (Np, dim*dim+2, E): wJ*dRdX[dir,d] (dir-major), MJI, MJ
     const double* sgeo;      // curved: (dim+1, 2*dim*Nfp, E): n, wsJ
     const int32_t* nbr;      // (2*dim, E): neighbour element across each face, -1 = boundary
     int64_t E;
@@ -55,6 +56,11 @@ struct StageArgs {
 cudaError_t launch_stage(int dim, int nq, int combo, int geom, int fp32, const StageArgs& a, cudaStream_t s);
 // Dynamic shared memory the kernel needs (bytes) and threads per block; 0 if not built.
 size_t stage_smem_bytes(int dim, int nq, int combo, int geom, int fp32);
+
+struct PipeArgs;  // pipelined_kernel.cuh
+// Persistent TMA-pipelined kernel for 3-D Nq = 8 affine flux differencing (KG, EC).
+cudaError_t launch_pipelined(int combo, int fp32, const PipeArgs& a, int grid, cudaStream_t s);
+int pipelined_blocks_per_sm(int combo, int fp32);
 
 // Reductions and face-map expansion (reduce.cu).
 cudaError_t launch_weighted_sums(const double* q, const double* elem_geo, const double* vgeo, const double* w,

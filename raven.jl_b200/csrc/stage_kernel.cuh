@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(Shape<DIM, NQ>::THREADS, 1)
 #pragma unroll
             for (int d = 0; d < DIM; ++d) lg[d] = (T)(wJ * drdx[d]);
         } else {
-            const double* vg = A.vgeo + (size_t)e * (DIM * DIM + 1) * NP;
+            const double* vg = A.vgeo + (size_t)e * (DIM * DIM + 2) * NP;  // fields: wJ*dRdX rows, MJI, MJ
 #pragma unroll
             for (int c = 0; c < DIM * DIM; ++c) lg[c] = (T)__ldg(vg + c * NP + n);
             mji = __ldg(vg + DIM * DIM * NP + n);
