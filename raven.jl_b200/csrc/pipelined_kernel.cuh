@@ -88,12 +88,21 @@ __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier
 
 template <typename T>
 struct Smem {
-    double q[2][NS][NP];     // state of the element being computed / prefetched
-    T dq[2][NS][NP];         // LSRK register (FP64 or FP32)
-    T aux[NAUX][NPP];        // per-node values the line partners need
-    T S[3][NQ][NQ];          // S_dir[a][id] * drdx_dir of the current element
-    uint64_t bar[2];
+    double q[2][NS][NP];      // state: element being computed / element prefetched
+    T dq[NS][NP];             // LSRK register of the element being computed
+    T aux[NAUX][NPP];         // per-node values the line partners need
+    T sflux[NS][384];         // face-slot contributions (wsJ * nf) * MJI
+    T S[3][NQ][NQ];           // S_dir[a][id] * drdx_dir of the current element
+    uint64_t bar[3];          // q buffers 0/1, dq buffer
 };
+
+__device__ __forceinline__ bool bounded_wait(uint64_t* bar, uint32_t parity) {
+    long it = 0;
+    while (!mbar_try_wait(bar, parity)) {
+        if (++it > kWaitLimit) return false;
+    }
+    return true;
+}
 
 }  // namespace pipe
 
@@ -115,42 +124,36 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
     if (t == 0) {
         mbar_init(&sm.bar[0], 1);
         mbar_init(&sm.bar[1], 1);
+        mbar_init(&sm.bar[2], 1);
         fence_mbar_init();
     }
     __syncthreads();
 
-    auto issue = [&](int64_t e, int b) {
-        // only thread 0 calls this
-        mbar_expect_tx(&sm.bar[b], qbytes + (read_dq ? dqbytes : 0));
-        bulk_g2s(&sm.q[b][0][0], A.q_in + (size_t)e * NS * NP, qbytes, &sm.bar[b]);
-        if (read_dq) {
-            const char* src = reinterpret_cast<const char*>(A.dq) + (size_t)e * dqbytes;
-            bulk_g2s(&sm.dq[b][0][0], src, dqbytes, &sm.bar[b]);
-        }
-    };
-
     int64_t e = blockIdx.x;
-    if (t == 0 && e < A.E) issue(e, 0);
-    uint32_t phase[2] = {0, 0};
+    if (t == 0 && e < A.E) {
+        mbar_expect_tx(&sm.bar[0], qbytes);
+        bulk_g2s(&sm.q[0][0][0], A.q_in + (size_t)e * NS * NP, qbytes, &sm.bar[0]);
+    }
+    uint32_t qphase[2] = {0, 0}, dqphase = 0;
     int b = 0;
     for (; e < A.E; e += gridDim.x, b ^= 1) {
         const int64_t enext = e + gridDim.x;
-        if (t == 0 && enext < A.E) {
-            fence_proxy_async();
-            issue(enext, b ^ 1);
-        }
-        // ---- neighbour traces for this thread's face slots (global/L2), issued early
-        // slot s0 = t: faces 0..3 (x-, x+, y-, y+); slot s1 = 256 + t (t < 128): faces 4, 5
+        // ---- element geometry, scaled S table, neighbour traces (global/L2) issued early
         const double* eg = A.elem_geo + 4 * e;
         const double drdx[3] = {__ldg(eg), __ldg(eg + 1), __ldg(eg + 2)};
         const double J = __ldg(eg + 3);
+        if (t < 192) {
+            const int dir = t >> 6, a = (t >> 3) & 7, id = t & 7;
+            const double dd = dir == 0 ? drdx[0] : (dir == 1 ? drdx[1] : drdx[2]);
+            sm.S[dir][a][id] = (T)(A.S[a * 8 + id] * dd);
+        }
+        // face slots: s0 = t (faces x-, x+, y-, y+), s1 = 256 + t for t < 128 (z-, z+)
         T qp[2][NS];
-        int fslot[2], vnode[2];
+        int vnode[2] = {0, 0};
         bool open_face[2] = {false, false};  // false: boundary face, q+ = q- (balancelaw.jl:77)
 #pragma unroll
         for (int sl = 0; sl < 2; ++sl) {
             const int slot = sl == 0 ? t : 256 + t;
-            fslot[sl] = -1;
             if (slot >= 384) continue;
             const int f = slot >> 6, jf = slot & 63;
             const int dir = f >> 1, side = f & 1;
@@ -159,7 +162,6 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
             if (dir == 0) { vn = c + 8 * (j1 + 8 * j2); opp = (NQ - 1 - c) + 8 * (j1 + 8 * j2); }
             else if (dir == 1) { vn = j1 + 8 * (c + 8 * j2); opp = j1 + 8 * ((NQ - 1 - c) + 8 * j2); }
             else { vn = j1 + 8 * (j2 + 8 * c); opp = j1 + 8 * (j2 + 8 * (NQ - 1 - c)); }
-            fslot[sl] = f;
             vnode[sl] = vn;
             const int ne = __ldg(A.nbr + 6 * e + f);
             open_face[sl] = ne >= 0;
@@ -169,25 +171,12 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
                 for (int s = 0; s < NS; ++s) qp[sl][s] = (T)__ldg(qn + s * NP);
             }
         }
-        // per-element scaled S table
-        if (t < 192) {
-            const int dir = t >> 6, a = (t >> 3) & 7, id = t & 7;
-            const double dd = dir == 0 ? drdx[0] : (dir == 1 ? drdx[1] : drdx[2]);
-            sm.S[dir][a][id] = (T)(A.S[a * 8 + id] * dd);
+        // ---- this element's state
+        if (__syncthreads_or(!bounded_wait(&sm.bar[b], qphase[b]))) {
+            if (t == 0) atomicExch(A.status, kStatusTimeout);
+            return;
         }
-        // ---- wait for this element's q (and dq)
-        {
-            long it = 0;
-            bool ok = true;
-            while (!mbar_try_wait(&sm.bar[b], phase[b])) {
-                if (++it > kWaitLimit) { ok = false; break; }
-            }
-            if (__syncthreads_or(!ok)) {
-                if (t == 0) atomicExch(A.status, kStatusTimeout);
-                return;
-            }
-            phase[b] ^= 1;
-        }
+        qphase[b] ^= 1;
         // ---- per-node partner values
         T own[2][NAUX];
 #pragma unroll
@@ -195,9 +184,9 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
             const int n = h ? n1 : n0;
             const T rho = (T)sm.q[b][0][n];
             const T rinv = T(1) / rho;
-            const T u0 = (T)sm.q[b][1][n] * rinv, u1 = (T)sm.q[b][2][n] * rinv, u2 = (T)sm.q[b][3][n] * rinv;
-            const T rhoe = (T)sm.q[b][4][n];
             const T m0 = (T)sm.q[b][1][n], m1 = (T)sm.q[b][2][n], m2 = (T)sm.q[b][3][n];
+            const T u0 = m0 * rinv, u1 = m1 * rinv, u2 = m2 * rinv;
+            const T rhoe = (T)sm.q[b][4][n];
             const T p = gm1 * (rhoe - (m0 * m0 + m1 * m1 + m2 * m2) / (T(2) * rho));
             if constexpr (COMBO == EUL_KG) {
                 own[h][0] = rho * T(0.5);
@@ -217,7 +206,20 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
 #pragma unroll
             for (int c = 0; c < NAUX; ++c) sm.aux[c][PAD(n)] = own[h][c];
         }
-        __syncthreads();
+        __syncthreads();  // #1: aux and S ready; every thread is past the previous element
+        if (t == 0) {
+            // the other q buffer and the dq buffer were last read before barrier #1
+            fence_proxy_async();
+            if (enext < A.E) {
+                mbar_expect_tx(&sm.bar[b ^ 1], qbytes);
+                bulk_g2s(&sm.q[b ^ 1][0][0], A.q_in + (size_t)enext * NS * NP, qbytes, &sm.bar[b ^ 1]);
+            }
+            if (read_dq) {
+                mbar_expect_tx(&sm.bar[2], dqbytes);
+                bulk_g2s(&sm.dq[0][0], reinterpret_cast<const char*>(A.dq) + (size_t)e * dqbytes, dqbytes,
+                         &sm.bar[2]);
+            }
+        }
 
         // ---- volume term (ordered pairs along x, y, z)
         T acc[2][NS];
@@ -262,7 +264,7 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
 
 #pragma unroll
         for (int a = 0; a < NQ; ++a) {
-            // x partners (a, jj, k) and y partners (ii, a, k) of both nodes
+            const T sx = sm.S[0][a][ii], sy = sm.S[1][a][jj];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int kk = k0 + 4 * h;
@@ -270,13 +272,12 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
                 const int nx = a + 8 * (jj + 8 * kk);
 #pragma unroll
                 for (int c = 0; c < NAUX; ++c) pv[c] = sm.aux[c][PAD(nx)];
-                pair(acc[h], own[h], pv, sm.S[0][a][ii], 0);
+                pair(acc[h], own[h], pv, sx, 0);
                 const int ny = ii + 8 * (a + 8 * kk);
 #pragma unroll
                 for (int c = 0; c < NAUX; ++c) pv[c] = sm.aux[c][PAD(ny)];
-                pair(acc[h], own[h], pv, sm.S[1][a][jj], 1);
+                pair(acc[h], own[h], pv, sy, 1);
             }
-            // z partner (ii, jj, a), shared by both nodes
             {
                 T pv[NAUX];
                 const int nz = ii + 8 * (jj + 8 * a);
@@ -287,13 +288,12 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
             }
         }
 
-        // ---- surface fluxes of this thread's slots (applied after the volume term)
-        T nf[2][NS];
-        T fscale[2];
+        // ---- face-slot contributions (wsJ * nf) * MJI into shared memory
 #pragma unroll
         for (int sl = 0; sl < 2; ++sl) {
-            if (fslot[sl] < 0) continue;
-            const int f = fslot[sl], dir = f >> 1, side = f & 1;
+            const int slot = sl == 0 ? t : 256 + t;
+            if (slot >= 384) continue;
+            const int f = slot >> 6, dir = f >> 1, side = f & 1;
             const int vn = vnode[sl];
             T qm[NS];
 #pragma unroll
@@ -322,53 +322,48 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
             side_flux(qm, Fn[0], ws[0]);
             side_flux(qp[sl], Fn[1], ws[1]);
             const T mx = fmax(ws[0], ws[1]);
-#pragma unroll
-            for (int s = 0; s < NS; ++s) {
-                const T fc = (Fn[0][s] + Fn[1][s]) * T(0.5);
-                nf[sl][s] = A.surface_rusanov ? fc - (mx * (qp[sl][s] - qm[s])) * T(0.5) : fc;
-            }
-            // wsJ * MJI of the face node (hexsurfacemetrics! on a brick, MJI = 1/wJ)
+            // wsJ (hexsurfacemetrics! on a brick) and MJI = 1/wJ of the face node
             const int vi = vn & 7, vj = (vn >> 3) & 7, vk = vn >> 6;
             const int i1 = dir == 0 ? vj : vi, i2 = dir == 2 ? vj : vk;
             const double sJ = fabs(J * (dir == 0 ? drdx[0] : (dir == 1 ? drdx[1] : drdx[2])));
-            fscale[sl] = (T)((sJ * A.w[i1]) * A.w[i2]);
-        }
-
-        // ---- dq (smem) = rka*dq + volume term, own nodes
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int n = h ? n1 : n0;
+            const T wsJ = (T)((sJ * A.w[i1]) * A.w[i2]);
+            const T mji = (T)(1.0 / (((A.w[vi] * A.w[vj]) * A.w[vk]) * J));
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
-                T v = acc[h][s];
-                if (A.mode == MODE_STAGE) v = (T)A.rka * sm.dq[b][s][n] + v;
-                else if (A.mode == MODE_TENDENCY_INC) v = (T)((double)sm.dq[b][s][n] + (double)v);
-                sm.dq[b][s][n] = v;
+                const T fc = (Fn[0][s] + Fn[1][s]) * T(0.5);
+                const T nf = A.surface_rusanov ? fc - (mx * (qp[sl][s] - qm[s])) * T(0.5) : fc;
+                sm.sflux[s][slot] = (wsJ * nf) * mji;
             }
         }
-        __syncthreads();
-        // ---- surface term in Raven's face order: x faces, y faces, z faces
-#pragma unroll
-        for (int ph = 0; ph < 3; ++ph) {
-#pragma unroll
-            for (int sl = 0; sl < 2; ++sl) {
-                if (fslot[sl] < 0 || (fslot[sl] >> 1) != ph) continue;
-                const int vn = vnode[sl];
-                const int vi = vn & 7, vj = (vn >> 3) & 7, vk = vn >> 6;
-                const T mji = (T)(1.0 / (((A.w[vi] * A.w[vj]) * A.w[vk]) * J));
-#pragma unroll
-                for (int s = 0; s < NS; ++s) sm.dq[b][s][vn] = sm.dq[b][s][vn] - (fscale[sl] * nf[sl][s]) * mji;
+        __syncthreads();  // #2: face-slot contributions ready
+        if (read_dq) {
+            if (__syncthreads_or(!bounded_wait(&sm.bar[2], dqphase))) {
+                if (t == 0) atomicExch(A.status, kStatusTimeout);
+                return;
             }
-            __syncthreads();
+            dqphase ^= 1;
         }
-        // ---- write back: dq and q_out = q + rkb*dt*dq
+        // ---- own nodes: dq = rka*dq + volume - faces (x, y, z order); q_out = q + rkb*dt*dq
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int n = h ? n1 : n0;
+            const int kk = k0 + 4 * h;
+            int slots[3] = {-1, -1, -1};
+            if (ii == 0) slots[0] = jj + 8 * kk;
+            else if (ii == NQ - 1) slots[0] = 64 + jj + 8 * kk;
+            if (jj == 0) slots[1] = 128 + ii + 8 * kk;
+            else if (jj == NQ - 1) slots[1] = 192 + ii + 8 * kk;
+            if (kk == 0) slots[2] = 256 + ii + 8 * jj;
+            else if (kk == NQ - 1) slots[2] = 320 + ii + 8 * jj;
             const size_t g = (size_t)e * NS * NP + n;
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
-                const T v = sm.dq[b][s][n];
+                T v = acc[h][s];
+                if (A.mode == MODE_STAGE) v = (T)A.rka * sm.dq[s][n] + v;
+                else if (A.mode == MODE_TENDENCY_INC) v = (T)((double)sm.dq[s][n] + (double)v);
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    if (slots[d] >= 0) v = v - sm.sflux[s][slots[d]];
                 if (stage) {
                     if (dq_is_f32) reinterpret_cast<float*>(A.dq)[g + s * NP] = (float)v;
                     else reinterpret_cast<double*>(A.dq)[g + s * NP] = (double)v;
@@ -378,7 +373,6 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
                 }
             }
         }
-        __syncthreads();  // buffer b is free for the copy issued two iterations ahead
     }
 }
 
