@@ -46,7 +46,7 @@ struct PipeArgs {
 namespace pipe {
 
 constexpr int NQ = 8, NP = 512, NS = 5, NT = 256, NAUX = 6;
-constexpr int PAD(int n) { return n + (n >> 4); }  // one slot of padding every 16 nodes
+constexpr int PAD(int n) { return n + (n >> 3); }  // one vector slot of padding every 8 nodes
 constexpr int NPP = PAD(NP);                       // padded plane length
 constexpr long kWaitLimit = 1L << 26;
 
@@ -87,10 +87,21 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
 template <typename T>
+struct Vec2;
+template <>
+struct Vec2<double> {
+    using type = double2;
+};
+template <>
+struct Vec2<float> {
+    using type = float2;
+};
+
+template <typename T>
 struct Smem {
     double q[2][NS][NP];      // state: element being computed / element prefetched
     T dq[NS][NP];             // LSRK register of the element being computed
-    T aux[NAUX][NPP];         // per-node values the line partners need
+    typename Vec2<T>::type aux[NAUX / 2][NPP];  // per-node partner values, two per vector load
     T sflux[NS][384];         // face-slot contributions (wsJ * nf) * MJI
     T S[3][NQ][NQ];           // S_dir[a][id] * drdx_dir of the current element
     uint64_t bar[3];          // q buffers 0/1, dq buffer
@@ -187,7 +198,7 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
             const T m0 = (T)sm.q[b][1][n], m1 = (T)sm.q[b][2][n], m2 = (T)sm.q[b][3][n];
             const T u0 = m0 * rinv, u1 = m1 * rinv, u2 = m2 * rinv;
             const T rhoe = (T)sm.q[b][4][n];
-            const T p = gm1 * (rhoe - (m0 * m0 + m1 * m1 + m2 * m2) / (T(2) * rho));
+            const T p = gm1 * (rhoe - (m0 * m0 + m1 * m1 + m2 * m2) * (T(0.5) * rinv));
             if constexpr (COMBO == EUL_KG) {
                 own[h][0] = rho * T(0.5);
                 own[h][1] = u0 * T(0.5);
@@ -204,7 +215,10 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
                 own[h][5] = u0 * u0 + u1 * u1 + u2 * u2;
             }
 #pragma unroll
-            for (int c = 0; c < NAUX; ++c) sm.aux[c][PAD(n)] = own[h][c];
+            for (int c = 0; c < NAUX / 2; ++c) {
+                sm.aux[c][PAD(n)].x = own[h][2 * c];
+                sm.aux[c][PAD(n)].y = own[h][2 * c + 1];
+            }
         }
         __syncthreads();  // #1: aux and S ready; every thread is past the previous element
         if (t == 0) {
@@ -262,6 +276,14 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
             }
         };
 
+        auto load_aux = [&](T (&pv)[NAUX], const int n) {
+#pragma unroll
+            for (int c = 0; c < NAUX / 2; ++c) {
+                const auto v = sm.aux[c][PAD(n)];
+                pv[2 * c] = v.x;
+                pv[2 * c + 1] = v.y;
+            }
+        };
 #pragma unroll
         for (int a = 0; a < NQ; ++a) {
             const T sx = sm.S[0][a][ii], sy = sm.S[1][a][jj];
@@ -270,19 +292,16 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
                 const int kk = k0 + 4 * h;
                 T pv[NAUX];
                 const int nx = a + 8 * (jj + 8 * kk);
-#pragma unroll
-                for (int c = 0; c < NAUX; ++c) pv[c] = sm.aux[c][PAD(nx)];
+                load_aux(pv, nx);
                 pair(acc[h], own[h], pv, sx, 0);
                 const int ny = ii + 8 * (a + 8 * kk);
-#pragma unroll
-                for (int c = 0; c < NAUX; ++c) pv[c] = sm.aux[c][PAD(ny)];
+                load_aux(pv, ny);
                 pair(acc[h], own[h], pv, sy, 1);
             }
             {
                 T pv[NAUX];
                 const int nz = ii + 8 * (jj + 8 * a);
-#pragma unroll
-                for (int c = 0; c < NAUX; ++c) pv[c] = sm.aux[c][PAD(nz)];
+                load_aux(pv, nz);
                 pair(acc[0], own[0], pv, sm.S[2][a][k0], 2);
                 pair(acc[1], own[1], pv, sm.S[2][a][k0 + 4], 2);
             }
@@ -304,11 +323,10 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
             }
             const T sn = side ? T(1) : T(-1);
             T Fn[2][NS], ws[2];
-            // normal flux and wave speed of one side (euler.jl:50-68 with n = sn e_dir)
-            auto side_flux = [&](const T (&qq)[NS], T (&F)[NS], T& w) {
-                const T rinv = T(1) / qq[0];
-                const T u0 = qq[1] * rinv, u1 = qq[2] * rinv, u2 = qq[3] * rinv;
-                const T p = gm1 * (qq[4] - (qq[1] * qq[1] + qq[2] * qq[2] + qq[3] * qq[3]) / (T(2) * qq[0]));
+            // normal flux and wave speed of one side (euler.jl:50-68 with n = sn e_dir),
+            // from the conserved state and its primitives u, p
+            auto side_flux = [&](const T (&qq)[NS], const T u0, const T u1, const T u2, const T p, const T rinv,
+                                 T (&F)[NS], T& w) {
                 const T ud = dir == 0 ? u0 : dir == 1 ? u1 : u2;
                 const T un = ud * sn;
                 const T mn = (dir == 0 ? qq[1] : dir == 1 ? qq[2] : qq[3]) * sn;
@@ -319,20 +337,45 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
                 F[4] = un * (qq[4] + p);
                 w = fabs(un) + sqrt(gam * p * rinv);
             };
-            side_flux(qm, Fn[0], ws[0]);
-            side_flux(qp[sl], Fn[1], ws[1]);
+            auto prim = [&](const T (&qq)[NS], T& u0, T& u1, T& u2, T& p, T& rinv) {
+                rinv = T(1) / qq[0];
+                u0 = qq[1] * rinv;
+                u1 = qq[2] * rinv;
+                u2 = qq[3] * rinv;
+                p = gm1 * (qq[4] - (qq[1] * qq[1] + qq[2] * qq[2] + qq[3] * qq[3]) * (T(0.5) * rinv));
+            };
+            {
+                T u0, u1, u2, p, rinv;
+                if constexpr (COMBO == EUL_KG) {
+                    // the element's own primitives are already staged (halves)
+                    const auto v0 = sm.aux[0][PAD(vn)], v1 = sm.aux[1][PAD(vn)], v2 = sm.aux[2][PAD(vn)];
+                    u0 = T(2) * v0.y;
+                    u1 = T(2) * v1.x;
+                    u2 = T(2) * v1.y;
+                    p = T(2) * v2.y;
+                    rinv = T(0.5) / v0.x;
+                } else {
+                    prim(qm, u0, u1, u2, p, rinv);
+                }
+                side_flux(qm, u0, u1, u2, p, rinv, Fn[0], ws[0]);
+                if (open_face[sl]) {
+                    prim(qp[sl], u0, u1, u2, p, rinv);
+                    side_flux(qp[sl], u0, u1, u2, p, rinv, Fn[1], ws[1]);
+                } else {
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) Fn[1][s] = Fn[0][s];
+                    ws[1] = ws[0];
+                }
+            }
             const T mx = fmax(ws[0], ws[1]);
-            // wsJ (hexsurfacemetrics! on a brick) and MJI = 1/wJ of the face node
-            const int vi = vn & 7, vj = (vn >> 3) & 7, vk = vn >> 6;
-            const int i1 = dir == 0 ? vj : vi, i2 = dir == 2 ? vj : vk;
-            const double sJ = fabs(J * (dir == 0 ? drdx[0] : (dir == 1 ? drdx[1] : drdx[2])));
-            const T wsJ = (T)((sJ * A.w[i1]) * A.w[i2]);
-            const T mji = (T)(1.0 / (((A.w[vi] * A.w[vj]) * A.w[vk]) * J));
+            // (wsJ * MJI) of a face node of an unwarped brick: wsJ = |J drdx| w_a w_b and
+            // MJI = 1 / (w_i w_j w_k J) leave |drdx_dir| / w_end (w_end = w_0 = w_N)
+            const T fsc = (T)(fabs(dir == 0 ? drdx[0] : (dir == 1 ? drdx[1] : drdx[2])) / A.w[0]);
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
                 const T fc = (Fn[0][s] + Fn[1][s]) * T(0.5);
                 const T nf = A.surface_rusanov ? fc - (mx * (qp[sl][s] - qm[s])) * T(0.5) : fc;
-                sm.sflux[s][slot] = (wsJ * nf) * mji;
+                sm.sflux[s][slot] = nf * fsc;
             }
         }
         __syncthreads();  // #2: face-slot contributions ready
