@@ -131,6 +131,29 @@ rb200_status rb200_sync_status(rb200_handle* h, void* stream);
  * (0 when the handle's configuration does not use it). */
 rb200_status rb200_get_info(const rb200_handle* h, int64_t* info, int32_t n);
 
+/* Weighted sums without any device allocation (no counterpart in the reference).
+ *
+ * For callers that cannot call cudaMalloc: code whose device memory is owned by a
+ * pooling allocator (CUDA.jl and PyTorch keep most of the device reserved in their
+ * caching pools, so a raw cudaMalloc from inside a library can fail or fragment the
+ * pool), and code that runs where allocating is not allowed, such as a monitoring hook
+ * called between the steps of a solve.  The handle API allocates in rb200_create;
+ * this entry point needs no handle and allocates nothing.
+ *
+ * sums_out[s] = sum(MJ .* q_s.^2) and sums_out[ns + s] = sum(MJ .* q_s), s < ns, in
+ * FP64 with a fixed reduction order: the squares give weightednorm (take square
+ * roots), the plain sums the conservation integrals.  q: device (np, ns, E) FP64, MJ:
+ * device (np, E) FP64 nodal weights (DGSEM's MJ), sums_out: device, 2*ns doubles.
+ *
+ * Scratch: a file-scope device array of 256 * 2 * 5 doubles (20 KB) that every device
+ * loading the library holds until exit; hence ns <= 5 (larger ns returns
+ * RB200_ERR_UNSUPPORTED), np <= 512.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress, with that device current); make that first call
+ * before any stream capture.  All calls share the array: calls that overlap on the GPU
+ * (for instance on two streams) race and must be ordered by the caller. */
+rb200_status rb200_weighted_sums_noalloc(const double* q, const double* MJ, int32_t np, int32_t ns,
+                                         int64_t num_elements, double* sums_out, void* stream);
+
 /* Last error message of a handle (empty if none); static text for NULL. */
 const char* rb200_last_error(const rb200_handle* h);
 const char* rb200_status_string(rb200_status s);

@@ -37,6 +37,7 @@ EXPORTED = [
     "rb200_get_info",
     "rb200_set_kernel_path",
     "rb200_sync_status",
+    "rb200_weighted_sums_noalloc",
     "rb200_last_error",
     "rb200_status_string",
 ]
@@ -98,6 +99,7 @@ def lib():
     L.rb200_get_info.argtypes = [P, P, I32]
     L.rb200_set_kernel_path.argtypes = [P, I32]
     L.rb200_sync_status.argtypes = [P, P]
+    L.rb200_weighted_sums_noalloc.argtypes = [P, P, I32, I32, I64, P, P]
     L.rb200_last_error.argtypes = [P]
     L.rb200_last_error.restype = ctypes.c_char_p
     L.rb200_status_string.argtypes = [ctypes.c_int]

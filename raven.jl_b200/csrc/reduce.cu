@@ -4,6 +4,9 @@
 // The reductions are deterministic: a fixed number of CTAs each own a fixed,
 // strided set of elements, partial sums are combined in a fixed tree, and a single
 // CTA adds the per-CTA partials in index order.
+#include <mutex>
+
+#include "../../include/raven_b200.h"
 #include "rb200_internal.h"
 
 namespace rb200 {
@@ -87,6 +90,47 @@ __global__ void face_vmapP_kernel(const int32_t* __restrict__ nbr, int dim, int 
     }
 }
 
+// Variant of weighted_sums_kernel for rb200_weighted_sums_noalloc: the caller passes
+// the nodal weights MJ (Np, E) instead of the handle's geometry.
+__global__ void __launch_bounds__(kRedThreads) weighted_sums_mj_kernel(const double* __restrict__ q,
+                                                                       const double* __restrict__ mj, int np,
+                                                                       int ns, int64_t E,
+                                                                       double* __restrict__ partial) {
+    __shared__ double red[kRedThreads];
+    for (int s = 0; s < ns; ++s) {
+        double a2 = 0.0, a1 = 0.0;
+        for (int64_t e = blockIdx.x; e < E; e += gridDim.x) {
+            for (int n = threadIdx.x; n < np; n += blockDim.x) {
+                const double w = mj[(size_t)e * np + n];
+                const double v = q[((size_t)e * ns + s) * np + n];
+                a2 += w * (v * v);
+                a1 += w * v;
+            }
+        }
+        for (int pass = 0; pass < 2; ++pass) {
+            red[threadIdx.x] = pass == 0 ? a2 : a1;
+            __syncthreads();
+            for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+                if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) partial[(size_t)blockIdx.x * 2 * ns + pass * ns + s] = red[0];
+            __syncthreads();
+        }
+    }
+}
+
+// Scratch of rb200_weighted_sums_noalloc: one slot per (CTA, sum).  Every CTA of a
+// call writes all of its slots before the final sum reads them, so nothing has to be
+// cleared between calls.  It lives in every device that loads the library, until exit.
+constexpr int kNoAllocBlocks = 256;
+constexpr int kNoAllocMaxFields = 5;
+__device__ __align__(256) double g_noalloc_partials[kNoAllocBlocks * 2 * kNoAllocMaxFields];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
+
 }  // namespace
 
 cudaError_t launch_weighted_sums(const double* q, const double* elem_geo, const double* vgeo, const double* w, int dim,
@@ -110,3 +154,36 @@ cudaError_t launch_face_vmapP(const int32_t* nbr, int dim, int nq, int64_t E, in
 }
 
 }  // namespace rb200
+
+// ---------------------------------------------------------------------------------
+// rb200_weighted_sums_noalloc (declared in include/raven_b200.h)
+// ---------------------------------------------------------------------------------
+extern "C" rb200_status rb200_weighted_sums_noalloc(const double* q, const double* MJ, int32_t np, int32_t ns,
+                                                    int64_t num_elements, double* sums_out, void* stream) {
+    using namespace rb200;
+    if (!q || !MJ || !sums_out) return RB200_ERR_BAD_ARG;
+    if (np < 1 || np > 512 || num_elements < 0) return RB200_ERR_BAD_ARG;
+    if (ns < 1 || ns > kNoAllocMaxFields) return RB200_ERR_UNSUPPORTED;  // beyond the scratch array
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return RB200_ERR_CUDA;
+    double* scratch;
+    {
+        // once per device, with that device current: the device address of the array
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_ptr[dev]) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p) {
+                cudaGetLastError();
+                return RB200_ERR_CUDA;
+            }
+            g_noalloc_ptr[dev] = static_cast<double*>(p);
+        }
+        scratch = g_noalloc_ptr[dev];
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    weighted_sums_mj_kernel<<<kNoAllocBlocks, kRedThreads, 0, s>>>(q, MJ, np, ns, num_elements, scratch);
+    if (cudaGetLastError() != cudaSuccess) return RB200_ERR_CUDA;
+    finish_sums_kernel<<<1, 32, 0, s>>>(scratch, kNoAllocBlocks, 2 * ns, sums_out);
+    if (cudaGetLastError() != cudaSuccess) return RB200_ERR_CUDA;
+    return RB200_OK;
+}
