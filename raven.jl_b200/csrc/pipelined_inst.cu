@@ -3,9 +3,14 @@
 
 namespace rb200 {
 
+#ifndef RB200_PIPE_NPT
+#define RB200_PIPE_NPT 2  // nodes per thread of the pipelined kernel
+#endif
+constexpr int kNPT = RB200_PIPE_NPT;
+
 template <int COMBO, typename T>
 static cudaError_t launch_p(const PipeArgs& a, int grid, cudaStream_t s) {
-    auto kern = pipelined_stage_kernel<COMBO, T>;
+    auto kern = pipelined_stage_kernel<COMBO, T, kNPT>;
     static bool configured = false;
     if (!configured) {
         cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -13,7 +18,7 @@ static cudaError_t launch_p(const PipeArgs& a, int grid, cudaStream_t s) {
         if (err != cudaSuccess) return err;
         configured = true;
     }
-    kern<<<grid, pipe::NT, sizeof(pipe::Smem<T>), s>>>(a);
+    kern<<<grid, 512 / kNPT, sizeof(pipe::Smem<T>), s>>>(a);
     return cudaGetLastError();
 }
 
@@ -25,12 +30,12 @@ cudaError_t launch_pipelined(int combo, int fp32, const PipeArgs& a, int grid, c
 
 template <int COMBO, typename T>
 static int occupancy_p() {
-    auto kern = pipelined_stage_kernel<COMBO, T>;
+    auto kern = pipelined_stage_kernel<COMBO, T, kNPT>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(pipe::Smem<T>)) !=
         cudaSuccess)
         return 0;
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, pipe::NT, sizeof(pipe::Smem<T>)) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, 512 / kNPT, sizeof(pipe::Smem<T>)) != cudaSuccess)
         return 0;
     return n;
 }

@@ -1,20 +1,21 @@
 // Persistent, TMA-pipelined stage kernel for 3-D hexahedra with Nq = 8 on unwarped
 // bricks, flux-differencing volume forms (Kennedy-Gruber, entropy conservative).
 //
-// Each CTA owns a strided set of elements (e = blockIdx.x + k*gridDim.x).  While it
-// computes element e, one thread has already issued 1-D bulk copies (cp.async.bulk,
-// completion on an mbarrier) of the next element's state q and LSRK register dq into
-// the other half of a double buffer, so the HBM stream overlaps the flux arithmetic.
-// Two CTAs share an SM.
+// Each CTA owns a strided set of elements (e = blockIdx.x + k*gridDim.x) and two CTAs
+// share an SM.  The element's state q arrives by one 1-D bulk copy (cp.async.bulk,
+// completion on an mbarrier) into shared memory; it is only needed to build the
+// per-node partner values, so right after the first barrier the copy of the CTA's next
+// element is issued into the same buffer and lands while the current element's flux
+// arithmetic runs.  Neighbour face traces are fetched with cp.async into the face-slot
+// buffer; the element's own old q and dq are read with coalesced loads at the end.
 //
-// Thread t owns the two nodes t and t+256 of the element (same i, j; k and k+4), so
-// the eight z-partners of its line are loaded once for both nodes.  The metric of an
+// A thread owns NPT nodes of the element (same i, j), so the eight z-partners of its
+// line are loaded once for all of them.  The metric of an
 // unwarped brick is folded into a per-element table S_dir[a][id] =
 // drdx_dir * (D[a,id] w_a / w_id - D[id,a]), which equals MJI_id * (D[a,id] l_g[a] -
-// D[id,a] l_g[id]) of esvolumeterm_dir! (src/balancelaws/dgsem.jl:576-600).
-// Neighbour traces are prefetched into registers before the volume loop; the face
-// fluxes are then applied in the order x-, x+, y-, y+, z-, z+ of surfaceterm!
-// (dgsem.jl:756-782).
+// D[id,a] l_g[id]) of esvolumeterm_dir! (src/balancelaws/dgsem.jl:576-600).  Face
+// fluxes are applied in the order x-, x+, y-, y+, z-, z+ of surfaceterm!
+// (dgsem.jl:756-782) by the owner of each face node.
 //
 // Every wait on an mbarrier is bounded: after kWaitLimit polls the CTA records
 // RB200 status TIMEOUT in *A.status and returns.
@@ -45,7 +46,7 @@ struct PipeArgs {
 
 namespace pipe {
 
-constexpr int NQ = 8, NP = 512, NS = 5, NT = 256, NAUX = 6;
+constexpr int NQ = 8, NP = 512, NS = 5, NAUX = 6, NSLOT = 384;
 constexpr int PAD(int n) { return n + (n >> 3); }  // one vector slot of padding every 8 nodes
 constexpr int NPP = PAD(NP);                       // padded plane length
 constexpr long kWaitLimit = 1L << 26;
@@ -83,6 +84,12 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
         : "memory");
 }
 
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
@@ -99,12 +106,11 @@ struct Vec2<float> {
 
 template <typename T>
 struct Smem {
-    double q[2][NS][NP];      // state: element being computed / element prefetched
-    T dq[NS][NP];             // LSRK register of the element being computed
+    double q[NS][NP];                           // state of the element (TMA destination)
     typename Vec2<T>::type aux[NAUX / 2][NPP];  // per-node partner values, two per vector load
-    T sflux[NS][384];         // face-slot contributions (wsJ * nf) * MJI
-    T S[3][NQ][NQ];           // S_dir[a][id] * drdx_dir of the current element
-    uint64_t bar[3];          // q buffers 0/1, dq buffer
+    double slot[NS][NSLOT];                     // neighbour trace, then (wsJ * nf) * MJI, per face slot
+    T S[3][NQ][NQ];                             // S_dir[a][id] * drdx_dir of the current element
+    uint64_t bar;
 };
 
 __device__ __forceinline__ bool bounded_wait(uint64_t* bar, uint32_t parity) {
@@ -115,89 +121,83 @@ __device__ __forceinline__ bool bounded_wait(uint64_t* bar, uint32_t parity) {
     return true;
 }
 
+// 0-based volume node of face slot `slot` (faces x-, x+, y-, y+, z-, z+; 64 slots each)
+// and the node of the opposite face with the same in-face index.
+__device__ __forceinline__ void slot_nodes(int slot, int& vn, int& opp) {
+    const int f = slot >> 6, jf = slot & 63;
+    const int dir = f >> 1, side = f & 1;
+    const int j1 = jf & 7, j2 = jf >> 3, c = side ? NQ - 1 : 0;
+    if (dir == 0) {
+        vn = c + 8 * (j1 + 8 * j2);
+        opp = (NQ - 1 - c) + 8 * (j1 + 8 * j2);
+    } else if (dir == 1) {
+        vn = j1 + 8 * (c + 8 * j2);
+        opp = j1 + 8 * ((NQ - 1 - c) + 8 * j2);
+    } else {
+        vn = j1 + 8 * (j2 + 8 * c);
+        opp = j1 + 8 * (j2 + 8 * (NQ - 1 - c));
+    }
+}
+
 }  // namespace pipe
 
-template <int COMBO, typename T>
-__global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __grid_constant__ PipeArgs A) {
+#ifndef RB200_PIPE_MIN_CTAS
+#define RB200_PIPE_MIN_CTAS 2  // CTAs per SM the register allocation is sized for
+#endif
+
+// NPT nodes per thread: thread t owns nodes t + (512/NPT)*h, h < NPT, which share i, j
+// (k = k0 + (8/NPT)*h), so their z-partners are loaded once.
+template <int COMBO, typename T, int NPT>
+__global__ void __launch_bounds__(512 / NPT, RB200_PIPE_MIN_CTAS)
+    pipelined_stage_kernel(const __grid_constant__ PipeArgs A) {
     using namespace pipe;
+    constexpr int NT = 512 / NPT, KS = 8 / NPT;
     extern __shared__ __align__(128) unsigned char pipe_smem_raw[];
     Smem<T>& sm = *reinterpret_cast<Smem<T>*>(pipe_smem_raw);
     const int t = threadIdx.x;
-    const int ii = t & 7, jj = (t >> 3) & 7, k0 = t >> 6;  // nodes (ii, jj, k0) and (ii, jj, k0 + 4)
-    const int n0 = t, n1 = t + 256;
+    const int ii = t & 7, jj = (t >> 3) & 7, k0 = t >> 6;
     const bool stage = A.mode >= MODE_STAGE;
-    const bool read_dq = A.mode == MODE_STAGE || A.mode == MODE_TENDENCY_INC;
     const bool dq_is_f32 = stage && sizeof(T) == 4;
     const uint32_t qbytes = NS * NP * sizeof(double);
-    const uint32_t dqbytes = NS * NP * (dq_is_f32 ? 4 : 8);
     const T gm1 = (T)(A.gamma - 1.0), gam = (T)A.gamma;
 
     if (t == 0) {
-        mbar_init(&sm.bar[0], 1);
-        mbar_init(&sm.bar[1], 1);
-        mbar_init(&sm.bar[2], 1);
+        mbar_init(&sm.bar, 1);
         fence_mbar_init();
     }
     __syncthreads();
 
     int64_t e = blockIdx.x;
     if (t == 0 && e < A.E) {
-        mbar_expect_tx(&sm.bar[0], qbytes);
-        bulk_g2s(&sm.q[0][0][0], A.q_in + (size_t)e * NS * NP, qbytes, &sm.bar[0]);
+        mbar_expect_tx(&sm.bar, qbytes);
+        bulk_g2s(&sm.q[0][0], A.q_in + (size_t)e * NS * NP, qbytes, &sm.bar);
     }
-    uint32_t qphase[2] = {0, 0}, dqphase = 0;
-    int b = 0;
-    for (; e < A.E; e += gridDim.x, b ^= 1) {
+    uint32_t phase = 0;
+    for (; e < A.E; e += gridDim.x) {
         const int64_t enext = e + gridDim.x;
-        // ---- element geometry, scaled S table, neighbour traces (global/L2) issued early
         const double* eg = A.elem_geo + 4 * e;
         const double drdx[3] = {__ldg(eg), __ldg(eg + 1), __ldg(eg + 2)};
-        const double J = __ldg(eg + 3);
         if (t < 192) {
             const int dir = t >> 6, a = (t >> 3) & 7, id = t & 7;
             const double dd = dir == 0 ? drdx[0] : (dir == 1 ? drdx[1] : drdx[2]);
             sm.S[dir][a][id] = (T)(A.S[a * 8 + id] * dd);
         }
-        // face slots: s0 = t (faces x-, x+, y-, y+), s1 = 256 + t for t < 128 (z-, z+)
-        T qp[2][NS];
-        int vnode[2] = {0, 0};
-        bool open_face[2] = {false, false};  // false: boundary face, q+ = q- (balancelaw.jl:77)
-#pragma unroll
-        for (int sl = 0; sl < 2; ++sl) {
-            const int slot = sl == 0 ? t : 256 + t;
-            if (slot >= 384) continue;
-            const int f = slot >> 6, jf = slot & 63;
-            const int dir = f >> 1, side = f & 1;
-            const int j1 = jf & 7, j2 = jf >> 3, c = side ? NQ - 1 : 0;
-            int vn, opp;
-            if (dir == 0) { vn = c + 8 * (j1 + 8 * j2); opp = (NQ - 1 - c) + 8 * (j1 + 8 * j2); }
-            else if (dir == 1) { vn = j1 + 8 * (c + 8 * j2); opp = j1 + 8 * ((NQ - 1 - c) + 8 * j2); }
-            else { vn = j1 + 8 * (j2 + 8 * c); opp = j1 + 8 * (j2 + 8 * (NQ - 1 - c)); }
-            vnode[sl] = vn;
-            const int ne = __ldg(A.nbr + 6 * e + f);
-            open_face[sl] = ne >= 0;
-            if (ne >= 0) {
-                const double* qn = A.q_in + (size_t)ne * NS * NP + opp;
-#pragma unroll
-                for (int s = 0; s < NS; ++s) qp[sl][s] = (T)__ldg(qn + s * NP);
-            }
-        }
         // ---- this element's state
-        if (__syncthreads_or(!bounded_wait(&sm.bar[b], qphase[b]))) {
+        if (__syncthreads_or(!bounded_wait(&sm.bar, phase))) {
             if (t == 0) atomicExch(A.status, kStatusTimeout);
             return;
         }
-        qphase[b] ^= 1;
+        phase ^= 1;
         // ---- per-node partner values
-        T own[2][NAUX];
+        T own[NPT][NAUX];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int n = h ? n1 : n0;
-            const T rho = (T)sm.q[b][0][n];
+        for (int h = 0; h < NPT; ++h) {
+            const int n = t + NT * h;
+            const T rho = (T)sm.q[0][n];
             const T rinv = T(1) / rho;
-            const T m0 = (T)sm.q[b][1][n], m1 = (T)sm.q[b][2][n], m2 = (T)sm.q[b][3][n];
+            const T m0 = (T)sm.q[1][n], m1 = (T)sm.q[2][n], m2 = (T)sm.q[3][n];
             const T u0 = m0 * rinv, u1 = m1 * rinv, u2 = m2 * rinv;
-            const T rhoe = (T)sm.q[b][4][n];
+            const T rhoe = (T)sm.q[4][n];
             const T p = gm1 * (rhoe - (m0 * m0 + m1 * m1 + m2 * m2) * (T(0.5) * rinv));
             if constexpr (COMBO == EUL_KG) {
                 own[h][0] = rho * T(0.5);
@@ -220,25 +220,32 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
                 sm.aux[c][PAD(n)].y = own[h][2 * c + 1];
             }
         }
-        __syncthreads();  // #1: aux and S ready; every thread is past the previous element
-        if (t == 0) {
-            // the other q buffer and the dq buffer were last read before barrier #1
+        __syncthreads();  // #1: aux and S ready; q and the slot buffer are free
+        if (t == 0 && enext < A.E) {
             fence_proxy_async();
-            if (enext < A.E) {
-                mbar_expect_tx(&sm.bar[b ^ 1], qbytes);
-                bulk_g2s(&sm.q[b ^ 1][0][0], A.q_in + (size_t)enext * NS * NP, qbytes, &sm.bar[b ^ 1]);
-            }
-            if (read_dq) {
-                mbar_expect_tx(&sm.bar[2], dqbytes);
-                bulk_g2s(&sm.dq[0][0], reinterpret_cast<const char*>(A.dq) + (size_t)e * dqbytes, dqbytes,
-                         &sm.bar[2]);
+            mbar_expect_tx(&sm.bar, qbytes);
+            bulk_g2s(&sm.q[0][0], A.q_in + (size_t)enext * NS * NP, qbytes, &sm.bar);
+        }
+        // neighbour traces of this thread's face slots t + NT * sl
+#pragma unroll
+        for (int sl = 0; sl < (NSLOT + NT - 1) / NT; ++sl) {
+            const int slot = t + NT * sl;
+            if (slot >= NSLOT) continue;
+            int vn, opp;
+            slot_nodes(slot, vn, opp);
+            const int ne = __ldg(A.nbr + 6 * e + (slot >> 6));
+            if (ne >= 0) {
+                const double* qn = A.q_in + (size_t)ne * NS * NP + opp;
+#pragma unroll
+                for (int s = 0; s < NS; ++s) cp_async8(&sm.slot[s][slot], qn + s * NP);
             }
         }
+        cp_async_commit();
 
         // ---- volume term (ordered pairs along x, y, z)
-        T acc[2][NS];
+        T acc[NPT][NS];
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
+        for (int h = 0; h < NPT; ++h)
 #pragma unroll
             for (int s = 0; s < NS; ++s) acc[h][s] = T(0);
 
@@ -275,7 +282,6 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
                 ac[4] = fma(un, cc * rlog + rlog * uaa + pt, ac[4]);
             }
         };
-
         auto load_aux = [&](T (&pv)[NAUX], const int n) {
 #pragma unroll
             for (int c = 0; c < NAUX / 2; ++c) {
@@ -288,84 +294,107 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
         for (int a = 0; a < NQ; ++a) {
             const T sx = sm.S[0][a][ii], sy = sm.S[1][a][jj];
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int kk = k0 + 4 * h;
+            for (int h = 0; h < NPT; ++h) {
+                const int kk = k0 + KS * h;
                 T pv[NAUX];
-                const int nx = a + 8 * (jj + 8 * kk);
-                load_aux(pv, nx);
+                load_aux(pv, a + 8 * (jj + 8 * kk));
                 pair(acc[h], own[h], pv, sx, 0);
-                const int ny = ii + 8 * (a + 8 * kk);
-                load_aux(pv, ny);
+                load_aux(pv, ii + 8 * (a + 8 * kk));
                 pair(acc[h], own[h], pv, sy, 1);
             }
-            {
-                T pv[NAUX];
-                const int nz = ii + 8 * (jj + 8 * a);
-                load_aux(pv, nz);
-                pair(acc[0], own[0], pv, sm.S[2][a][k0], 2);
-                pair(acc[1], own[1], pv, sm.S[2][a][k0 + 4], 2);
-            }
+            T pv[NAUX];
+            load_aux(pv, ii + 8 * (jj + 8 * a));
+#pragma unroll
+            for (int h = 0; h < NPT; ++h) pair(acc[h], own[h], pv, sm.S[2][a][k0 + KS * h], 2);
         }
 
-        // ---- face-slot contributions (wsJ * nf) * MJI into shared memory
+        // ---- own old state and register, read now so that the loads overlap the faces
+        const size_t g0 = (size_t)e * NS * NP + t;
+        double qold[NPT][NS];
+        T dqold[NPT][NS];
 #pragma unroll
-        for (int sl = 0; sl < 2; ++sl) {
-            const int slot = sl == 0 ? t : 256 + t;
-            if (slot >= 384) continue;
-            const int f = slot >> 6, dir = f >> 1, side = f & 1;
-            const int vn = vnode[sl];
-            T qm[NS];
+        for (int h = 0; h < NPT; ++h)
 #pragma unroll
-            for (int s = 0; s < NS; ++s) qm[s] = (T)sm.q[b][s][vn];
-            if (!open_face[sl]) {
-#pragma unroll
-                for (int s = 0; s < NS; ++s) qp[sl][s] = qm[s];
+            for (int s = 0; s < NS; ++s) {
+                const size_t g = g0 + NT * h + s * NP;
+                qold[h][s] = stage ? __ldg(A.q_in + g) : 0.0;
+                if (A.mode == MODE_STAGE || A.mode == MODE_TENDENCY_INC)
+                    dqold[h][s] = dq_is_f32 ? (T)__ldg(reinterpret_cast<const float*>(A.dq) + g)
+                                            : (T)__ldg(reinterpret_cast<const double*>(A.dq) + g);
+                else
+                    dqold[h][s] = T(0);
             }
-            const T sn = side ? T(1) : T(-1);
-            T Fn[2][NS], ws[2];
-            // normal flux and wave speed of one side (euler.jl:50-68 with n = sn e_dir),
-            // from the conserved state and its primitives u, p
-            auto side_flux = [&](const T (&qq)[NS], const T u0, const T u1, const T u2, const T p, const T rinv,
-                                 T (&F)[NS], T& w) {
-                const T ud = dir == 0 ? u0 : dir == 1 ? u1 : u2;
-                const T un = ud * sn;
-                const T mn = (dir == 0 ? qq[1] : dir == 1 ? qq[2] : qq[3]) * sn;
-                F[0] = mn;
-                F[1] = mn * u0 + (dir == 0 ? p * sn : T(0));
-                F[2] = mn * u1 + (dir == 1 ? p * sn : T(0));
-                F[3] = mn * u2 + (dir == 2 ? p * sn : T(0));
-                F[4] = un * (qq[4] + p);
-                w = fabs(un) + sqrt(gam * p * rinv);
-            };
-            auto prim = [&](const T (&qq)[NS], T& u0, T& u1, T& u2, T& p, T& rinv) {
-                rinv = T(1) / qq[0];
-                u0 = qq[1] * rinv;
-                u1 = qq[2] * rinv;
-                u2 = qq[3] * rinv;
-                p = gm1 * (qq[4] - (qq[1] * qq[1] + qq[2] * qq[2] + qq[3] * qq[3]) * (T(0.5) * rinv));
-            };
+
+        // ---- face-slot contributions (wsJ * nf) * MJI, written over the slot's trace
+        cp_async_wait_all();
+#pragma unroll
+        for (int sl = 0; sl < (NSLOT + NT - 1) / NT; ++sl) {
+            const int slot = t + NT * sl;
+            if (slot >= NSLOT) continue;
+            const int f = slot >> 6, dir = f >> 1, side = f & 1;
+            int vn, opp;
+            slot_nodes(slot, vn, opp);
+            const bool open_face = __ldg(A.nbr + 6 * e + f) >= 0;
+            // q- and its primitives from the staged partner values of the element
+            T qm[NS], u0, u1, u2, p, rinv;
             {
-                T u0, u1, u2, p, rinv;
+                const auto v0 = sm.aux[0][PAD(vn)], v1 = sm.aux[1][PAD(vn)], v2 = sm.aux[2][PAD(vn)];
                 if constexpr (COMBO == EUL_KG) {
-                    // the element's own primitives are already staged (halves)
-                    const auto v0 = sm.aux[0][PAD(vn)], v1 = sm.aux[1][PAD(vn)], v2 = sm.aux[2][PAD(vn)];
+                    const T rho = T(2) * v0.x;
                     u0 = T(2) * v0.y;
                     u1 = T(2) * v1.x;
                     u2 = T(2) * v1.y;
                     p = T(2) * v2.y;
-                    rinv = T(0.5) / v0.x;
+                    rinv = T(1) / rho;
+                    qm[0] = rho;
+                    qm[4] = rho * (T(2) * v2.x);
                 } else {
-                    prim(qm, u0, u1, u2, p, rinv);
+                    const T rho = v0.x;
+                    u0 = v0.y;
+                    u1 = v1.x;
+                    u2 = v1.y;
+                    p = rho / (T(2) * v2.x);
+                    rinv = T(1) / rho;
+                    qm[0] = rho;
+                    qm[4] = p / gm1 + T(0.5) * rho * v2.y;
                 }
-                side_flux(qm, u0, u1, u2, p, rinv, Fn[0], ws[0]);
-                if (open_face[sl]) {
-                    prim(qp[sl], u0, u1, u2, p, rinv);
-                    side_flux(qp[sl], u0, u1, u2, p, rinv, Fn[1], ws[1]);
-                } else {
+                qm[1] = qm[0] * u0;
+                qm[2] = qm[0] * u1;
+                qm[3] = qm[0] * u2;
+            }
+            const T sn = side ? T(1) : T(-1);
+            T Fn[2][NS], ws[2];
+            // normal flux and wave speed of one side (euler.jl:50-68 with n = sn e_dir)
+            auto side_flux = [&](const T (&qq)[NS], const T a0, const T a1, const T a2, const T pp, const T ri,
+                                 T (&F)[NS], T& w) {
+                const T ud = dir == 0 ? a0 : dir == 1 ? a1 : a2;
+                const T un = ud * sn;
+                const T mn = (dir == 0 ? qq[1] : dir == 1 ? qq[2] : qq[3]) * sn;
+                F[0] = mn;
+                F[1] = mn * a0 + (dir == 0 ? pp * sn : T(0));
+                F[2] = mn * a1 + (dir == 1 ? pp * sn : T(0));
+                F[3] = mn * a2 + (dir == 2 ? pp * sn : T(0));
+                F[4] = un * (qq[4] + pp);
+                w = fabs(un) + sqrt(gam * pp * ri);
+            };
+            side_flux(qm, u0, u1, u2, p, rinv, Fn[0], ws[0]);
+            T qp[NS];
+            if (open_face) {
 #pragma unroll
-                    for (int s = 0; s < NS; ++s) Fn[1][s] = Fn[0][s];
-                    ws[1] = ws[0];
+                for (int s = 0; s < NS; ++s) qp[s] = (T)sm.slot[s][slot];
+                rinv = T(1) / qp[0];
+                u0 = qp[1] * rinv;
+                u1 = qp[2] * rinv;
+                u2 = qp[3] * rinv;
+                p = gm1 * (qp[4] - (qp[1] * qp[1] + qp[2] * qp[2] + qp[3] * qp[3]) * (T(0.5) * rinv));
+                side_flux(qp, u0, u1, u2, p, rinv, Fn[1], ws[1]);
+            } else {  // boundary face: q+ = q- (balancelaw.jl:77)
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    qp[s] = qm[s];
+                    Fn[1][s] = Fn[0][s];
                 }
+                ws[1] = ws[0];
             }
             const T mx = fmax(ws[0], ws[1]);
             // (wsJ * MJI) of a face node of an unwarped brick: wsJ = |J drdx| w_a w_b and
@@ -374,23 +403,15 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
                 const T fc = (Fn[0][s] + Fn[1][s]) * T(0.5);
-                const T nf = A.surface_rusanov ? fc - (mx * (qp[sl][s] - qm[s])) * T(0.5) : fc;
-                sm.sflux[s][slot] = nf * fsc;
+                const T nf = A.surface_rusanov ? fc - (mx * (qp[s] - qm[s])) * T(0.5) : fc;
+                sm.slot[s][slot] = (double)(nf * fsc);
             }
         }
         __syncthreads();  // #2: face-slot contributions ready
-        if (read_dq) {
-            if (__syncthreads_or(!bounded_wait(&sm.bar[2], dqphase))) {
-                if (t == 0) atomicExch(A.status, kStatusTimeout);
-                return;
-            }
-            dqphase ^= 1;
-        }
         // ---- own nodes: dq = rka*dq + volume - faces (x, y, z order); q_out = q + rkb*dt*dq
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int n = h ? n1 : n0;
-            const int kk = k0 + 4 * h;
+        for (int h = 0; h < NPT; ++h) {
+            const int kk = k0 + KS * h;
             int slots[3] = {-1, -1, -1};
             if (ii == 0) slots[0] = jj + 8 * kk;
             else if (ii == NQ - 1) slots[0] = 64 + jj + 8 * kk;
@@ -398,21 +419,21 @@ __global__ void __launch_bounds__(pipe::NT, 2) pipelined_stage_kernel(const __gr
             else if (jj == NQ - 1) slots[1] = 192 + ii + 8 * kk;
             if (kk == 0) slots[2] = 256 + ii + 8 * jj;
             else if (kk == NQ - 1) slots[2] = 320 + ii + 8 * jj;
-            const size_t g = (size_t)e * NS * NP + n;
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
                 T v = acc[h][s];
-                if (A.mode == MODE_STAGE) v = (T)A.rka * sm.dq[s][n] + v;
-                else if (A.mode == MODE_TENDENCY_INC) v = (T)((double)sm.dq[s][n] + (double)v);
+                if (A.mode == MODE_STAGE) v = (T)A.rka * dqold[h][s] + v;
+                else if (A.mode == MODE_TENDENCY_INC) v = (T)((double)dqold[h][s] + (double)v);
 #pragma unroll
                 for (int d = 0; d < 3; ++d)
-                    if (slots[d] >= 0) v = v - sm.sflux[s][slots[d]];
+                    if (slots[d] >= 0) v = v - (T)sm.slot[s][slots[d]];
+                const size_t g = g0 + NT * h + s * NP;
                 if (stage) {
-                    if (dq_is_f32) reinterpret_cast<float*>(A.dq)[g + s * NP] = (float)v;
-                    else reinterpret_cast<double*>(A.dq)[g + s * NP] = (double)v;
-                    A.q_out[g + s * NP] = sm.q[b][s][n] + A.rkb_dt * (double)v;
+                    if (dq_is_f32) reinterpret_cast<float*>(A.dq)[g] = (float)v;
+                    else reinterpret_cast<double*>(A.dq)[g] = (double)v;
+                    A.q_out[g] = qold[h][s] + A.rkb_dt * (double)v;
                 } else {
-                    reinterpret_cast<double*>(A.dq)[g + s * NP] = (double)v;
+                    reinterpret_cast<double*>(A.dq)[g] = (double)v;
                 }
             }
         }
