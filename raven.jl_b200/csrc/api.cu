@@ -46,6 +46,14 @@ struct rb200_handle {
     int32_t* d_status = nullptr;  // bounded-wait error word written by the kernels
     int red_blocks = 0;
     int kernel_path = 0;          // 0 automatic, 1 generic stage kernel only
+    // CUDA graph of two LSRK steps (10 stage launches) for one (q, dq, dt), replayed by
+    // rb200_lsrk54_step; captured on a stream of the handle, launched on the caller's
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    const double* graph_q = nullptr;
+    const void* graph_dq = nullptr;
+    double graph_dt = 0.0;
+    int use_graphs = 1;
     int pipe_grid = 0;            // CTAs of the pipelined kernel (0: not eligible)
     double pipe_S[64] = {0};      // D[a,id] w[a] / w[id] - D[id,a]
     std::string err;
@@ -103,7 +111,17 @@ rb200_status dev_alloc(rb200_handle* h, T** p, size_t count) {
     return RB200_OK;
 }
 
+void free_graph(rb200_handle* h) {
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    h->graph_exec = nullptr;
+    h->graph_q = nullptr;
+    h->graph_dq = nullptr;
+}
+
 void free_all(rb200_handle* h) {
+    free_graph(h);
+    if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
+    h->cap_stream = nullptr;
     void* ptrs[] = {h->d_elem_geo, h->d_vgeo, h->d_sgeo,    h->d_w,    h->d_nbr,   h->d_qtmp,
                     h->d_dq32,     h->d_hq,   h->d_hdq,     h->d_partial, h->d_sums, h->d_status};
     for (void* p : ptrs)
@@ -161,14 +179,12 @@ StageArgs base_args(const rb200_handle* h) {
     return a;
 }
 
-rb200_status run_steps(rb200_handle* h, double* q, void* dq, double dt, int32_t nsteps, cudaStream_t st) {
-    const size_t nstate = (size_t)h->np * h->ns * h->E;
-    if (!h->d_qtmp) {
-        rb200_status s = dev_alloc(h, &h->d_qtmp, nstate);
-        if (s != RB200_OK) return s;
-    }
+// Enqueues `nsteps` LSRK(5,4) steps with q_in/q_out alternating between q and the
+// handle's second state buffer; returns the buffer holding the result.
+rb200_status enqueue_steps(rb200_handle* h, double* q, void* dq, double dt, int32_t nsteps, cudaStream_t st,
+                           double** result) {
     StageArgs a = base_args(h);
-    a.dq = h->prec == RB200_PRECISION_FP32_BULK ? (void*)h->d_dq32 : dq;
+    a.dq = dq;
     double* cur = q;
     double* oth = h->d_qtmp;
     for (int32_t step = 0; step < nsteps; ++step) {
@@ -184,6 +200,58 @@ rb200_status run_steps(rb200_handle* h, double* q, void* dq, double dt, int32_t 
             cur = oth;
             oth = t;
         }
+    }
+    *result = cur;
+    return RB200_OK;
+}
+
+rb200_status run_steps(rb200_handle* h, double* q, void* dq, double dt, int32_t nsteps, cudaStream_t st) {
+    const size_t nstate = (size_t)h->np * h->ns * h->E;
+    if (!h->d_qtmp) {
+        rb200_status s = dev_alloc(h, &h->d_qtmp, nstate);
+        if (s != RB200_OK) return s;
+    }
+    if (h->prec == RB200_PRECISION_FP32_BULK) dq = h->d_dq32;
+    double* cur = q;
+    rb200_status rs;
+    int32_t done = 0;
+    if (h->use_graphs && nsteps >= 4) {
+        // two steps (an even number of stages, so the state is back in q) run eagerly:
+        // kernel attributes get configured outside the capture
+        if ((rs = enqueue_steps(h, q, dq, dt, 2, st, &cur)) != RB200_OK) return rs;
+        done = 2;
+        if (!h->graph_exec || h->graph_q != q || h->graph_dq != dq || h->graph_dt != dt) {
+            free_graph(h);
+            cudaError_t e = cudaSuccess;
+            if (!h->cap_stream) e = cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking);
+            if (e != cudaSuccess) return cuda_fail(h, e, "graph stream");
+            cudaGraph_t graph = nullptr;
+            e = cudaStreamBeginCapture(h->cap_stream, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) return cuda_fail(h, e, "graph capture");
+            double* gres = nullptr;
+            rs = enqueue_steps(h, q, dq, dt, 2, h->cap_stream, &gres);
+            e = cudaStreamEndCapture(h->cap_stream, &graph);
+            if (rs != RB200_OK) {
+                if (graph) cudaGraphDestroy(graph);
+                return rs;
+            }
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&h->graph_exec, graph, 0);
+            if (graph) cudaGraphDestroy(graph);
+            if (e != cudaSuccess) {
+                h->graph_exec = nullptr;
+                return cuda_fail(h, e, "graph instantiate");
+            }
+            h->graph_q = q;
+            h->graph_dq = dq;
+            h->graph_dt = dt;
+        }
+        for (; done + 2 <= nsteps; done += 2) {
+            cudaError_t e = cudaGraphLaunch(h->graph_exec, st);
+            if (e != cudaSuccess) return cuda_fail(h, e, "graph launch");
+        }
+    }
+    if (done < nsteps) {
+        if ((rs = enqueue_steps(h, q, dq, dt, nsteps - done, st, &cur)) != RB200_OK) return rs;
     }
     if (cur != q) {
         cudaError_t e = cudaMemcpyAsync(q, cur, nstate * sizeof(double), cudaMemcpyDeviceToDevice, st);
