@@ -154,6 +154,88 @@ rb200_status rb200_get_info(const rb200_handle* h, int64_t* info, int32_t n);
 rb200_status rb200_weighted_sums_noalloc(const double* q, const double* MJ, int32_t np, int32_t ns,
                                          int64_t num_elements, double* sums_out, void* stream);
 
+/* ------------------------------------------------------------------------------------
+ * Serving loop: many independent brick solves on one GPU (no counterpart in the
+ * reference, whose drivers run one solve!(q, timeend, LSRK54(dg, q, dt)) per process,
+ * odesolvers.jl:9-30).
+ *
+ * A server owns one device arena, allocated in rb200_server_create.  It admits submitted
+ * solves in FIFO order as their footprint fits, and a request that does not fit yet lets
+ * later ones pass.  A solve's footprint is 2 state buffers + the LSRK register + 32 B of
+ * geometry and 8*dim B of connectivity per element.  Admitted solves advance one
+ * LSRK(5,4) step per tick, batched with every running solve of the same class:
+ *   class = (dim, nq, law, volume form and flux, surface flux, precision, gamma,
+ *            advection velocity, D, w).
+ * A finished solve's state is copied to q_out.  A solve's result does not depend on the
+ * solves it shares launches with: it equals the same solve run alone, bit for bit.
+ *
+ * Served configurations are unwarped bricks (affine elements): dim 2 or 3, nq 4, 6 or 8.
+ *   - Advection: weak form.
+ *   - Euler: flux differencing with Kennedy-Gruber.
+ * The surface flux is Rusanov or central, and the precision is FP64 or FP32_BULK.
+ * ------------------------------------------------------------------------------------ */
+typedef struct rb200_request {
+    int32_t abi_version;       /* RB200_ABI_VERSION */
+    int32_t dim;               /* 2 or 3 */
+    int32_t nq;                /* 4, 6 or 8 */
+    int32_t law;               /* RB200_LAW_* */
+    int64_t num_elements;      /* E */
+    int32_t volume_form;       /* RB200_FORM_* */
+    int32_t volume_flux;       /* RB200_FLUX_KENNEDY_GRUBER for Euler */
+    int32_t surface_flux;      /* RB200_FLUX_RUSANOV or RB200_FLUX_CENTRAL */
+    int32_t precision;         /* RB200_PRECISION_* */
+    double gamma;
+    double advection_velocity[3];
+    const double* D;           /* (nq, nq) col-major derivative matrix */
+    const double* w;           /* (nq) LGL weights */
+    const double* r;           /* (nq) LGL points; needed when q0 is NULL */
+    const double* elem_geo;    /* (4, E): dr/dx, ds/dy, dt/dz (0 in 2-D), J of each element */
+    const int32_t* neighbors;  /* (2*dim, E): element across faces -x,+x,-y,+y(,-z,+z),
+                                  0-based; -1 = boundary face (exterior state = interior) */
+    const double* q0;          /* host (nq^dim, Ns, E) initial state, copied during submit;
+                                  NULL = initial data evaluated on the device (init_kind) */
+    int32_t init_kind;         /* with q0 NULL: 1 = Euler isentropic vortex (init_params:
+                                  strength, u0, centre x, centre y); 2 = advection
+                                  sin(2 pi x)sin(2 pi y)[sin(2 pi z)] + Gaussian (width,
+                                  centre xyz) */
+    double init_params[8];
+    const double* corners;     /* (2, dim, E): lower corner and width of each element along
+                                  each direction (node x = fma(width, (r+1)/2, corner)) */
+    double dt;
+    int32_t nsteps;            /* LSRK54 steps */
+    double* q_out;             /* host (nq^dim, Ns, E) final state; NULL = discard.  Must
+                                  stay valid until rb200_server_wait returns */
+} rb200_request;
+
+typedef struct rb200_server rb200_server;
+
+/* Allocates the arena (arena_bytes of device memory on `device`) and starts the loop. */
+rb200_status rb200_server_create(int32_t device, uint64_t arena_bytes, rb200_server** out);
+
+/* Queues one solve; the request's host arrays are copied before return.  ticket: id for
+ * rb200_server_wait.  RB200_ERR_OOM: the footprint exceeds the whole arena.  Thread-safe. */
+rb200_status rb200_server_submit(rb200_server* s, const rb200_request* req, uint64_t* ticket);
+
+/* Blocks until the solve finishes (q_out written) or timeout_s passes (RB200_ERR_TIMEOUT;
+ * the ticket stays valid).  latency_s: submit-to-finish wall time.  Thread-safe. */
+rb200_status rb200_server_wait(rb200_server* s, uint64_t ticket, double timeout_s, double* latency_s);
+
+/* out[0..8]: completed, submitted, running, queued, DOF updates (nodes * Ns * 5 stages *
+ * steps of completed solves), arena bytes in use, peak arena bytes, class ticks, seconds
+ * from the first submit to the last completion.  Returns the server's error status. */
+rb200_status rb200_server_stats(rb200_server* s, double* out, int32_t n);
+
+/* Per class, 4 values: dim, nq, internal kernel combination, elements per CTA that the
+ * autotuner chose (0 while it is still timing).  Unused entries are 0. */
+rb200_status rb200_server_class_tiles(rb200_server* s, int32_t* out, int32_t n);
+
+/* Message of the error that stopped the server (empty if none).  Valid until destroy. */
+const char* rb200_server_last_error(rb200_server* s);
+
+/* Stops the loop (unfinished solves are abandoned) and frees everything.  No call on
+ * the server may run concurrently with or after this one. */
+rb200_status rb200_server_destroy(rb200_server* s);
+
 /* Last error message of a handle (empty if none); static text for NULL. */
 const char* rb200_last_error(const rb200_handle* h);
 const char* rb200_status_string(rb200_status s);

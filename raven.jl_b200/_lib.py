@@ -38,9 +38,17 @@ EXPORTED = [
     "rb200_set_kernel_path",
     "rb200_sync_status",
     "rb200_weighted_sums_noalloc",
+    "rb200_server_create",
+    "rb200_server_submit",
+    "rb200_server_wait",
+    "rb200_server_stats",
+    "rb200_server_class_tiles",
+    "rb200_server_last_error",
+    "rb200_server_destroy",
     "rb200_last_error",
     "rb200_status_string",
 ]
+_STRING_RESULT = ("rb200_last_error", "rb200_status_string", "rb200_server_last_error")
 
 
 class Desc(ctypes.Structure):
@@ -64,6 +72,36 @@ class Desc(ctypes.Structure):
         ("vmapP", ctypes.c_void_p),
         ("boundary_codes", ctypes.c_void_p),
         ("device", ctypes.c_int32),
+    ]
+
+
+class Request(ctypes.Structure):
+    """Mirror of rb200_request (one solve submitted to a server)."""
+
+    _fields_ = [
+        ("abi_version", ctypes.c_int32),
+        ("dim", ctypes.c_int32),
+        ("nq", ctypes.c_int32),
+        ("law", ctypes.c_int32),
+        ("num_elements", ctypes.c_int64),
+        ("volume_form", ctypes.c_int32),
+        ("volume_flux", ctypes.c_int32),
+        ("surface_flux", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("gamma", ctypes.c_double),
+        ("advection_velocity", ctypes.c_double * 3),
+        ("D", ctypes.c_void_p),
+        ("w", ctypes.c_void_p),
+        ("r", ctypes.c_void_p),
+        ("elem_geo", ctypes.c_void_p),
+        ("neighbors", ctypes.c_void_p),
+        ("q0", ctypes.c_void_p),
+        ("init_kind", ctypes.c_int32),
+        ("init_params", ctypes.c_double * 8),
+        ("corners", ctypes.c_void_p),
+        ("dt", ctypes.c_double),
+        ("nsteps", ctypes.c_int32),
+        ("q_out", ctypes.c_void_p),
     ]
 
 
@@ -104,8 +142,16 @@ def lib():
     L.rb200_last_error.restype = ctypes.c_char_p
     L.rb200_status_string.argtypes = [ctypes.c_int]
     L.rb200_status_string.restype = ctypes.c_char_p
+    L.rb200_server_create.argtypes = [I32, ctypes.c_uint64, ctypes.POINTER(P)]
+    L.rb200_server_submit.argtypes = [P, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)]
+    L.rb200_server_wait.argtypes = [P, ctypes.c_uint64, D, ctypes.POINTER(D)]
+    L.rb200_server_stats.argtypes = [P, P, I32]
+    L.rb200_server_class_tiles.argtypes = [P, P, I32]
+    L.rb200_server_last_error.argtypes = [P]
+    L.rb200_server_last_error.restype = ctypes.c_char_p
+    L.rb200_server_destroy.argtypes = [P]
     for name in EXPORTED:
-        if name not in ("rb200_last_error", "rb200_status_string"):
+        if name not in _STRING_RESULT:
             getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

@@ -37,7 +37,10 @@ def _sources():
     for d, q in DIMS_NQS:
         units.append((os.path.join(CSRC, "stage_inst.cu"), os.path.join(BUILD, f"stage_d{d}_q{q}.o"),
                       [f"-DRB_DIM={d}", f"-DRB_NQ={q}"]))
-    for name in ("dispatch", "reduce", "pipelined_inst", "api"):
+    for d in (2, 3):
+        units.append((os.path.join(CSRC, "serve_inst.cu"), os.path.join(BUILD, f"serve_d{d}.o"),
+                      [f"-DRB_SERVE_DIM={d}"]))
+    for name in ("dispatch", "reduce", "pipelined_inst", "serve", "api"):
         units.append((os.path.join(CSRC, f"{name}.cu"), os.path.join(BUILD, f"{name}.o"), []))
     return units
 

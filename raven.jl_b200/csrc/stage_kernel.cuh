@@ -31,12 +31,13 @@ struct IPow<N, 0> {
     static constexpr int v = 1;
 };
 
-template <int DIM, int NQ>
+// EPBX > 0 overrides the default number of elements per CTA (the serving loop's tiles).
+template <int DIM, int NQ, int EPBX = 0>
 struct Shape {
     static constexpr int NP = IPow<NQ, DIM>::v;
     static constexpr int NFP = IPow<NQ, DIM - 1>::v;
     static constexpr int NF = 2 * DIM;
-    static constexpr int EPB = NP >= 256 ? 1 : 256 / NP;  // elements per CTA
+    static constexpr int EPB = EPBX > 0 ? EPBX : (NP >= 256 ? 1 : 256 / NP);  // elements per CTA
     static constexpr int THREADS = EPB * NP;
 };
 
@@ -53,9 +54,9 @@ struct CSize {
                                                     : DIM + 3;         // EC: rho, u, b, |u|^2
 };
 
-template <int DIM, int NQ, int COMBO, int GEOM, typename T>
+template <int DIM, int NQ, int COMBO, int GEOM, typename T, int EPBX = 0>
 struct KernelCfg {
-    using S = Shape<DIM, NQ>;
+    using S = Shape<DIM, NQ, EPBX>;
     using C = CSize<COMBO, DIM>;
     static constexpr int NLG = GEOM == GEOM_AFFINE ? DIM : DIM * DIM;
     static constexpr size_t smem = (size_t)S::EPB * (C::NAUX + NLG) * S::NP * sizeof(T);
@@ -88,25 +89,42 @@ __device__ __forceinline__ T logavg(T a, T b) {
     return (a + b) / (T(2) * F);
 }
 
-template <int DIM, int NQ, int COMBO, int GEOM, typename T>
-__global__ void __launch_bounds__(Shape<DIM, NQ>::THREADS, 1)
-    stage_kernel(const __grid_constant__ StageArgs A) {
-    using S = Shape<DIM, NQ>;
+// Buffers of the element being updated: the DGSEM handle takes them from StageArgs,
+// the serving loop from each solve's descriptor.
+struct ElemPtrs {
+    const double* q_in;
+    double* q_out;
+    void* dq;
+    const double* elem_geo;
+    const double* vgeo;
+    const double* sgeo;
+    const int32_t* nbr;
+    double rkb_dt;
+};
+
+__device__ __forceinline__ ElemPtrs elem_ptrs(const StageArgs& A) {
+    return ElemPtrs{A.q_in, A.q_out, A.dq, A.elem_geo, A.vgeo, A.sgeo, A.nbr, A.rkb_dt};
+}
+
+// One element per group of Np threads: the whole fused stage for element e.  All
+// threads of the CTA must call it (it contains a barrier); inactive groups pass
+// active = false.
+template <int DIM, int NQ, int COMBO, int GEOM, typename T, int EPBX>
+__device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs& P, const int64_t e,
+                                              const bool active, unsigned char* smem_raw) {
+    using S = Shape<DIM, NQ, EPBX>;
     using C = CSize<COMBO, DIM>;
-    using K = KernelCfg<DIM, NQ, COMBO, GEOM, T>;
+    using K = KernelCfg<DIM, NQ, COMBO, GEOM, T, EPBX>;
     constexpr int NP = S::NP, NFP = S::NFP, NF = S::NF, EPB = S::EPB;
     constexpr int NS = C::NS, NAUX = C::NAUX, NLG = K::NLG;
     constexpr bool AFF = GEOM == GEOM_AFFINE;
 
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     T* s_aux = reinterpret_cast<T*>(smem_raw);
     T* s_lg = s_aux + EPB * NAUX * NP;
 
     const int tid = threadIdx.x;
     const int el = tid / NP;
     const int n = tid - el * NP;
-    const int64_t e = (int64_t)blockIdx.x * EPB + el;
-    const bool active = e < A.E;
     int id[3];
     id[0] = n % NQ;
     id[1] = DIM > 1 ? (n / NQ) % NQ : 0;
@@ -122,14 +140,14 @@ __global__ void __launch_bounds__(Shape<DIM, NQ>::THREADS, 1)
     double drdx[3] = {0.0, 0.0, 0.0};
 
     if (active) {
-        const double* qe = A.q_in + (size_t)e * NS * NP;
+        const double* qe = P.q_in + (size_t)e * NS * NP;
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
             qd[s] = __ldg(qe + s * NP + n);
             q[s] = (T)qd[s];
         }
         if constexpr (AFF) {
-            const double* eg = A.elem_geo + 4 * e;
+            const double* eg = P.elem_geo + 4 * e;
 #pragma unroll
             for (int d = 0; d < DIM; ++d) drdx[d] = __ldg(eg + d);
             J = __ldg(eg + 3);
@@ -142,7 +160,7 @@ __global__ void __launch_bounds__(Shape<DIM, NQ>::THREADS, 1)
 #pragma unroll
             for (int d = 0; d < DIM; ++d) lg[d] = (T)(wJ * drdx[d]);
         } else {
-            const double* vg = A.vgeo + (size_t)e * (DIM * DIM + 2) * NP;  // fields: wJ*dRdX rows, MJI, MJ
+            const double* vg = P.vgeo + (size_t)e * (DIM * DIM + 2) * NP;  // fields: wJ*dRdX rows, MJI, MJ
 #pragma unroll
             for (int c = 0; c < DIM * DIM; ++c) lg[c] = (T)__ldg(vg + c * NP + n);
             mji = __ldg(vg + DIM * DIM * NP + n);
@@ -343,11 +361,11 @@ __global__ void __launch_bounds__(Shape<DIM, NQ>::THREADS, 1)
         T v = acc[s] * mjiT;
         if (A.mode == MODE_STAGE) {
             T old;
-            if (sizeof(T) == 4) old = (T) reinterpret_cast<const float*>(A.dq)[node0 + s * NP];
-            else old = (T) reinterpret_cast<const double*>(A.dq)[node0 + s * NP];
+            if (sizeof(T) == 4) old = (T) reinterpret_cast<const float*>(P.dq)[node0 + s * NP];
+            else old = (T) reinterpret_cast<const double*>(P.dq)[node0 + s * NP];
             v = (T)A.rka * old + v;
         } else if (A.mode == MODE_TENDENCY_INC) {
-            v = (T)(reinterpret_cast<const double*>(A.dq)[node0 + s * NP] + (double)v);
+            v = (T)(reinterpret_cast<const double*>(P.dq)[node0 + s * NP] + (double)v);
         }
         t[s] = v;
     }
@@ -362,11 +380,11 @@ __global__ void __launch_bounds__(Shape<DIM, NQ>::THREADS, 1)
             if ((side == 0 && idd != 0) || (side == 1 && idd != NQ - 1)) continue;
             const int f = 2 * dir + side;
             const int stride = dir == 0 ? 1 : (dir == 1 ? NQ : NQ * NQ);
-            const int ne = __ldg(A.nbr + (size_t)NF * e + f);
+            const int ne = __ldg(P.nbr + (size_t)NF * e + f);
             T qp[NS];
             if (ne >= 0) {
                 const int nn = n + (side == 0 ? (NQ - 1) * stride : -(NQ - 1) * stride);
-                const double* qn = A.q_in + (size_t)ne * NS * NP + nn;
+                const double* qn = P.q_in + (size_t)ne * NS * NP + nn;
 #pragma unroll
                 for (int s = 0; s < NS; ++s) qp[s] = (T)__ldg(qn + s * NP);
             } else {
@@ -392,7 +410,7 @@ __global__ void __launch_bounds__(Shape<DIM, NQ>::THREADS, 1)
                     wsJ = (sJ * A.w[i1]) * A.w[i2];
                 }
             } else {
-                const double* sg = A.sgeo + ((size_t)e * NF * NFP + (size_t)f * NFP + j) * (DIM + 1);
+                const double* sg = P.sgeo + ((size_t)e * NF * NFP + (size_t)f * NFP + j) * (DIM + 1);
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) nv[d] = (T)__ldg(sg + d);
                 wsJ = __ldg(sg + DIM);
@@ -460,14 +478,23 @@ __global__ void __launch_bounds__(Shape<DIM, NQ>::THREADS, 1)
     if (stage) {
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
-            if (sizeof(T) == 4) reinterpret_cast<float*>(A.dq)[node0 + s * NP] = (float)t[s];
-            else reinterpret_cast<double*>(A.dq)[node0 + s * NP] = (double)t[s];
-            A.q_out[node0 + s * NP] = qd[s] + A.rkb_dt * (double)t[s];
+            if (sizeof(T) == 4) reinterpret_cast<float*>(P.dq)[node0 + s * NP] = (float)t[s];
+            else reinterpret_cast<double*>(P.dq)[node0 + s * NP] = (double)t[s];
+            P.q_out[node0 + s * NP] = qd[s] + P.rkb_dt * (double)t[s];
         }
     } else {
 #pragma unroll
-        for (int s = 0; s < NS; ++s) reinterpret_cast<double*>(A.dq)[node0 + s * NP] = (double)t[s];
+        for (int s = 0; s < NS; ++s) reinterpret_cast<double*>(P.dq)[node0 + s * NP] = (double)t[s];
     }
+}
+
+template <int DIM, int NQ, int COMBO, int GEOM, typename T>
+__global__ void __launch_bounds__(Shape<DIM, NQ>::THREADS, 1)
+    stage_kernel(const __grid_constant__ StageArgs A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using S = Shape<DIM, NQ>;
+    const int64_t e = (int64_t)blockIdx.x * S::EPB + threadIdx.x / S::NP;
+    stage_element<DIM, NQ, COMBO, GEOM, T, 0>(A, elem_ptrs(A), e, e < A.E, smem_raw);
 }
 
 template <int DIM, int NQ, int COMBO, int GEOM, typename T>
