@@ -10,6 +10,12 @@ LSRK(5,4) time step (5 fused stage kernels).  The 1.3 GB state is larger than L2
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
 
+Serving workload (--workload serve_poisson_mix_fp32bulk): a seeded stream of --requests
+independent solves arriving as a Poisson process at --rate per second (dim 2 or 3,
+advection or Euler, N in {3, 5, 7}, 8-64 (2-D) or 4-32 (3-D) elements per side,
+50-500 LSRK(5,4) steps, FP32 bulk) is replayed against the serving loop; the line
+reports p50/p99 latency and solves/s beside the DOF-update rate.
+
 Multi-GPU (torchrun): every rank runs an independent replica of the workload (the
 single-grid path has no cross-rank exchange on one rank); time is the max over ranks.
 """
@@ -39,6 +45,7 @@ WORKLOADS = {
     "adv2d_weak_n4_16_fp64": dict(dim=2, N=4, K=16, L=1.0, law="advection", vflux="weak", precision="fp64",
                                   warp=False),
 }
+SERVE_WORKLOAD = "serve_poisson_mix_fp32bulk"
 DEFAULT = "euler3d_kg_n7_32_fp64"
 METRIC = "DOF-updates/s per RHS"
 UNIT = "DOF-updates/s"
@@ -296,16 +303,247 @@ def run_reference(args, w):
     return 0
 
 
+def serve_bytes_per_dof(precision):
+    """Algorithmic HBM bytes per DOF update (per RHS) of the batched stage kernel,
+    averaged over the 5 stages: q read + write (16 B), dq write (every stage) and dq
+    read (stages 2-5); the per-element geometry is negligible (32 B per element)."""
+    dqb = 4 if precision == "fp32_bulk" else 8
+    return 16 + dqb + 4 * dqb / 5
+
+
+def serve_cpu_sample(arrivals, max_seconds=20.0):
+    """The oracle on the host cores over a bounded sample of the stream: the solves of
+    the stream in order, each run for at most 5 steps, until ~max_seconds have passed."""
+    import numpy as np
+
+    import oracle as O
+
+    done_dof, t0, solves = 0, time.perf_counter(), 0
+    for a in arrivals:
+        s = a.spec
+        og = O.Grid(s.dim, s.nq, list(s.K), list(s.lo), list(s.hi), [1] * s.dim)
+        if s.law == 1:
+            law = O.Law(O.LAW_EULER, s.dim, form=O.FORM_FLUXDIFF, volume_flux=O.FLUX_KG)
+            q = og.initial_condition(law, 4, [s.init_params[0], s.init_params[1], 5.0, 5.0])
+        else:
+            law = O.Law(O.LAW_ADVECTION, s.dim, adv=list(s.advection_velocity[: s.dim]))
+            q = og.initial_condition(law, 3, list(s.init_params[:4]))
+        dq = og.state(law)
+        n = min(5, s.nsteps)
+        for i in range(n):
+            og.lsrk54_step(law, q, dq, i * s.dt, s.dt)
+        done_dof += og.np * og.E * law.ns * 5 * n
+        solves += 1
+        if time.perf_counter() - t0 >= max_seconds:
+            break
+    el = time.perf_counter() - t0
+    return {
+        "value": done_dof / el,
+        "unit": UNIT,
+        "cores": O.num_threads(),
+        "kind": "port",
+        "sample": f"the first {solves} solves of the same seeded stream, 5 LSRK(5,4) steps each, FP64 C++ "
+                  f"restatement of Raven's CPU path, OpenMP over elements, {el:.1f} s including grid set-up",
+    }
+
+
+def run_serving(args):
+    """The serving loop under the seeded Poisson stream (one server per GPU; replicas)."""
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        return run_serving_reference(args)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    rb = load_product()
+    from raven_b200 import serving as S
+
+    arrivals = S.poisson_mix(args.seed, args.requests, rate=args.rate)
+    srv = S.Server(arena_bytes=48 << 30, device=local)
+    # warm-up: one short solve per class of the stream (creates the class, captures its
+    # graphs and lets the autotuner pick its tile), then W more rounds of the same
+    warm = []
+    for dim in (2, 3):
+        for nq in (4, 6, 8):
+            for law in (0, 1):
+                f = S.vortex_spec if law == 1 else S.wave_spec
+                warm.append(f(dim, nq, (4,) * dim if dim == 3 else (8, 8), 10,
+                              precision=rb._lib.PRECISION_FP32_BULK))
+    for _ in range(max(1, args.warmup)):
+        for t in [srv.submit(sp, keep_result=False) for sp in warm]:
+            srv.wait(t)
+    srv.close()
+    # the timed stream on a fresh server whose classes are warm in the process (module
+    # loading, kernel attributes); class graphs are captured again at first use
+    srv = S.Server(arena_bytes=48 << 30, device=local)
+    for t in [srv.submit(sp, keep_result=False) for sp in warm]:
+        srv.wait(t)
+    base = srv.stats()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    sampler = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local)
+    sampler.start()
+    time.sleep(0.3)
+    t0 = time.perf_counter()
+    res = S.run_load(srv, arrivals, keep_results=True)
+    wall = time.perf_counter() - t0
+    sampler.stop()
+    st = srv.stats()
+    tiles = srv.class_tiles()
+    srv.close()
+    lat = res["latencies"]
+    dof = float(sum(a.spec.dof_updates() for a in arrivals))
+    first_t = arrivals[0].t
+    # busy time of the stream: first arrival to last completion (the server's clock)
+    busy = wall
+    if dist is not None:
+        t = torch.tensor([busy], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        busy = float(t.item())
+    value = world * dof / busy
+    ticks = st["ticks"] - base["ticks"]
+    peak, peak_kind = measured_peaks()
+    bpd = serve_bytes_per_dof("fp32_bulk")
+    achieved = dof * bpd / busy / 1e9
+    h2d = sum(a.spec.num_elements * (32 + 8 * a.spec.dim + 16 * a.spec.dim) for a in arrivals)
+    d2h = sum(a.spec.np * a.spec.ns * a.spec.num_elements * 8 for a in arrivals)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = serve_cpu_sample(arrivals)
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.requests,
+            "warmup": args.warmup,
+            "ms_per_step": busy / args.requests * 1e3,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32+f64",
+            "data": "synthetic",
+            "config": {
+                "workload": SERVE_WORKLOAD,
+                "requests": args.requests,
+                "arrival_rate_per_s": args.rate,
+                "seed": args.seed,
+                "dims": [2, 3],
+                "equations": ["advection (weak form)", "euler (kennedy-gruber flux differencing)"],
+                "polynomial_orders": [3, 5, 7],
+                "elements_per_side": {"2d": [8, 64], "3d": [4, 32], "distribution": "log-uniform"},
+                "lsrk_steps": [50, 500],
+                "precision": "fp32_bulk",
+                "initial_data": "sine_plus_gaussian (advection), isentropic vortex strength 3 (euler)",
+                "step_meaning": "one request of the stream; value = DOF updates of all requests / busy time",
+                "l2_flush": "not needed: the running solves' state (GBs) is larger than L2",
+                "parallelism": "replicas",
+            },
+            "serving": {
+                "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                "mean_ms": float(lat.mean() * 1e3),
+                "max_ms": float(lat.max() * 1e3),
+                "solves_per_s": world * args.requests / busy,
+                "busy_seconds": busy,
+                "stream_seconds": arrivals[-1].t - first_t,
+                "total_dof_updates": dof,
+                "arena_peak_bytes": st["arena_peak"],
+                "class_tiles": [list(t) for t in tiles],
+            },
+            "roofline": {
+                "bound": "hbm",
+                "achieved": achieved,
+                "peak": peak,
+                "unit": "GB/s",
+                "frac": achieved / peak,
+                "traffic": None,
+                "peak_source": peak_kind,
+                "kernel": "batched_stage_kernel (all running solves of a class per launch)",
+                "algorithmic_bytes_per_dof_update": bpd,
+            },
+            "cpu_baseline": cpu,
+            "e2e": {
+                "value": value,
+                "unit": UNIT,
+                "h2d_bytes_per_step": h2d / args.requests,
+                "d2h_bytes_per_step": d2h / args.requests,
+                "note": "the value is already end to end: host requests in, final states copied to host",
+            },
+            "gpu_launches": int(6 * ticks + args.requests),
+            "clocks": sampler.summary(),
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_serving_reference(args):
+    """Reference arm of the serving workload: the oracle port runs the stream's solves
+    one after another on the host cores (the reference has no serving loop), each
+    truncated to its first 5 steps; value = DOF updates per second."""
+    import oracle as O
+
+    O.build()
+    rb = load_product()
+    from raven_b200 import serving as S
+
+    arrivals = S.poisson_mix(args.seed, args.requests, rate=args.rate)
+    cpu = serve_cpu_sample(arrivals, max_seconds=60.0)
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": cpu["value"],
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": args.requests,
+        "warmup": args.warmup,
+        "ms_per_step": None,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": SERVE_WORKLOAD, "requests": args.requests, "arrival_rate_per_s": args.rate,
+                   "seed": args.seed},
+        "cpu_baseline": cpu,
+        "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main(argv=None):
     p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=3)
-    p.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
+    p.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS) + [SERVE_WORKLOAD])
+    p.add_argument("--requests", type=int, default=200, help="serving workload: solves in the timed stream")
+    p.add_argument("--rate", type=float, default=200.0, help="serving workload: arrivals per second")
+    p.add_argument("--seed", type=int, default=0, help="serving workload: stream seed")
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
     args = p.parse_args(argv)
+    if args.workload == SERVE_WORKLOAD:
+        return run_serving(args)
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
         return run_reference(args, w)
