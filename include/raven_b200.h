@@ -236,6 +236,57 @@ const char* rb200_server_last_error(rb200_server* s);
  * the server may run concurrently with or after this one. */
 rb200_status rb200_server_destroy(rb200_server* s);
 
+/* ------------------------------------------------------------------------------------
+ * Utilities Raven exports beside the DGSEM path: Kron (kron.jl), gather!/scatter!
+ * (gatherscatter.jl) and decode (facecode.jl).  Device arrays, asynchronous on
+ * `stream`.  Results are bit-identical to the reference's arithmetic.
+ * ------------------------------------------------------------------------------------ */
+
+/* Kron(args) * f  (kron.jl:15-387).  args = (X_n, ..., X_1) as in Julia, X_1 acting on
+ * the fastest index.  mats[d] = X_{d+1}: a HOST column-major rows[d] x cols[d] matrix
+ * of `dtype` (0 = double, 1 = float), or NULL for Eye(rows[d]) (cols[d] = rows[d]);
+ * rows, cols <= 16.  The node index of f runs over prod(cols) entries, that of the
+ * result over prod(rows); element (node, comp, col) of f is at
+ * in[node*in_strides[0] + comp*in_strides[1] + col*in_strides[2]], likewise for out.
+ * A GridArray parent (Np, Ns, E) has strides (1, Np, Np*Ns) and ncomp = Ns; an array of
+ * SVector{C} columns has strides (C, 1, C*Np) and ncomp = C.  The arithmetic is that
+ * of the method Julia dispatches to:
+ *   - all factors Eye: a copy;
+ *   - one dense factor: one fma chain;
+ *   - otherwise: the generic nested sum, with Eye entries used as 0/1 values. */
+rb200_status rb200_kron_apply(int32_t nfactors, const void* const* mats, const int32_t* rows, const int32_t* cols,
+                              int32_t dtype, const void* in, const int64_t* in_strides, void* out,
+                              const int64_t* out_strides, int64_t ncols, int32_t ncomp, void* stream);
+
+/* Where element i, component c of an array lives:
+ *   (i % block) * node_stride + (i / block) * block_stride + c * comp_stride.
+ * A discontinuous GridArray (Np, Ns, E) is {Np, 1, Np*Ns, Np}.  A continuous one
+ * (Ns, Nc) is {Nc, Ns, 0, 1}. */
+typedef struct rb200_layout {
+    int64_t block, node_stride, block_stride, comp_stride;
+} rb200_layout;
+
+/* scatter!(dest, src, dtoc)  (gatherscatter.jl:17-34): dest[i] = src[dtoc[i]] for
+ * i < n, for every component.  dtoc: device int64, 1-based (discontinuoustocontinuous).
+ * dtype: 0 double, 1 float, 2 int64, 3 int32. */
+rb200_status rb200_scatter(void* dest, const rb200_layout* dest_layout, const void* src,
+                           const rb200_layout* src_layout, const int64_t* dtoc, int64_t n, int32_t ncomp,
+                           int32_t dtype, void* stream);
+
+/* gather!(dest, src, ctod; op, init)  (gatherscatter.jl:36-103): for each column j of
+ * the CSC matrix ctod (continuoustodiscontinuous; colptr: ncols+1, rowval: nnz, device
+ * int64, 1-based), dest[j] = op(...op(init, src[r_1])..., src[r_k]) over the column's
+ * rows in stored order.  op: 0 = +, 1 = min, 2 = max (Julia semantics: NaN propagates,
+ * -0.0 < 0.0).  init is converted to dtype. */
+rb200_status rb200_gather(void* dest, const rb200_layout* dest_layout, const void* src,
+                          const rb200_layout* src_layout, const int64_t* colptr, const int64_t* rowval, int64_t ncols,
+                          int32_t ncomp, int32_t dtype, int32_t op, double init, void* stream);
+
+/* decode(facecode)  (facecode.jl:1-140) for n device codes.  bits = 8 (2-D quadrant
+ * codes, uint8): out (4, n) hanging-face values.  bits = 16 (3-D octant codes,
+ * uint16): out (18, n) = 6 hanging-face then 12 hanging-edge values. */
+rb200_status rb200_decode_facecodes(const void* codes, int32_t bits, int64_t n, uint8_t* out, void* stream);
+
 /* Last error message of a handle (empty if none); static text for NULL. */
 const char* rb200_last_error(const rb200_handle* h);
 const char* rb200_status_string(rb200_status s);

@@ -1,12 +1,15 @@
 """TEST INFRASTRUCTURE ONLY -- the CPU FP64 oracle for the DGSEM tendency + LSRK(5,4) path.
 
 This package wraps ``oracle/oracle.cpp`` (a C++ restatement of Raven.jl's brick grid,
-DGSEM tendency and LSRK(5,4) stepper, citations in that file).  Only ``tests/``,
+DGSEM tendency and LSRK(5,4) stepper, citations in that file) and
+``oracle/utilities.cpp`` (Kron, gather!/scatter! and decode).  Only ``tests/``,
 ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` may import it; the
 product package (``raven.jl_b200``) never does.
 
 The oracle is pinned against the reference's own golden values
-(``tests/golden/reference_goldens.json``, produced by ``tests/golden/make_goldens.py``).
+(``tests/golden/reference_goldens.json``, produced by ``tests/golden/make_goldens.py``,
+and ``tests/golden/facecode_goldens.json``, produced by
+``tests/golden/make_facecode_goldens.py``).
 """
 
 import ctypes
@@ -26,18 +29,18 @@ WARP_NONE, WARP_SINE, WARP_IDENTITY_CURVED = 0, 1, 2
 
 def build(force=False):
     """Compile oracle.cpp into oracle/_build/liboracle.so (g++, -ffp-contract=off, OpenMP)."""
-    src = os.path.join(HERE, "oracle.cpp")
+    srcs = [os.path.join(HERE, "oracle.cpp"), os.path.join(HERE, "utilities.cpp")]
     hdr = os.path.join(HERE, "oracle.h")
     os.makedirs(os.path.dirname(LIB_PATH), exist_ok=True)
     if (
         not force
         and os.path.exists(LIB_PATH)
-        and os.path.getmtime(LIB_PATH) >= max(os.path.getmtime(src), os.path.getmtime(hdr))
+        and os.path.getmtime(LIB_PATH) >= max([os.path.getmtime(f) for f in srcs] + [os.path.getmtime(hdr)])
     ):
         return LIB_PATH
     cmd = [
         "g++", "-O2", "-std=gnu++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
-        "-fno-fast-math", "-o", LIB_PATH, src, "-lquadmath",
+        "-fno-fast-math", "-o", LIB_PATH, *srcs, "-lquadmath",
     ]
     subprocess.check_call(cmd)
     return LIB_PATH
@@ -80,6 +83,12 @@ def lib():
         L.og_weightednorm.restype = ctypes.c_double
         L.og_weightednorm.argtypes = [P, P, ctypes.c_int, P]
         L.og_integrals.argtypes = [P, P, ctypes.c_int, P]
+        L.og_decode8.argtypes = [P, ctypes.c_int64, P]
+        L.og_decode16.argtypes = [P, ctypes.c_int64, P]
+        L.og_kron_apply_f64.argtypes = [ctypes.c_int, P, P, P, P, P, P, P, ctypes.c_int64, ctypes.c_int]
+        L.og_kron_apply_f32.argtypes = [ctypes.c_int, P, P, P, P, P, P, P, ctypes.c_int64, ctypes.c_int]
+        L.og_scatter_f64.argtypes = [P, P, P, P, P, ctypes.c_int64, ctypes.c_int]
+        L.og_gather_f64.argtypes = [P, P, P, P, P, P, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_double]
         L.og_num_threads.restype = ctypes.c_int
         L.og_set_num_threads.argtypes = [ctypes.c_int]
         _lib = L
@@ -209,3 +218,66 @@ def num_threads():
 
 def set_num_threads(n):
     lib().og_set_num_threads(int(n))
+
+
+# ------------------------------------------------------------------------- utilities
+
+
+def decode(codes):
+    """decode(facecode) for an array of UInt8 (-> (n, 4) hangingface) or UInt16 codes
+    (-> (n, 18): 6 hangingface then 12 hangingedge values)."""
+    codes = np.ascontiguousarray(codes)
+    n = codes.size
+    if codes.dtype == np.uint8:
+        out = np.zeros((n, 4), dtype=np.uint8)
+        lib().og_decode8(_ptr(codes), n, _ptr(out))
+    elif codes.dtype == np.uint16:
+        out = np.zeros((n, 18), dtype=np.uint8)
+        lib().og_decode16(_ptr(codes), n, _ptr(out))
+    else:
+        raise TypeError("facecodes are uint8 (2-D) or uint16 (3-D)")
+    return out
+
+
+def kron_apply(mats, sizes, f, ncomp=1, in_strides=None, out_strides=None, ncol=None):
+    """Kron(args) * f: mats[d] = X_{d+1} (acts on index d, fastest first) or None for
+    Eye(sizes[d]).  f: flat array addressed f[node*sn + comp*sc + col*scol]."""
+    nf = len(mats)
+    dt = f.dtype
+    rows = np.array([m.shape[0] if m is not None else sizes[d] for d, m in enumerate(mats)], dtype=np.int32)
+    cols = np.array([m.shape[1] if m is not None else sizes[d] for d, m in enumerate(mats)], dtype=np.int32)
+    keep = [None if m is None else np.asfortranarray(m, dtype=dt) for m in mats]
+    ptrs = (ctypes.c_void_p * nf)(*[None if m is None else m.ctypes.data for m in keep])
+    nin, nout = int(np.prod(cols)), int(np.prod(rows))
+    if in_strides is None:
+        in_strides = (1, nin, nin * ncomp)
+    if out_strides is None:
+        out_strides = (1, nout, nout * ncomp)
+    if ncol is None:
+        ncol = f.size // (nin * ncomp)
+    out = np.zeros(max(1, out_strides[0] * (nout - 1) + out_strides[1] * (ncomp - 1)
+                       + out_strides[2] * (ncol - 1) + 1), dtype=dt)
+    si = np.array(in_strides, dtype=np.int64)
+    so = np.array(out_strides, dtype=np.int64)
+    fc = np.ascontiguousarray(f)
+    fn = lib().og_kron_apply_f64 if dt == np.float64 else lib().og_kron_apply_f32
+    fn(nf, ptrs, _ptr(rows), _ptr(cols), _ptr(fc), _ptr(si), _ptr(out), _ptr(so), int(ncol), int(ncomp))
+    return out
+
+
+def scatter(dest, dest_layout, src, src_layout, dtoc, ncomp):
+    dl = np.array(dest_layout, dtype=np.int64)
+    sl = np.array(src_layout, dtype=np.int64)
+    d = np.ascontiguousarray(dtoc, dtype=np.int64)
+    lib().og_scatter_f64(_ptr(dest), _ptr(dl), _ptr(src), _ptr(sl), _ptr(d), d.size, int(ncomp))
+    return dest
+
+
+def gather(dest, dest_layout, src, src_layout, colptr, rowval, ncomp, op=0, init=0.0):
+    dl = np.array(dest_layout, dtype=np.int64)
+    sl = np.array(src_layout, dtype=np.int64)
+    cp = np.ascontiguousarray(colptr, dtype=np.int64)
+    rv = np.ascontiguousarray(rowval, dtype=np.int64)
+    lib().og_gather_f64(_ptr(dest), _ptr(dl), _ptr(src), _ptr(sl), _ptr(cp), _ptr(rv), cp.size - 1, int(ncomp),
+                        int(op), float(init))
+    return dest

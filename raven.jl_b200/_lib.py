@@ -45,6 +45,10 @@ EXPORTED = [
     "rb200_server_class_tiles",
     "rb200_server_last_error",
     "rb200_server_destroy",
+    "rb200_kron_apply",
+    "rb200_scatter",
+    "rb200_gather",
+    "rb200_decode_facecodes",
     "rb200_last_error",
     "rb200_status_string",
 ]
@@ -105,6 +109,13 @@ class Request(ctypes.Structure):
     ]
 
 
+class Layout(ctypes.Structure):
+    """Mirror of rb200_layout."""
+
+    _fields_ = [("block", ctypes.c_int64), ("node_stride", ctypes.c_int64), ("block_stride", ctypes.c_int64),
+                ("comp_stride", ctypes.c_int64)]
+
+
 class RB200Error(RuntimeError):
     def __init__(self, status, message):
         super().__init__(f"{STATUS.get(status, status)}: {message}")
@@ -150,6 +161,11 @@ def lib():
     L.rb200_server_last_error.argtypes = [P]
     L.rb200_server_last_error.restype = ctypes.c_char_p
     L.rb200_server_destroy.argtypes = [P]
+    L.rb200_kron_apply.argtypes = [I32, P, P, P, I32, P, P, P, P, I64, I32, P]
+    LP = ctypes.POINTER(Layout)
+    L.rb200_scatter.argtypes = [P, LP, P, LP, P, I64, I32, I32, P]
+    L.rb200_gather.argtypes = [P, LP, P, LP, P, P, I64, I32, I32, I32, D, P]
+    L.rb200_decode_facecodes.argtypes = [P, I32, I64, P, P]
     for name in EXPORTED:
         if name not in _STRING_RESULT:
             getattr(L, name).restype = ctypes.c_int
