@@ -1,21 +1,25 @@
 // Persistent, TMA-pipelined stage kernel for 3-D hexahedra with Nq = 8 on unwarped
 // bricks, flux-differencing volume forms (Kennedy-Gruber, entropy conservative).
 //
-// Each CTA owns a strided set of elements (e = blockIdx.x + k*gridDim.x) and two CTAs
-// share an SM.  The element's state q arrives by one 1-D bulk copy (cp.async.bulk,
-// completion on an mbarrier) into shared memory; it is only needed to build the
-// per-node partner values, so right after the first barrier the copy of the CTA's next
-// element is issued into the same buffer and lands while the current element's flux
-// arithmetic runs.  Neighbour face traces are fetched with cp.async into the face-slot
-// buffer; the element's own old q and dq are read with coalesced loads at the end.
+// Each CTA owns a strided set of elements (e = blockIdx.x + k*gridDim.x); two CTAs share
+// an SM in FP64, three in FP32 bulk.
+// * The element's state q arrives by one 1-D bulk copy (cp.async.bulk, completion on an
+//   mbarrier) into shared memory.  It is only needed to build the per-node partner
+//   values, so right after the first barrier the copy of the CTA's next element is
+//   issued into the same buffer and lands while the current element's flux arithmetic
+//   runs.
+// * The next element's geometry and neighbour ids, the neighbour face traces and (FP32
+//   bulk) the element's LSRK register are fetched with cp.async during the volume term.
+// * The element's own old q (and the FP64 register) are read with coalesced loads at
+//   the end, so that they hold no registers across the flux arithmetic.
 //
 // A thread owns NPT nodes of the element (same i, j), so the eight z-partners of its
-// line are loaded once for all of them.  The metric of an
-// unwarped brick is folded into a per-element table S_dir[a][id] =
-// drdx_dir * (D[a,id] w_a / w_id - D[id,a]), which equals MJI_id * (D[a,id] l_g[a] -
-// D[id,a] l_g[id]) of esvolumeterm_dir! (src/balancelaws/dgsem.jl:576-600).  Face
-// fluxes are applied in the order x-, x+, y-, y+, z-, z+ of surfaceterm!
-// (dgsem.jl:756-782) by the owner of each face node.
+// line are loaded once for all of them.  The metric of an unwarped brick is folded into
+// a per-element table S_dir[a][id] = drdx_dir * (D[a,id] w_a / w_id - D[id,a]), which
+// equals MJI_id * (D[a,id] l_g[a] - D[id,a] l_g[id]) of esvolumeterm_dir!
+// (src/balancelaws/dgsem.jl:576-600); S_dir[id][id] = 0, so the z pair of a node with
+// itself is skipped.  Face fluxes are applied in the order x-, x+, y-, y+, z-, z+ of
+// surfaceterm! (dgsem.jl:756-782) by the owner of each face node.
 //
 // Every wait on an mbarrier is bounded: after kWaitLimit polls the CTA records
 // RB200 status TIMEOUT in *A.status and returns.
@@ -87,6 +91,12 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
 }
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
@@ -110,6 +120,12 @@ struct Smem {
     typename Vec2<T>::type aux[NAUX / 2][NPP];  // per-node partner values, two per vector load
     double slot[NS][NSLOT];                     // neighbour trace, then (wsJ * nf) * MJI, per face slot
     T S[3][NQ][NQ];                             // S_dir[a][id] * drdx_dir of the current element
+    // FP32 LSRK register of the element, staged during the volume term (FP64 reads it at
+    // the end instead: the larger shared footprint costs more than the exposed latency)
+    __align__(16) T dqs[sizeof(T) == 4 ? NS : 1][sizeof(T) == 4 ? NP : 1];
+    T rs[3][NQ];                                // sum_a S[dir][a][id]
+    double geo[2][4];                           // elem_geo of the current / next element
+    int32_t nb[2][8];                           // neighbours of the current / next element
     uint64_t bar;
 };
 
@@ -141,14 +157,17 @@ __device__ __forceinline__ void slot_nodes(int slot, int& vn, int& opp) {
 
 }  // namespace pipe
 
-#ifndef RB200_PIPE_MIN_CTAS
-#define RB200_PIPE_MIN_CTAS 2  // CTAs per SM the register allocation is sized for
-#endif
+// CTAs per SM the register allocation is sized for: 2 for FP64 (128 registers a
+// thread), 3 for FP32 bulk (80 registers a thread)
+template <typename T>
+constexpr int pipe_min_ctas() {
+    return sizeof(T) == 4 ? 3 : 2;
+}
 
 // NPT nodes per thread: thread t owns nodes t + (512/NPT)*h, h < NPT, which share i, j
 // (k = k0 + (8/NPT)*h), so their z-partners are loaded once.
 template <int COMBO, typename T, int NPT>
-__global__ void __launch_bounds__(512 / NPT, RB200_PIPE_MIN_CTAS)
+__global__ void __launch_bounds__(512 / NPT, pipe_min_ctas<T>())
     pipelined_stage_kernel(const __grid_constant__ PipeArgs A) {
     using namespace pipe;
     constexpr int NT = 512 / NPT, KS = 8 / NPT;
@@ -158,6 +177,7 @@ __global__ void __launch_bounds__(512 / NPT, RB200_PIPE_MIN_CTAS)
     const int ii = t & 7, jj = (t >> 3) & 7, k0 = t >> 6;
     const bool stage = A.mode >= MODE_STAGE;
     const bool dq_is_f32 = stage && sizeof(T) == 4;
+    constexpr bool kStageDq = sizeof(T) == 4;
     const uint32_t qbytes = NS * NP * sizeof(double);
     const T gm1 = (T)(A.gamma - 1.0), gam = (T)A.gamma;
 
@@ -165,22 +185,36 @@ __global__ void __launch_bounds__(512 / NPT, RB200_PIPE_MIN_CTAS)
         mbar_init(&sm.bar, 1);
         fence_mbar_init();
     }
+    int64_t e = blockIdx.x;
+    if (e < A.E) {
+        if (t < 4) cp_async8(&sm.geo[0][t], A.elem_geo + 4 * e + t);
+        else if (t < 10) cp_async4(&sm.nb[0][t - 4], A.nbr + 6 * e + (t - 4));
+    }
+    cp_async_commit();
+    cp_async_wait_all();
     __syncthreads();
 
-    int64_t e = blockIdx.x;
     if (t == 0 && e < A.E) {
         mbar_expect_tx(&sm.bar, qbytes);
         bulk_g2s(&sm.q[0][0], A.q_in + (size_t)e * NS * NP, qbytes, &sm.bar);
     }
     uint32_t phase = 0;
-    for (; e < A.E; e += gridDim.x) {
+    int buf = 0;
+    for (; e < A.E; e += gridDim.x, buf ^= 1) {
         const int64_t enext = e + gridDim.x;
-        const double* eg = A.elem_geo + 4 * e;
-        const double drdx[3] = {__ldg(eg), __ldg(eg + 1), __ldg(eg + 2)};
-        if (t < 192) {
-            const int dir = t >> 6, a = (t >> 3) & 7, id = t & 7;
+        const double drdx[3] = {sm.geo[buf][0], sm.geo[buf][1], sm.geo[buf][2]};
+        for (int q = t; q < 192; q += NT) {
+            const int dir = q >> 6, a = (q >> 3) & 7, id = q & 7;
             const double dd = dir == 0 ? drdx[0] : (dir == 1 ? drdx[1] : drdx[2]);
             sm.S[dir][a][id] = (T)(A.S[a * 8 + id] * dd);
+        }
+        if (COMBO == EUL_KG && t < 24) {
+            const int dir = t >> 3, id = t & 7;
+            const double dd = dir == 0 ? drdx[0] : (dir == 1 ? drdx[1] : drdx[2]);
+            T r = T(0);
+#pragma unroll
+            for (int a = 0; a < NQ; ++a) r += (T)(A.S[a * 8 + id] * dd);
+            sm.rs[dir][id] = r;
         }
         // ---- this element's state
         if (__syncthreads_or(!bounded_wait(&sm.bar, phase))) {
@@ -226,6 +260,11 @@ __global__ void __launch_bounds__(512 / NPT, RB200_PIPE_MIN_CTAS)
             mbar_expect_tx(&sm.bar, qbytes);
             bulk_g2s(&sm.q[0][0], A.q_in + (size_t)enext * NS * NP, qbytes, &sm.bar);
         }
+        // geometry and neighbours of the next element, with the traces below
+        if (enext < A.E) {
+            if (t < 4) cp_async8(&sm.geo[buf ^ 1][t], A.elem_geo + 4 * enext + t);
+            else if (t < 10) cp_async4(&sm.nb[buf ^ 1][t - 4], A.nbr + 6 * enext + (t - 4));
+        }
         // neighbour traces of this thread's face slots t + NT * sl
 #pragma unroll
         for (int sl = 0; sl < (NSLOT + NT - 1) / NT; ++sl) {
@@ -233,35 +272,48 @@ __global__ void __launch_bounds__(512 / NPT, RB200_PIPE_MIN_CTAS)
             if (slot >= NSLOT) continue;
             int vn, opp;
             slot_nodes(slot, vn, opp);
-            const int ne = __ldg(A.nbr + 6 * e + (slot >> 6));
+            const int ne = sm.nb[buf][slot >> 6];
             if (ne >= 0) {
                 const double* qn = A.q_in + (size_t)ne * NS * NP + opp;
 #pragma unroll
                 for (int s = 0; s < NS; ++s) cp_async8(&sm.slot[s][slot], qn + s * NP);
             }
         }
+        if (kStageDq && A.mode == MODE_STAGE) {  // the element's FP32 register, for the end of the stage
+            const char* src = reinterpret_cast<const char*>(A.dq) + (size_t)e * NS * NP * sizeof(T);
+            char* dst = reinterpret_cast<char*>(&sm.dqs[0][0]);
+            for (int c = t; c < NS * NP * (int)sizeof(T) / 16; c += NT) cp_async16(dst + 16 * c, src + 16 * c);
+        }
         cp_async_commit();
 
         // ---- volume term (ordered pairs along x, y, z)
-        T acc[NPT][NS];
+        T acc[NPT][NS], accu[NPT];
 #pragma unroll
-        for (int h = 0; h < NPT; ++h)
+        for (int h = 0; h < NPT; ++h) {
+            accu[h] = T(0);
 #pragma unroll
             for (int s = 0; s < NS; ++s) acc[h][s] = T(0);
+        }
 
-        auto pair = [&](T (&ac)[NS], const T (&o)[NAUX], const T (&pv)[NAUX], const T sc, const int dir) {
+        // KG with the own-node parts of the averages factored out of the sums:
+        //   sum F (o_k + p_k) = o_k sum F + sum F p_k, F = rho_avg * u_avg,dir * S,
+        //   sum S (o_5 + p_5) = o_5 rs_dir + sum S p_5,
+        //   sum U (rho_avg (o_4 + p_4) + o_5 + p_5) = o_4 sum F + o_5 sum U + sum (F p_4 + U p_5)
+        // (o, p: halves of the own and partner rho, u, e, p); the own parts are added after
+        // the pair loop.
+        auto pair = [&](T (&ac)[NS], T& au, const T (&o)[NAUX], const T (&pv)[NAUX], const T sc, const int dir) {
             if constexpr (COMBO == EUL_KG) {
                 const T rb = o[0] + pv[0];
-                const T ub0 = o[1] + pv[1], ub1 = o[2] + pv[2], ub2 = o[3] + pv[3];
-                const T eb = o[4] + pv[4], pb = o[5] + pv[5];
-                const T un = (dir == 0 ? ub0 : dir == 1 ? ub1 : ub2) * sc;
+                const T un = (dir == 0 ? o[1] + pv[1] : dir == 1 ? o[2] + pv[2] : o[3] + pv[3]) * sc;
                 const T f1 = rb * un;
                 ac[0] += f1;
-                ac[1] = fma(f1, ub0, ac[1]);
-                ac[2] = fma(f1, ub1, ac[2]);
-                ac[3] = fma(f1, ub2, ac[3]);
-                ac[1 + dir] = fma(pb, sc, ac[1 + dir]);
-                ac[4] = fma(un, fma(rb, eb, pb), ac[4]);
+                au += un;
+                ac[1] = fma(f1, pv[1], ac[1]);
+                ac[2] = fma(f1, pv[2], ac[2]);
+                ac[3] = fma(f1, pv[3], ac[3]);
+                ac[1 + dir] = fma(pv[5], sc, ac[1 + dir]);
+                ac[4] = fma(f1, pv[4], ac[4]);
+                ac[4] = fma(un, pv[5], ac[4]);
             } else {
                 const T ua0 = (o[1] + pv[1]) * T(0.5), ua1 = (o[2] + pv[2]) * T(0.5), ua2 = (o[3] + pv[3]) * T(0.5);
                 const T ra = (o[0] + pv[0]) * T(0.5);
@@ -298,33 +350,31 @@ __global__ void __launch_bounds__(512 / NPT, RB200_PIPE_MIN_CTAS)
                 const int kk = k0 + KS * h;
                 T pv[NAUX];
                 load_aux(pv, a + 8 * (jj + 8 * kk));
-                pair(acc[h], own[h], pv, sx, 0);
+                pair(acc[h], accu[h], own[h], pv, sx, 0);
                 load_aux(pv, ii + 8 * (a + 8 * kk));
-                pair(acc[h], own[h], pv, sy, 1);
+                pair(acc[h], accu[h], own[h], pv, sy, 1);
             }
             T pv[NAUX];
             load_aux(pv, ii + 8 * (jj + 8 * a));
 #pragma unroll
-            for (int h = 0; h < NPT; ++h) pair(acc[h], own[h], pv, sm.S[2][a][k0 + KS * h], 2);
+            for (int h = 0; h < NPT; ++h)
+                if (a != k0 + KS * h) pair(acc[h], accu[h], own[h], pv, sm.S[2][a][k0 + KS * h], 2);  // S_aa = 0
         }
 
-        // ---- own old state and register, read now so that the loads overlap the faces
-        const size_t g0 = (size_t)e * NS * NP + t;
-        double qold[NPT][NS];
-        T dqold[NPT][NS];
+        if constexpr (COMBO == EUL_KG) {
 #pragma unroll
-        for (int h = 0; h < NPT; ++h)
-#pragma unroll
-            for (int s = 0; s < NS; ++s) {
-                const size_t g = g0 + NT * h + s * NP;
-                qold[h][s] = stage ? __ldg(A.q_in + g) : 0.0;
-                if (A.mode == MODE_STAGE || A.mode == MODE_TENDENCY_INC)
-                    dqold[h][s] = dq_is_f32 ? (T)__ldg(reinterpret_cast<const float*>(A.dq) + g)
-                                            : (T)__ldg(reinterpret_cast<const double*>(A.dq) + g);
-                else
-                    dqold[h][s] = T(0);
+            for (int h = 0; h < NPT; ++h) {
+                const int kk = k0 + KS * h;
+                const T o5 = own[h][5];
+                acc[h][1] = fma(own[h][1], acc[h][0], acc[h][1]);
+                acc[h][2] = fma(own[h][2], acc[h][0], acc[h][2]);
+                acc[h][3] = fma(own[h][3], acc[h][0], acc[h][3]);
+                acc[h][1] = fma(o5, sm.rs[0][ii], acc[h][1]);
+                acc[h][2] = fma(o5, sm.rs[1][jj], acc[h][2]);
+                acc[h][3] = fma(o5, sm.rs[2][kk], acc[h][3]);
+                acc[h][4] = fma(own[h][4], acc[h][0], fma(o5, accu[h], acc[h][4]));
             }
-
+        }
         // ---- face-slot contributions (wsJ * nf) * MJI, written over the slot's trace
         cp_async_wait_all();
 #pragma unroll
@@ -334,7 +384,7 @@ __global__ void __launch_bounds__(512 / NPT, RB200_PIPE_MIN_CTAS)
             const int f = slot >> 6, dir = f >> 1, side = f & 1;
             int vn, opp;
             slot_nodes(slot, vn, opp);
-            const bool open_face = __ldg(A.nbr + 6 * e + f) >= 0;
+            const bool open_face = sm.nb[buf][f] >= 0;
             // q- and its primitives from the staged partner values of the element
             T qm[NS], u0, u1, u2, p, rinv;
             {
@@ -408,6 +458,25 @@ __global__ void __launch_bounds__(512 / NPT, RB200_PIPE_MIN_CTAS)
             }
         }
         __syncthreads();  // #2: face-slot contributions ready
+        // ---- own old state and register, read now so that the loads overlap the faces
+        const size_t g0 = (size_t)e * NS * NP + t;
+        double qold[NPT][NS];
+        T dqold[NPT][NS];
+#pragma unroll
+        for (int h = 0; h < NPT; ++h)
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                const size_t g = g0 + NT * h + s * NP;
+                qold[h][s] = stage ? __ldg(A.q_in + g) : 0.0;
+                if (kStageDq && A.mode == MODE_STAGE)
+                    dqold[h][s] = sm.dqs[kStageDq ? s : 0][kStageDq ? t + NT * h : 0];
+                else if (A.mode == MODE_STAGE || A.mode == MODE_TENDENCY_INC)
+                    dqold[h][s] = dq_is_f32 ? (T)__ldg(reinterpret_cast<const float*>(A.dq) + g)
+                                            : (T)__ldg(reinterpret_cast<const double*>(A.dq) + g);
+                else
+                    dqold[h][s] = T(0);
+            }
+
         // ---- own nodes: dq = rka*dq + volume - faces (x, y, z order); q_out = q + rkb*dt*dq
 #pragma unroll
         for (int h = 0; h < NPT; ++h) {
