@@ -38,6 +38,8 @@ if ROOT not in sys.path:
 WORKLOADS = {
     # name: dim, N, elements per side, domain side, law, volume flux, precision, warp
     "euler3d_kg_n7_32_fp64": dict(dim=3, N=7, K=32, L=10.0, law="euler", vflux="kg", precision="fp64", warp=False),
+    "euler3d_kg_n7_32_fp32bulk": dict(dim=3, N=7, K=32, L=10.0, law="euler", vflux="kg", precision="fp32_bulk",
+                                      warp=False),
     "euler3d_kg_n7_32_fp32bulk_warped": dict(dim=3, N=7, K=32, L=10.0, law="euler", vflux="kg",
                                              precision="fp32_bulk", warp=True),
     "euler3d_kg_n7_32_fp64_warped": dict(dim=3, N=7, K=32, L=10.0, law="euler", vflux="kg", precision="fp64",
@@ -541,10 +543,14 @@ def main(argv=None):
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--elements-per-side", type=int, default=None,
+                   help="override the workload's elements per side (smaller cases for profiling)")
     args = p.parse_args(argv)
     if args.workload == SERVE_WORKLOAD:
         return run_serving(args)
-    w = WORKLOADS[args.workload]
+    w = dict(WORKLOADS[args.workload])
+    if args.elements_per_side:
+        w["K"] = int(args.elements_per_side)
     if args.impl == "reference":
         return run_reference(args, w)
 
