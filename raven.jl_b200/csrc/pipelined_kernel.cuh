@@ -103,21 +103,50 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
+// Per-node partner values (6 per node), read as vectors: three 16-byte loads in FP64, one
+// 16-byte and one 8-byte load in FP32.
 template <typename T>
-struct Vec2;
+struct AuxBuf;
 template <>
-struct Vec2<double> {
-    using type = double2;
+struct AuxBuf<double> {
+    double2 v[NAUX / 2][NPP];
+    __device__ __forceinline__ void put(int i, const double (&o)[NAUX]) {
+#pragma unroll
+        for (int c = 0; c < NAUX / 2; ++c) v[c][i] = make_double2(o[2 * c], o[2 * c + 1]);
+    }
+    __device__ __forceinline__ void get(int i, double (&o)[NAUX]) const {
+#pragma unroll
+        for (int c = 0; c < NAUX / 2; ++c) {
+            const double2 x = v[c][i];
+            o[2 * c] = x.x;
+            o[2 * c + 1] = x.y;
+        }
+    }
 };
 template <>
-struct Vec2<float> {
-    using type = float2;
+struct AuxBuf<float> {
+    float4 a[NPP];
+    float2 b[NPP];
+    __device__ __forceinline__ void put(int i, const float (&o)[NAUX]) {
+        a[i] = make_float4(o[0], o[1], o[2], o[3]);
+        b[i] = make_float2(o[4], o[5]);
+    }
+    __device__ __forceinline__ void get(int i, float (&o)[NAUX]) const {
+        const float4 x = a[i];
+        const float2 y = b[i];
+        o[0] = x.x;
+        o[1] = x.y;
+        o[2] = x.z;
+        o[3] = x.w;
+        o[4] = y.x;
+        o[5] = y.y;
+    }
 };
 
 template <typename T>
 struct Smem {
     double q[NS][NP];                           // state of the element (TMA destination)
-    typename Vec2<T>::type aux[NAUX / 2][NPP];  // per-node partner values, two per vector load
+    AuxBuf<T> aux;                              // per-node partner values
     double slot[NS][NSLOT];                     // neighbour trace, then (wsJ * nf) * MJI, per face slot
     T S[3][NQ][NQ];                             // S_dir[a][id] * drdx_dir of the current element
     // FP32 LSRK register of the element, staged during the volume term (FP64 reads it at
@@ -248,11 +277,7 @@ __global__ void __launch_bounds__(512 / NPT, pipe_min_ctas<T>())
                 own[h][4] = rho / (T(2) * p);
                 own[h][5] = u0 * u0 + u1 * u1 + u2 * u2;
             }
-#pragma unroll
-            for (int c = 0; c < NAUX / 2; ++c) {
-                sm.aux[c][PAD(n)].x = own[h][2 * c];
-                sm.aux[c][PAD(n)].y = own[h][2 * c + 1];
-            }
+            sm.aux.put(PAD(n), own[h]);
         }
         __syncthreads();  // #1: aux and S ready; q and the slot buffer are free
         if (t == 0 && enext < A.E) {
@@ -334,14 +359,7 @@ __global__ void __launch_bounds__(512 / NPT, pipe_min_ctas<T>())
                 ac[4] = fma(un, cc * rlog + rlog * uaa + pt, ac[4]);
             }
         };
-        auto load_aux = [&](T (&pv)[NAUX], const int n) {
-#pragma unroll
-            for (int c = 0; c < NAUX / 2; ++c) {
-                const auto v = sm.aux[c][PAD(n)];
-                pv[2 * c] = v.x;
-                pv[2 * c + 1] = v.y;
-            }
-        };
+        auto load_aux = [&](T (&pv)[NAUX], const int n) { sm.aux.get(PAD(n), pv); };
 #pragma unroll
         for (int a = 0; a < NQ; ++a) {
             const T sx = sm.S[0][a][ii], sy = sm.S[1][a][jj];
@@ -388,25 +406,26 @@ __global__ void __launch_bounds__(512 / NPT, pipe_min_ctas<T>())
             // q- and its primitives from the staged partner values of the element
             T qm[NS], u0, u1, u2, p, rinv;
             {
-                const auto v0 = sm.aux[0][PAD(vn)], v1 = sm.aux[1][PAD(vn)], v2 = sm.aux[2][PAD(vn)];
+                T v[NAUX];
+                sm.aux.get(PAD(vn), v);
                 if constexpr (COMBO == EUL_KG) {
-                    const T rho = T(2) * v0.x;
-                    u0 = T(2) * v0.y;
-                    u1 = T(2) * v1.x;
-                    u2 = T(2) * v1.y;
-                    p = T(2) * v2.y;
+                    const T rho = T(2) * v[0];
+                    u0 = T(2) * v[1];
+                    u1 = T(2) * v[2];
+                    u2 = T(2) * v[3];
+                    p = T(2) * v[5];
                     rinv = T(1) / rho;
                     qm[0] = rho;
-                    qm[4] = rho * (T(2) * v2.x);
+                    qm[4] = rho * (T(2) * v[4]);
                 } else {
-                    const T rho = v0.x;
-                    u0 = v0.y;
-                    u1 = v1.x;
-                    u2 = v1.y;
-                    p = rho / (T(2) * v2.x);
+                    const T rho = v[0];
+                    u0 = v[1];
+                    u1 = v[2];
+                    u2 = v[3];
+                    p = rho / (T(2) * v[4]);
                     rinv = T(1) / rho;
                     qm[0] = rho;
-                    qm[4] = p / gm1 + T(0.5) * rho * v2.y;
+                    qm[4] = p / gm1 + T(0.5) * rho * v[5];
                 }
                 qm[1] = qm[0] * u0;
                 qm[2] = qm[0] * u1;
