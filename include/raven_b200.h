@@ -171,7 +171,8 @@ rb200_status rb200_weighted_sums_noalloc(const double* q, const double* MJ, int3
  *
  * Served configurations are unwarped bricks (affine elements): dim 2 or 3, nq 4, 6 or 8.
  *   - Advection: weak form.
- *   - Euler: flux differencing with Kennedy-Gruber.
+ *   - Euler: flux differencing with Kennedy-Gruber.  3-D nq = 8 Euler classes run the
+ *     persistent TMA-pipelined kernel of the DGSEM handle over their chunks.
  * The surface flux is Rusanov or central, and the precision is FP64 or FP32_BULK.
  * ------------------------------------------------------------------------------------ */
 typedef struct rb200_request {

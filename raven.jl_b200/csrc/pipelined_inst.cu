@@ -1,4 +1,5 @@
-// Instantiations and launch helpers of the pipelined 3-D Nq = 8 stage kernel.
+// Instantiations and launch helpers of the pipelined 3-D Nq = 8 stage kernel: one state
+// (the DGSEM handle) or the chunks of a serving class (BATCH).
 #include "pipelined_kernel.cuh"
 
 namespace rb200 {
@@ -8,9 +9,9 @@ namespace rb200 {
 #endif
 constexpr int kNPT = RB200_PIPE_NPT;
 
-template <int COMBO, typename T>
-static cudaError_t launch_p(const PipeArgs& a, int grid, cudaStream_t s) {
-    auto kern = pipelined_stage_kernel<COMBO, T, kNPT>;
+template <int COMBO, typename T, bool BATCH>
+static cudaError_t launch_p(const PipeArgs& a, const PipeBatch& b, int grid, cudaStream_t s) {
+    auto kern = pipelined_stage_kernel<COMBO, T, kNPT, BATCH>;
     static bool configured = false;
     if (!configured) {
         cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -18,19 +19,29 @@ static cudaError_t launch_p(const PipeArgs& a, int grid, cudaStream_t s) {
         if (err != cudaSuccess) return err;
         configured = true;
     }
-    kern<<<grid, 512 / kNPT, sizeof(pipe::Smem<T>), s>>>(a);
+    kern<<<grid, 512 / kNPT, sizeof(pipe::Smem<T>), s>>>(a, b);
     return cudaGetLastError();
 }
 
 cudaError_t launch_pipelined(int combo, int fp32, const PipeArgs& a, int grid, cudaStream_t s) {
-    if (combo == EUL_KG) return fp32 ? launch_p<EUL_KG, float>(a, grid, s) : launch_p<EUL_KG, double>(a, grid, s);
-    if (combo == EUL_EC) return fp32 ? launch_p<EUL_EC, float>(a, grid, s) : launch_p<EUL_EC, double>(a, grid, s);
+    const PipeBatch none{};
+    if (combo == EUL_KG)
+        return fp32 ? launch_p<EUL_KG, float, false>(a, none, grid, s) : launch_p<EUL_KG, double, false>(a, none, grid, s);
+    if (combo == EUL_EC)
+        return fp32 ? launch_p<EUL_EC, float, false>(a, none, grid, s) : launch_p<EUL_EC, double, false>(a, none, grid, s);
     return cudaErrorInvalidValue;
 }
 
-template <int COMBO, typename T>
+cudaError_t launch_pipelined_batch(int combo, int fp32, const PipeArgs& a, const PipeBatch& b, int grid,
+                                   cudaStream_t s) {
+    if (combo == EUL_KG)
+        return fp32 ? launch_p<EUL_KG, float, true>(a, b, grid, s) : launch_p<EUL_KG, double, true>(a, b, grid, s);
+    return cudaErrorInvalidValue;
+}
+
+template <int COMBO, typename T, bool BATCH>
 static int occupancy_p() {
-    auto kern = pipelined_stage_kernel<COMBO, T, kNPT>;
+    auto kern = pipelined_stage_kernel<COMBO, T, kNPT, BATCH>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(pipe::Smem<T>)) !=
         cudaSuccess)
         return 0;
@@ -41,8 +52,13 @@ static int occupancy_p() {
 }
 
 int pipelined_blocks_per_sm(int combo, int fp32) {
-    if (combo == EUL_KG) return fp32 ? occupancy_p<EUL_KG, float>() : occupancy_p<EUL_KG, double>();
-    if (combo == EUL_EC) return fp32 ? occupancy_p<EUL_EC, float>() : occupancy_p<EUL_EC, double>();
+    if (combo == EUL_KG) return fp32 ? occupancy_p<EUL_KG, float, false>() : occupancy_p<EUL_KG, double, false>();
+    if (combo == EUL_EC) return fp32 ? occupancy_p<EUL_EC, float, false>() : occupancy_p<EUL_EC, double, false>();
+    return 0;
+}
+
+int pipelined_batch_blocks_per_sm(int combo, int fp32) {
+    if (combo == EUL_KG) return fp32 ? occupancy_p<EUL_KG, float, true>() : occupancy_p<EUL_KG, double, true>();
     return 0;
 }
 

@@ -48,6 +48,28 @@ struct PipeArgs {
     double w[8];
 };
 
+// Serving loop: the elements of a launch are the chunks of a class's running solves
+// instead of the strided elements of one state (SolveDesc, Chunk: rb200_internal.h).
+struct PipeBatch {
+    const SolveDesc* solves;
+    const Chunk* chunks;
+    const int32_t* nchunks;  // chunk slots in use (device)
+    const int64_t* tick;     // class tick counter (device)
+    int32_t stage;           // 0..4: selects the ping-pong buffer with the tick
+    double rkb;              // LSRK b coefficient of the stage (times each solve's dt)
+};
+
+// One element as the kernel sees it: its state's buffers and its index there.
+struct ElemRef {
+    const double* q;     // q_in of the element's state (neighbours are in the same state)
+    double* q_out;
+    void* dq;
+    const double* geo;   // elem_geo of the state
+    const int32_t* nbr;  // neighbour table of the state
+    int64_t e;           // element index in its state; -1: none (end of the CTA's work)
+    double rkb_dt;
+};
+
 namespace pipe {
 
 constexpr int NQ = 8, NP = 512, NS = 5, NAUX = 6, NSLOT = 384;
@@ -155,6 +177,7 @@ struct Smem {
     T rs[3][NQ];                                // sum_a S[dir][a][id]
     double geo[2][4];                           // elem_geo of the current / next element
     int32_t nb[2][8];                           // neighbours of the current / next element
+    ElemRef ref[2];                             // the current / next element
     uint64_t bar;
 };
 
@@ -184,6 +207,60 @@ __device__ __forceinline__ void slot_nodes(int slot, int& vn, int& opp) {
     }
 }
 
+// The CTA's sequence of elements, advanced by thread 0 one element ahead of the work.
+// One state: elements blockIdx.x + k*gridDim.x.  Serving batch: the elements of chunks
+// blockIdx.x + k*gridDim.x, in order.
+template <bool BATCH>
+struct Cursor {
+    int64_t e = 0;  // one state: element; batch: index within the chunk
+    int ci = 0;     // batch: chunk slot
+    int nch = 0;    // batch: chunk slots in use
+
+    __device__ bool start(const PipeArgs& A, const PipeBatch& B) {
+        if constexpr (!BATCH) {
+            e = blockIdx.x;
+            return e < A.E;
+        } else {
+            nch = *B.nchunks;
+            ci = blockIdx.x;
+            e = 0;
+            return skip_empty(B);
+        }
+    }
+    __device__ bool advance(const PipeArgs& A, const PipeBatch& B) {
+        if constexpr (!BATCH) {
+            e += gridDim.x;
+            return e < A.E;
+        } else {
+            if (++e < B.chunks[ci].count) return true;
+            ci += gridDim.x;
+            e = 0;
+            return skip_empty(B);
+        }
+    }
+    __device__ bool skip_empty(const PipeBatch& B) {
+        while (ci < nch && (B.chunks[ci].solve < 0 || B.chunks[ci].count <= 0)) ci += gridDim.x;
+        return ci < nch;
+    }
+    __device__ void resolve(const PipeArgs& A, const PipeBatch& B, ElemRef& r) const {
+        if constexpr (!BATCH) {
+            r = ElemRef{A.q_in, A.q_out, A.dq, A.elem_geo, A.nbr, e, A.rkb_dt};
+        } else {
+            const Chunk c = B.chunks[ci];
+            const SolveDesc& sd = B.solves[c.solve];
+            const int par = (int)((*B.tick - sd.start_tick + B.stage) & 1);
+            r = ElemRef{sd.q[par], sd.q[par ^ 1], sd.dq, sd.elem_geo, sd.nbr, c.first + e, B.rkb * sd.dt};
+        }
+    }
+};
+
+// Threads 0..9: one value each of the geometry (4) and neighbour ids (6) of element r
+// into a shared slot (cp.async).
+__device__ __forceinline__ void fetch_part(const ElemRef& r, int t, double (&geo)[4], int32_t (&nb)[8]) {
+    if (t < 4) cp_async8(&geo[t], r.geo + 4 * r.e + t);
+    else cp_async4(&nb[t - 4], r.nbr + 6 * r.e + (t - 4));
+}
+
 }  // namespace pipe
 
 // CTAs per SM the register allocation is sized for: 2 for FP64 (128 registers a
@@ -195,9 +272,9 @@ constexpr int pipe_min_ctas() {
 
 // NPT nodes per thread: thread t owns nodes t + (512/NPT)*h, h < NPT, which share i, j
 // (k = k0 + (8/NPT)*h), so their z-partners are loaded once.
-template <int COMBO, typename T, int NPT>
+template <int COMBO, typename T, int NPT, bool BATCH>
 __global__ void __launch_bounds__(512 / NPT, pipe_min_ctas<T>())
-    pipelined_stage_kernel(const __grid_constant__ PipeArgs A) {
+    pipelined_stage_kernel(const __grid_constant__ PipeArgs A, const __grid_constant__ PipeBatch B) {
     using namespace pipe;
     constexpr int NT = 512 / NPT, KS = 8 / NPT;
     extern __shared__ __align__(128) unsigned char pipe_smem_raw[];
@@ -210,27 +287,31 @@ __global__ void __launch_bounds__(512 / NPT, pipe_min_ctas<T>())
     const uint32_t qbytes = NS * NP * sizeof(double);
     const T gm1 = (T)(A.gamma - 1.0), gam = (T)A.gamma;
 
+    Cursor<BATCH> cur;  // meaningful in threads 0..9
     if (t == 0) {
         mbar_init(&sm.bar, 1);
         fence_mbar_init();
     }
-    int64_t e = blockIdx.x;
-    if (e < A.E) {
-        if (t < 4) cp_async8(&sm.geo[0][t], A.elem_geo + 4 * e + t);
-        else if (t < 10) cp_async4(&sm.nb[0][t - 4], A.nbr + 6 * e + (t - 4));
+    if (t < 10) {
+        ElemRef r{};
+        r.e = -1;
+        if (cur.start(A, B)) cur.resolve(A, B, r);
+        if (t == 0) sm.ref[0] = r;
+        if (r.e >= 0) fetch_part(r, t, sm.geo[0], sm.nb[0]);
     }
     cp_async_commit();
     cp_async_wait_all();
     __syncthreads();
 
-    if (t == 0 && e < A.E) {
+    if (t == 0 && sm.ref[0].e >= 0) {
         mbar_expect_tx(&sm.bar, qbytes);
-        bulk_g2s(&sm.q[0][0], A.q_in + (size_t)e * NS * NP, qbytes, &sm.bar);
+        bulk_g2s(&sm.q[0][0], sm.ref[0].q + (size_t)sm.ref[0].e * NS * NP, qbytes, &sm.bar);
     }
     uint32_t phase = 0;
-    int buf = 0;
-    for (; e < A.E; e += gridDim.x, buf ^= 1) {
-        const int64_t enext = e + gridDim.x;
+    int64_t es = blockIdx.x;  // one state: the current element, kept in registers
+    for (int buf = 0;; buf ^= 1, es += gridDim.x) {
+        const int64_t e = BATCH ? sm.ref[buf].e : (es < A.E ? es : -1);
+        if (e < 0) break;
         const double drdx[3] = {sm.geo[buf][0], sm.geo[buf][1], sm.geo[buf][2]};
         for (int q = t; q < 192; q += NT) {
             const int dir = q >> 6, a = (q >> 3) & 7, id = q & 7;
@@ -280,16 +361,23 @@ __global__ void __launch_bounds__(512 / NPT, pipe_min_ctas<T>())
             sm.aux.put(PAD(n), own[h]);
         }
         __syncthreads();  // #1: aux and S ready; q and the slot buffer are free
-        if (t == 0 && enext < A.E) {
-            fence_proxy_async();
-            mbar_expect_tx(&sm.bar, qbytes);
-            bulk_g2s(&sm.q[0][0], A.q_in + (size_t)enext * NS * NP, qbytes, &sm.bar);
+        if (t < 10) {  // the next element: its state by TMA, its geometry and neighbours with the traces
+            ElemRef rn{};
+            rn.e = -1;
+            if (cur.advance(A, B)) cur.resolve(A, B, rn);
+            if (t == 0) {
+                sm.ref[buf ^ 1] = rn;
+                if (rn.e >= 0) {
+                    fence_proxy_async();
+                    mbar_expect_tx(&sm.bar, qbytes);
+                    bulk_g2s(&sm.q[0][0], rn.q + (size_t)rn.e * NS * NP, qbytes, &sm.bar);
+                }
+            }
+            if (rn.e >= 0) fetch_part(rn, t, sm.geo[buf ^ 1], sm.nb[buf ^ 1]);
         }
-        // geometry and neighbours of the next element, with the traces below
-        if (enext < A.E) {
-            if (t < 4) cp_async8(&sm.geo[buf ^ 1][t], A.elem_geo + 4 * enext + t);
-            else if (t < 10) cp_async4(&sm.nb[buf ^ 1][t - 4], A.nbr + 6 * enext + (t - 4));
-        }
+        // the element's state buffers (one state: the kernel parameters)
+        const double* const qin_e = BATCH ? sm.ref[buf].q : A.q_in;
+        void* const dq_e = BATCH ? sm.ref[buf].dq : A.dq;
         // neighbour traces of this thread's face slots t + NT * sl
 #pragma unroll
         for (int sl = 0; sl < (NSLOT + NT - 1) / NT; ++sl) {
@@ -299,13 +387,13 @@ __global__ void __launch_bounds__(512 / NPT, pipe_min_ctas<T>())
             slot_nodes(slot, vn, opp);
             const int ne = sm.nb[buf][slot >> 6];
             if (ne >= 0) {
-                const double* qn = A.q_in + (size_t)ne * NS * NP + opp;
+                const double* qn = qin_e + (size_t)ne * NS * NP + opp;
 #pragma unroll
                 for (int s = 0; s < NS; ++s) cp_async8(&sm.slot[s][slot], qn + s * NP);
             }
         }
         if (kStageDq && A.mode == MODE_STAGE) {  // the element's FP32 register, for the end of the stage
-            const char* src = reinterpret_cast<const char*>(A.dq) + (size_t)e * NS * NP * sizeof(T);
+            const char* src = reinterpret_cast<const char*>(dq_e) + (size_t)e * NS * NP * sizeof(T);
             char* dst = reinterpret_cast<char*>(&sm.dqs[0][0]);
             for (int c = t; c < NS * NP * (int)sizeof(T) / 16; c += NT) cp_async16(dst + 16 * c, src + 16 * c);
         }
@@ -479,6 +567,8 @@ __global__ void __launch_bounds__(512 / NPT, pipe_min_ctas<T>())
         __syncthreads();  // #2: face-slot contributions ready
         // ---- own old state and register, read now so that the loads overlap the faces
         const size_t g0 = (size_t)e * NS * NP + t;
+        double* const qout_e = BATCH ? sm.ref[buf].q_out : A.q_out;
+        const double rkb_dt = BATCH ? sm.ref[buf].rkb_dt : A.rkb_dt;
         double qold[NPT][NS];
         T dqold[NPT][NS];
 #pragma unroll
@@ -486,12 +576,12 @@ __global__ void __launch_bounds__(512 / NPT, pipe_min_ctas<T>())
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
                 const size_t g = g0 + NT * h + s * NP;
-                qold[h][s] = stage ? __ldg(A.q_in + g) : 0.0;
+                qold[h][s] = stage ? __ldg(qin_e + g) : 0.0;
                 if (kStageDq && A.mode == MODE_STAGE)
                     dqold[h][s] = sm.dqs[kStageDq ? s : 0][kStageDq ? t + NT * h : 0];
                 else if (A.mode == MODE_STAGE || A.mode == MODE_TENDENCY_INC)
-                    dqold[h][s] = dq_is_f32 ? (T)__ldg(reinterpret_cast<const float*>(A.dq) + g)
-                                            : (T)__ldg(reinterpret_cast<const double*>(A.dq) + g);
+                    dqold[h][s] = dq_is_f32 ? (T)__ldg(reinterpret_cast<const float*>(dq_e) + g)
+                                            : (T)__ldg(reinterpret_cast<const double*>(dq_e) + g);
                 else
                     dqold[h][s] = T(0);
             }
@@ -517,11 +607,11 @@ __global__ void __launch_bounds__(512 / NPT, pipe_min_ctas<T>())
                     if (slots[d] >= 0) v = v - (T)sm.slot[s][slots[d]];
                 const size_t g = g0 + NT * h + s * NP;
                 if (stage) {
-                    if (dq_is_f32) reinterpret_cast<float*>(A.dq)[g] = (float)v;
-                    else reinterpret_cast<double*>(A.dq)[g] = (double)v;
-                    A.q_out[g] = qold[h][s] + A.rkb_dt * (double)v;
+                    if (dq_is_f32) reinterpret_cast<float*>(dq_e)[g] = (float)v;
+                    else reinterpret_cast<double*>(dq_e)[g] = (double)v;
+                    qout_e[g] = qold[h][s] + rkb_dt * (double)v;
                 } else {
-                    reinterpret_cast<double*>(A.dq)[g] = (double)v;
+                    reinterpret_cast<double*>(dq_e)[g] = (double)v;
                 }
             }
         }

@@ -52,6 +52,23 @@ struct StageArgs {
     double w[kMaxNq];
 };
 
+// Serving loop: one running solve of a class, and one chunk of its elements.
+struct SolveDesc {
+    double* q[2];             // ping-pong state buffers
+    void* dq;                 // LSRK register (FP64 or FP32)
+    const double* elem_geo;   // (4, E) unwarped brick geometry
+    const int32_t* nbr;       // (2*dim, E) neighbour table
+    int64_t E;
+    double dt;
+    int64_t start_tick;       // class tick at which the solve's state sat in q[0]
+};
+
+struct Chunk {
+    int32_t solve;  // index into the descriptor table, or -1
+    int32_t count;  // elements in this chunk (0: empty slot)
+    int64_t first;  // first element of the chunk within the solve
+};
+
 // Launches one stage kernel; returns cudaSuccess or the launch error.
 cudaError_t launch_stage(int dim, int nq, int combo, int geom, int fp32, const StageArgs& a, cudaStream_t s);
 // Dynamic shared memory the kernel needs (bytes) and threads per block; 0 if not built.
@@ -61,6 +78,11 @@ struct PipeArgs;  // pipelined_kernel.cuh
 // Persistent TMA-pipelined kernel for 3-D Nq = 8 affine flux differencing (KG, EC).
 cudaError_t launch_pipelined(int combo, int fp32, const PipeArgs& a, int grid, cudaStream_t s);
 int pipelined_blocks_per_sm(int combo, int fp32);
+struct PipeBatch;  // pipelined_kernel.cuh
+// The same kernel over the chunks of a serving class (Euler KG only).
+cudaError_t launch_pipelined_batch(int combo, int fp32, const PipeArgs& a, const PipeBatch& b, int grid,
+                                   cudaStream_t s);
+int pipelined_batch_blocks_per_sm(int combo, int fp32);
 
 // Reductions and face-map expansion (reduce.cu).
 cudaError_t launch_weighted_sums(const double* q, const double* elem_geo, const double* vgeo, const double* w,

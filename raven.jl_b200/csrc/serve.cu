@@ -35,6 +35,7 @@
 #include <vector>
 
 #include "../../include/raven_b200.h"
+#include "pipelined_kernel.cuh"
 #include "serve_kernel.cuh"
 
 namespace rb200 {
@@ -218,6 +219,8 @@ struct Class {
     int tune_n[3] = {0, 0, 0};
     int last_tile = 1;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // tick start (while tuning) and end
+    bool pipelined = false;                      // 3-D Nq=8 Euler KG: the pipelined kernel
+    int32_t* d_status = nullptr;                 // its bounded waits report here
     int active = 0;
     bool launched = false;
 };
@@ -295,6 +298,8 @@ cudaError_t make_class(rb200_server* s, Class& c, const Req& r) {
     if (e == cudaSuccess) e = cudaMalloc(&c.d_tick, sizeof(int64_t));
     if (e == cudaSuccess) e = cudaMemsetAsync(c.d_nchunks, 0, sizeof(int32_t), c.stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(c.d_tick, 0, sizeof(int64_t), c.stream);
+    if (e == cudaSuccess) e = cudaMalloc(&c.d_status, sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemsetAsync(c.d_status, 0, sizeof(int32_t), c.stream);
     if (e == cudaSuccess) e = cudaEventCreate(&c.ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&c.ev1);
     if (e != cudaSuccess) return e;
@@ -304,6 +309,41 @@ cudaError_t make_class(rb200_server* s, Class& c, const Req& r) {
     c.chunk_elems = 8 * c.epb[1];
     int nsm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, s->device);
+    c.pipelined = c.dim == 3 && c.nq == 8 && c.combo == EUL_KG;
+    if (c.pipelined) {
+        // one configuration (the persistent TMA-pipelined kernel): nothing to tune
+        c.ntiles = 1;
+        c.tile = 0;
+        const int bps = pipelined_batch_blocks_per_sm(c.combo, c.prec);
+        if (bps <= 0) return cudaErrorInvalidConfiguration;
+        PipeArgs pa{};
+        pa.status = c.d_status;
+        pa.surface_rusanov = c.base.surface_rusanov;
+        pa.gamma = c.base.gamma;
+        for (int a = 0; a < 8; ++a)
+            for (int id = 0; id < 8; ++id)
+                pa.S[a * 8 + id] = c.base.D[a + 8 * id] * (c.base.w[a] / c.base.w[id]) - c.base.D[id + 8 * a];
+        for (int i = 0; i < 8; ++i) pa.w[i] = c.base.w[i];
+        cudaGraph_t g = nullptr;
+        e = cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return e;
+        for (int st = 0; st < 5 && e == cudaSuccess; ++st) {
+            pa.mode = kRKA[st] == 0.0 ? MODE_STAGE_FIRST : MODE_STAGE;
+            pa.rka = kRKA[st];
+            const PipeBatch b{c.d_solves, c.d_chunks, c.d_nchunks, c.d_tick, st, kRKB[st]};
+            e = launch_pipelined_batch(c.combo, c.prec, pa, b, bps * nsm, c.stream);
+        }
+        if (e == cudaSuccess) {
+            advance_tick_kernel<<<1, 1, 0, c.stream>>>(c.d_tick);
+            e = cudaGetLastError();
+        }
+        cudaError_t e2 = cudaStreamEndCapture(c.stream, &g);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&c.graph[0], g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) return e;
+        return cudaStreamSynchronize(c.stream);
+    }
     for (int t = 0; t < c.ntiles; ++t) {
         int bps = 0;
         BatchArgs probe{};
@@ -346,6 +386,7 @@ void destroy_class(Class& c) {
     if (c.d_chunks) cudaFree(c.d_chunks);
     if (c.d_nchunks) cudaFree(c.d_nchunks);
     if (c.d_tick) cudaFree(c.d_tick);
+    if (c.d_status) cudaFree(c.d_status);
     if (c.ev0) cudaEventDestroy(c.ev0);
     if (c.ev1) cudaEventDestroy(c.ev1);
     if (c.stream) cudaStreamDestroy(c.stream);
@@ -504,7 +545,13 @@ cudaError_t finish_tick(rb200_server* s, Class& c) {
         if (sv->steps_done < r.nsteps) continue;
         const size_t nstate = (size_t)r.np * r.ns * r.E;
         cudaError_t e = cudaSuccess;
-        if (r.q_out) e = cudaMemcpy(r.q_out, sv->desc.q[sv->steps_done & 1], nstate * 8, cudaMemcpyDeviceToHost);
+        if (c.pipelined) {  // a bounded wait of the pipelined kernel gave up: the result is void
+            int32_t status = 0;
+            e = cudaMemcpy(&status, c.d_status, sizeof(status), cudaMemcpyDeviceToHost);
+            if (e == cudaSuccess && status != 0) return cudaErrorTimeout;
+        }
+        if (e == cudaSuccess && r.q_out)
+            e = cudaMemcpy(r.q_out, sv->desc.q[sv->steps_done & 1], nstate * 8, cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) return e;
         r.state = 2;
         r.t_done = now_s();
@@ -558,6 +605,10 @@ void server_loop(rb200_server* s) {
                 if (e != cudaSuccess) break;
                 ++in_flight;
             }
+        }
+        if (e == cudaErrorTimeout) {
+            fail_server(s, RB200_ERR_TIMEOUT, "a bounded wait of the pipelined stage kernel expired");
+            break;
         }
         if (e != cudaSuccess) {
             fail_server(s, RB200_ERR_CUDA, std::string("tick: ") + cudaGetErrorString(e));

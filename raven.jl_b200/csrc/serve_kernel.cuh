@@ -12,22 +12,6 @@
 
 namespace rb200 {
 
-struct SolveDesc {
-    double* q[2];             // ping-pong state buffers
-    void* dq;                 // LSRK register (FP64 or FP32)
-    const double* elem_geo;   // (4, E) unwarped brick geometry
-    const int32_t* nbr;       // (2*dim, E) neighbour table
-    int64_t E;
-    double dt;
-    int64_t start_tick;       // class tick at which the solve's state sat in q[0]
-};
-
-struct Chunk {
-    int32_t solve;  // index into the descriptor table, or -1
-    int32_t count;  // elements in this chunk (0: empty slot)
-    int64_t first;  // first element of the chunk within the solve
-};
-
 struct BatchArgs {
     StageArgs base;               // class constants (D, w, gamma, advection velocity, mode, rka)
     const SolveDesc* solves;

@@ -1,8 +1,9 @@
 """The serving loop on the GPU (rb200_server_* through raven_b200.serving).
 
 What is checked, and to which tolerance:
-  * a served solve equals the same solve through the DGSEM handle's generic stage kernel
-    bit for bit (FP64 and FP32 bulk), and the oracle's FP64 LSRK(5,4) steps to 1e-12
+  * a served solve equals the same solve through the DGSEM handle bit for bit (FP64 and
+    FP32 bulk), on the same kernel: the pipelined kernel for 3-D Nq=8 Euler classes, the
+    generic stage kernel otherwise; and the oracle's FP64 LSRK(5,4) steps to 1e-12
     relative (max norm over the state array);
   * a solve's result in a mixed stream of other classes and other solves of its own class
     equals its result alone, bit for bit, whichever tile the autotuner picked;
@@ -57,7 +58,7 @@ def _spec(S, dim, nq, law, K, nsteps, prec=0):
     return f(dim, nq, K, nsteps, precision=prec)
 
 
-def _dgsem_generic(rb, spec, q0):
+def _dgsem_same_kernel(rb, spec, q0):
     grid = _grid(rb, spec)
     if spec.law == rb._lib.LAW_EULER:
         law, form = rb.EulerLaw(spec.dim), rb.FluxDifferencingForm(rb.KennedyGruberFlux())
@@ -65,7 +66,10 @@ def _dgsem_generic(rb, spec, q0):
         law, form = rb.AdvectionLaw(spec.dim, spec.advection_velocity[: spec.dim]), rb.WeakForm()
     dg = rb.DGSEM(law=law, grid=grid, volume_form=form, surface_numericalflux=rb.RusanovFlux(),
                   precision="fp64" if spec.precision == 0 else "fp32_bulk")
-    dg.set_kernel_path("generic")
+    pipelined = spec.dim == 3 and spec.nq == 8 and spec.law == rb._lib.LAW_EULER
+    dg.set_kernel_path("auto" if pipelined else "generic")
+    if pipelined:
+        assert dg.pipelined_ctas > 0
     q = rb.GridArray.from_numpy(q0)
     dq = q.similar()
     dg.lsrk54_steps(q, dq, 0.0, spec.dt, spec.nsteps)
@@ -92,13 +96,13 @@ def _pid(c):
 
 
 @pytest.mark.parametrize("case", PARITY, ids=_pid)
-def test_served_equals_dgsem_generic(rb, S, server, case):
+def test_served_equals_dgsem(rb, S, server, case):
     dim, nq, law, K, steps, prec = case
     spec = _spec(S, dim, nq, law, K, steps, prec)
     spec.q0 = _host_q0(rb, spec)
     q_srv, lat = server.wait(server.submit(spec))
     assert lat > 0
-    q_ref = _dgsem_generic(rb, spec, spec.q0)
+    q_ref = _dgsem_same_kernel(rb, spec, spec.q0)
     assert q_srv.shape == q_ref.shape
     assert np.array_equal(q_srv, q_ref), f"max diff {np.abs(q_srv - q_ref).max()}"
 
