@@ -116,6 +116,24 @@ rb200_status rb200_integrals(rb200_handle* h, const double* q, double* out, void
  * neighbour table the kernels use, for bit-exact comparison with facemaps(grid).vmapP. */
 rb200_status rb200_face_vmapP(rb200_handle* h, int64_t* vmapP_out, void* stream);
 
+/* Mortars of an adapted (non-conforming) grid, after rb200_create.  The reference's
+ * surfaceterm! leaves hanging faces uncoupled (vmapP = vmapM there,
+ * lobattocells.jl:2073-2074); with mortars each hanging face is coupled to its small
+ * neighbours instead, conservatively:
+ *   - the large face's trace is interpolated to each small face (tohalves operators,
+ *     lobattocells.jl:16-17);
+ *   - the surface flux is taken there;
+ *   - the large face gets the lumped L2 projection of the small faces' fluxes.
+ * mortars: host (2 + 2^(dim-1), M) int64 0-based columns: large element, its face
+ * (0..2*dim-1: x-, x+, y-, y+, z-, z+), the small elements by position on the face (first
+ * in-face direction fastest).  The large face and the small elements' opposite faces must
+ * be unconnected in the face maps.  IL, IU: (nq, nq) row-major interpolation from the
+ * LGL nodes to those of the lower / upper half, I[i*nq + j] = l_j((r_i -+ 1)/2).  PL, PU:
+ * the projections back, P[j*nq + i] = I[i*nq + j] w_i / (2 w_j).  Unwarped elements
+ * only; the generic stage kernel runs with one mortar launch before each stage. */
+rb200_status rb200_set_mortars(rb200_handle* h, const int64_t* mortars, int64_t num_mortars, const double* IL,
+                               const double* IU, const double* PL, const double* PU);
+
 /* Kernel selection: 0 = automatic (the persistent TMA-pipelined kernel for 3-D, nq = 8,
  * unwarped-brick flux differencing when the state pointers are 16-byte aligned, the
  * generic stage kernel otherwise), 1 = generic stage kernel only. */

@@ -70,6 +70,9 @@ def lib():
         L.og_grid_create.restype = P
         L.og_grid_create.argtypes = [ctypes.c_int, ctypes.c_int, P, P, P, P, ctypes.c_int, ctypes.c_double]
         L.og_grid_destroy.argtypes = [P]
+        L.og_grid_from_arrays.restype = P
+        L.og_grid_from_arrays.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int64, P, P, P, P, P, P]
+        L.og_grid_set_mortars.argtypes = [P, P, ctypes.c_int64, P, P, P, P]
         for name in ("og_grid_sizes", "og_grid_points", "og_grid_vmet", "og_grid_smet", "og_grid_vmapM",
                      "og_grid_vmapP", "og_grid_boundary", "og_grid_tree_coords"):
             getattr(L, name).argtypes = [P, P]
@@ -138,6 +141,28 @@ class Grid:
         s = np.zeros(8, dtype=np.int64)
         lib().og_grid_sizes(self.h, _ptr(s))
         self.dim, self.nq, self.np, self.nfp, self.nfaces, self.E, self.nvmet, self.nsmet = (int(v) for v in s)
+
+    @classmethod
+    def from_arrays(cls, dim, nq, points, volume_metrics, surface_metrics, vmapM, vmapP, boundarycodes,
+                    mortars=None, tohalves=None):
+        """A grid from the arrays of a generated grid (adapted grids); with mortars
+        ((2 + 2^(dim-1), M) int64 0-based) and tohalves (I_lower, I_upper, P_lower,
+        P_upper) the hanging faces are coupled through mortars."""
+        self = cls.__new__(cls)
+        keep = [np.asfortranarray(a, dtype=np.float64) for a in (points, volume_metrics, surface_metrics)]
+        keep += [np.asfortranarray(a, dtype=np.int64) for a in (vmapM, vmapP, boundarycodes)]
+        E = keep[0].shape[2]
+        self.h = lib().og_grid_from_arrays(dim, nq, E, *[_ptr(a) for a in keep])
+        self._keep = keep
+        s = np.zeros(8, dtype=np.int64)
+        lib().og_grid_sizes(self.h, _ptr(s))
+        self.dim, self.nq, self.np, self.nfp, self.nfaces, self.E, self.nvmet, self.nsmet = (int(v) for v in s)
+        if mortars is not None and mortars.size:
+            m = np.asfortranarray(mortars, dtype=np.int64)
+            ops = [np.ascontiguousarray(a, dtype=np.float64) for a in tohalves]
+            lib().og_grid_set_mortars(self.h, _ptr(m), m.shape[1], *[_ptr(a) for a in ops])
+            self._keep += [m] + ops
+        return self
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:

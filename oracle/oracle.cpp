@@ -128,6 +128,11 @@ struct og_grid {
     std::vector<double> smet;      // (nsmet, nfaces*nfp, E)
     std::vector<int64_t> vmapM, vmapP, bc;
     std::vector<double> MJI;       // DGSEM's MJI = 1 ./ MJ (dgsem.jl:56)
+    // mortars of an adapted grid: (2 + 2^(dim-1), M) columns (large element, its face,
+    // small elements); operators to and from the halves, (nq, nq) row-major [i][j]
+    std::vector<int64_t> mortars;
+    std::vector<double> IL, IU, PL, PU;
+    std::vector<uint8_t> ncface;   // (nfaces, E): 1 on faces coupled through a mortar
 };
 
 // Correctly rounded value of lo + (hi-lo)*i/K (Julia `range(lo, stop=hi, length=K+1)`).
@@ -794,7 +799,7 @@ static int num_states(const og_grid* g, const og_law* L) { return L->law == OG_L
 // ---------------------------------------------------------------------------------
 
 static void element_tendency(const og_grid* g, const Phys& Ph, double* dq, const double* q, bool increment,
-                             int64_t e, std::vector<double>& scratch) {
+                             int64_t e, std::vector<double>& scratch, const double* ncflux) {
     const int dim = g->dim, nq = g->nq, np = g->np, ns = Ph.ns, nv = g->nvmet;
     const double* D = g->D.data();
     auto Dm = [&](int i, int j) { return D[i + nq * j]; };
@@ -899,6 +904,15 @@ static void element_tendency(const og_grid* g, const Phys& Ph, double* dq, const
             int64_t em = idm / np, nm = idm % np;
             double qm[MAXS], qp[MAXS];
             for (int s = 0; s < ns; ++s) qm[s] = q[(size_t)np * ns * em + (size_t)np * s + nm];
+            if (ncflux && g->ncface[(size_t)nf * e + face]) {  // mortar face: its flux comes precomputed
+                const double mji = g->MJI[idm];
+                for (int s = 0; s < ns; ++s) {
+                    const double nfl = ncflux[(((size_t)nf * e + face) * ns + s) * nfp + i];
+                    double& t = dq[(size_t)np * ns * em + (size_t)np * s + nm];
+                    t = t - (fMJ * nfl) * mji;
+                }
+                continue;
+            }
             if (g->bc[(size_t)nf * e + face] == 0) {
                 int64_t idp = g->vmapP[j] - 1;
                 int64_t ep = idp / np, npn = idp % np;
@@ -917,15 +931,158 @@ static void element_tendency(const og_grid* g, const Phys& Ph, double* dq, const
     }
 }
 
+// Face-node index j of face f (x-, x+, y-, y+, z-, z+): volume node (lobattocells.jl:2012-2053).
+static int face_vol_node(int dim, int nq, int f, int j) {
+    const int d = f / 2, c = (f % 2) ? nq - 1 : 0;
+    if (dim == 2) return d == 0 ? c + nq * j : j + nq * c;
+    const int j1 = j % nq, j2 = j / nq;
+    if (d == 0) return c + nq * (j1 + nq * j2);
+    if (d == 1) return j1 + nq * (c + nq * j2);
+    return j1 + nq * (j2 + nq * c);
+}
+
+// Mortar fluxes of an adapted grid (a project-defined restatement: the reference's
+// surfaceterm! leaves non-conforming faces uncoupled).  For each mortar, the large
+// face's trace is interpolated to the nodes of each small face, the surface flux is
+// taken there with the large element's outward normal, the small element gets its
+// negative, and the large element gets the lumped L2 projection of the small faces'
+// fluxes back onto its face nodes.  ncflux: (nfaces, E) faces x (ns, nfp), only mortar
+// faces written.
+static void mortar_fluxes(const og_grid* g, const Phys& Ph, const double* q, double* ncflux) {
+    const int dim = g->dim, nq = g->nq, np = g->np, nfp = g->nfp, nf = g->nfaces, ns = Ph.ns;
+    const int nsmall = dim == 3 ? 4 : 2, mcols = 2 + nsmall;
+    const int nq2 = dim == 3 ? nq : 1;  // second in-face direction (none in 2-D)
+    const int64_t M = (int64_t)g->mortars.size() / mcols;
+    const double one = 1.0;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t m = 0; m < M; ++m) {
+        const int64_t* col = &g->mortars[(size_t)mcols * m];
+        const int64_t eC = col[0];
+        const int fC = (int)col[1], fF = fC ^ 1;
+        double n[3] = {0, 0, 0};
+        n[fC / 2] = (fC % 2) ? 1.0 : -1.0;
+        std::vector<double> qC((size_t)ns * nfp), nfm((size_t)nsmall * ns * nfp);
+        for (int j = 0; j < nfp; ++j) {
+            const int v = face_vol_node(dim, nq, fC, j);
+            for (int s = 0; s < ns; ++s) qC[(size_t)s * nfp + j] = q[(size_t)np * ns * eC + (size_t)np * s + v];
+        }
+        for (int k = 0; k < nsmall; ++k) {
+            const int64_t eF = col[2 + k];
+            const double* Ia = (k & 1) ? g->IU.data() : g->IL.data();
+            const double* Ib = (k >> 1) ? g->IU.data() : g->IL.data();
+            for (int j = 0; j < nfp; ++j) {
+                const int j1 = j % nq, j2 = j / nq;
+                double qi[MAXS], qf[MAXS], nfl[MAXS];
+                const int v = face_vol_node(dim, nq, fF, j);
+                for (int s = 0; s < ns; ++s) {
+                    double acc = 0.0;
+                    for (int b = 0; b < nq2; ++b) {
+                        double t = 0.0;
+                        for (int a = 0; a < nq; ++a) t = std::fma(Ia[j1 * nq + a], qC[(size_t)s * nfp + a + nq * b], t);
+                        acc = std::fma(dim == 3 ? Ib[j2 * nq + b] : one, t, acc);
+                    }
+                    qi[s] = acc;
+                    qf[s] = q[(size_t)np * ns * eF + (size_t)np * s + v];
+                }
+                surfaceflux(Ph, n, qi, qf, nfl);
+                for (int s = 0; s < ns; ++s) {
+                    nfm[((size_t)k * ns + s) * nfp + j] = nfl[s];
+                    ncflux[(((size_t)nf * eF + fF) * ns + s) * nfp + j] = -nfl[s];
+                }
+            }
+        }
+        for (int j = 0; j < nfp; ++j) {
+            const int j1 = j % nq, j2 = j / nq;
+            for (int s = 0; s < ns; ++s) {
+                double acc = 0.0;
+                for (int k = 0; k < nsmall; ++k) {
+                    const double* Pa = (k & 1) ? g->PU.data() : g->PL.data();
+                    const double* Pb = (k >> 1) ? g->PU.data() : g->PL.data();
+                    for (int b = 0; b < nq2; ++b) {
+                        double t = 0.0;
+                        for (int a = 0; a < nq; ++a)
+                            t = std::fma(Pa[j1 * nq + a], nfm[((size_t)k * ns + s) * nfp + a + nq * b], t);
+                        acc = std::fma(dim == 3 ? Pb[j2 * nq + b] : one, t, acc);
+                    }
+                }
+                ncflux[(((size_t)nf * eC + fC) * ns + s) * nfp + j] = acc;
+            }
+        }
+    }
+}
+
 extern "C" void og_tendency(const og_grid* g, const og_law* law, double* dq, const double* q, double t,
                             int increment, int64_t e0, int64_t e1) {
     (void)t;
     Phys Ph{g->dim, num_states(g, law), *law};
+    std::vector<double> ncflux;
+    if (!g->mortars.empty()) {
+        ncflux.assign((size_t)g->nfaces * g->E * Ph.ns * g->nfp, 0.0);
+        mortar_fluxes(g, Ph, q, ncflux.data());
+    }
+    const double* nc = ncflux.empty() ? nullptr : ncflux.data();
 #pragma omp parallel
     {
         std::vector<double> scratch;
 #pragma omp for schedule(dynamic, 16)
-        for (int64_t e = e0; e < e1; ++e) element_tendency(g, Ph, dq, q, increment != 0, e, scratch);
+        for (int64_t e = e0; e < e1; ++e) element_tendency(g, Ph, dq, q, increment != 0, e, scratch, nc);
+    }
+}
+
+// A grid from the arrays of a generated Raven grid (adapted grids are built on the host
+// by the product's forest module; their arrays are the oracle's input here).
+extern "C" og_grid* og_grid_from_arrays(int dim, int nq, int64_t E, const double* points, const double* vmet,
+                                        const double* smet, const int64_t* vmapM, const int64_t* vmapP,
+                                        const int64_t* bc) {
+    og_grid* g = new og_grid();
+    g->dim = dim;
+    g->nq = nq;
+    g->np = 1;
+    for (int d = 0; d < dim; ++d) g->np *= nq;
+    g->nfp = g->np / nq;
+    g->nfaces = 2 * dim;
+    g->nvmet = dim * dim + 2;
+    g->nsmet = dim + 2;
+    g->warp = OG_WARP_NONE;
+    g->E = E;
+    for (int d = 0; d < 3; ++d) {
+        g->K[d] = 1;
+        g->periodic[d] = 0;
+    }
+    g->r.resize(nq);
+    g->w.resize(nq);
+    g->D.resize(nq * nq);
+    og_lgl(nq, g->r.data(), g->w.data(), g->D.data());
+    g->tree.assign(E, {0, 0, 0});
+    const size_t np = g->np, nfp = g->nfp, nf = g->nfaces;
+    g->points.assign(points, points + np * dim * E);
+    g->vmet.assign(vmet, vmet + np * g->nvmet * E);
+    g->smet.assign(smet, smet + (size_t)g->nsmet * nf * nfp * E);
+    g->vmapM.assign(vmapM, vmapM + nf * nfp * E);
+    g->vmapP.assign(vmapP, vmapP + nf * nfp * E);
+    g->bc.assign(bc, bc + nf * E);
+    g->MJI.resize(np * E);
+    for (int64_t e = 0; e < E; ++e)
+        for (size_t n = 0; n < np; ++n) g->MJI[np * e + n] = 1.0 / g->vmet[n + np * (g->nvmet - 1 + (size_t)g->nvmet * e)];
+    return g;
+}
+
+// Mortars of an adapted grid: (2 + 2^(dim-1), M) int64 0-based, and the (nq, nq)
+// row-major operators I_lower, I_upper, P_lower, P_upper.
+extern "C" void og_grid_set_mortars(og_grid* g, const int64_t* mortars, int64_t M, const double* IL,
+                                    const double* IU, const double* PL, const double* PU) {
+    const int mcols = 2 + (g->dim == 3 ? 4 : 2);
+    g->mortars.assign(mortars, mortars + (size_t)mcols * M);
+    const size_t q2 = (size_t)g->nq * g->nq;
+    g->IL.assign(IL, IL + q2);
+    g->IU.assign(IU, IU + q2);
+    g->PL.assign(PL, PL + q2);
+    g->PU.assign(PU, PU + q2);
+    g->ncface.assign((size_t)g->nfaces * g->E, 0);
+    for (int64_t m = 0; m < M; ++m) {
+        const int64_t* col = &g->mortars[(size_t)mcols * m];
+        g->ncface[(size_t)g->nfaces * col[0] + col[1]] = 1;
+        for (int k = 2; k < mcols; ++k) g->ncface[(size_t)g->nfaces * col[k] + (col[1] ^ 1)] = 1;
     }
 }
 

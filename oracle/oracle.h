@@ -58,6 +58,19 @@ void og_grid_vmapP(const og_grid* g, int64_t* out);
 void og_grid_boundary(const og_grid* g, int64_t* out); /* (nfaces, E) */
 void og_grid_tree_coords(const og_grid* g, int32_t* out); /* (3, E) lattice coordinates */
 
+/* A grid from the arrays of a generated grid (used for adapted grids, which the product's
+ * forest module builds): points (Np, dim, E), volume metrics (Np, dim*dim+2, E), surface
+ * metrics (dim+2, nfaces*Nfp, E), vmapM/vmapP (nfaces*Nfp, E) 1-based, boundary codes
+ * (nfaces, E). */
+og_grid* og_grid_from_arrays(int dim, int nq, int64_t E, const double* points, const double* vmet,
+                             const double* smet, const int64_t* vmapM, const int64_t* vmapP,
+                             const int64_t* bc);
+/* Mortars coupling the hanging faces of an adapted grid: (2 + 2^(dim-1), M) int64 0-based
+ * columns (large element, its face, small elements by position on the face) and the
+ * (nq, nq) row-major interpolation to / projection from the two halves. */
+void og_grid_set_mortars(og_grid* g, const int64_t* mortars, int64_t M, const double* IL, const double* IU,
+                         const double* PL, const double* PU);
+
 /* Standalone LGL operators for nq points (computed in __float128, rounded). */
 void og_lgl(int nq, double* r, double* w, double* D);
 

@@ -32,13 +32,15 @@ import numpy as np
 
 from . import _lib
 from ._lib import RB200Error
+from .forest import AdaptCoarsen, AdaptNone, AdaptRefine, Forest, ForestGrid
 from .grids import Grid, brick_tree_order, jl_range, lobatto_operators
 
 __all__ = [
     "LobattoCell", "brick", "BrickGrid", "GridManager", "generate", "Grid", "AdvectionLaw", "EulerLaw",
     "RusanovFlux", "CentralFlux", "KennedyGruberFlux", "EntropyConservativeFlux", "WeakForm",
     "FluxDifferencingForm", "GridArray", "DGSEM", "LSRK54", "solve", "weightednorm", "integrals",
-    "jl_range", "RB200Error", "brick_tree_order",
+    "jl_range", "RB200Error", "brick_tree_order", "adapt", "AdaptRefine", "AdaptNone", "AdaptCoarsen",
+    "ForestGrid",
 ]
 
 # --------------------------------------------------------------------------- cells and grids
@@ -93,23 +95,42 @@ def brick(coordinates, periodic=None):
 
 
 class GridManager:
+    """GridManager(cell, coarsegrid; min_level) (src/gridmanager.jl:53-94): a forest of
+    trees on the brick, each refined uniformly to min_level, adaptable with adapt."""
+
     def __init__(self, cell, coarsegrid, min_level=0):
-        if min_level != 0:
-            raise NotImplementedError("only level-0 bricks (one element per tree) are generated")
         if len(coarsegrid.coordinates) != cell.dim:
             raise ValueError("cell and coarse grid dimensions differ")
         self.cell = cell
         self.coarsegrid = coarsegrid
+        K = [len(c) - 1 for c in coarsegrid.coordinates]
+        self.forest = Forest(cell.dim, K, coarsegrid.periodic, min_level=min_level)
+
+    def __len__(self):
+        return len(self.forest)
+
+
+def adapt(gm, flags):
+    """adapt!(gm, flags) (src/gridmanager.jl:160-173): refine (AdaptRefine), keep
+    (AdaptNone) or coarsen (AdaptCoarsen, whole families) each leaf, then balance 2:1
+    across faces."""
+    gm.forest.adapt(flags)
 
 
 def generate(arg, gm=None):
     """generate(gm) or generate(warp, gm) (src/gridmanager.jl:1084-1208).  `warp` maps
-    the coordinate arrays (x, y[, z]) to new ones; a warped grid gets curved metrics."""
+    the coordinate arrays (x, y[, z]) to new ones; a warped grid gets curved metrics.
+    A forest that is not one level-0 leaf per tree gives an adapted grid (ForestGrid)
+    whose hanging faces are coupled by mortars."""
     if gm is None:
         gm, warp = arg, None
     else:
         warp = arg
-    return Grid(gm.cell, gm.coarsegrid, warp=warp)
+    if all(L[1] == 0 for L in gm.forest.leaves):
+        return Grid(gm.cell, gm.coarsegrid, warp=warp)
+    if warp is not None:
+        raise NotImplementedError("warped adapted grids are not generated")
+    return ForestGrid(gm.cell, gm.forest, gm.coarsegrid.coordinates)
 
 
 # ------------------------------------------------------------------------ laws and fluxes
@@ -287,6 +308,17 @@ class DGSEM:
                 L.rb200_destroy(h)
             self._h = None
             raise RB200Error(st, msg)
+        mortars = getattr(grid, "mortars", None)
+        if mortars is not None and mortars.size:
+            m = np.asfortranarray(mortars, dtype=np.int64)
+            ops = [np.ascontiguousarray(a, dtype=np.float64) for a in grid.tohalves]
+            st = L.rb200_set_mortars(h, m.ctypes.data_as(ctypes.c_void_p), m.shape[1],
+                                     *[a.ctypes.data_as(ctypes.c_void_p) for a in ops])
+            if st != 0:
+                msg = L.rb200_last_error(h).decode()
+                L.rb200_destroy(h)
+                self._h = None
+                raise RB200Error(st, msg)
         info = (ctypes.c_int64 * 9)()
         L.rb200_get_info(h, info, 9)
         self.info = list(info)

@@ -35,6 +35,7 @@ EXPORTED = [
     "rb200_integrals",
     "rb200_face_vmapP",
     "rb200_get_info",
+    "rb200_set_mortars",
     "rb200_set_kernel_path",
     "rb200_sync_status",
     "rb200_weighted_sums_noalloc",
@@ -147,6 +148,7 @@ def lib():
     L.rb200_face_vmapP.argtypes = [P, P, P]
     L.rb200_get_info.argtypes = [P, P, I32]
     L.rb200_set_kernel_path.argtypes = [P, I32]
+    L.rb200_set_mortars.argtypes = [P, P, I64, P, P, P, P]
     L.rb200_sync_status.argtypes = [P, P]
     L.rb200_weighted_sums_noalloc.argtypes = [P, P, I32, I32, I64, P, P]
     L.rb200_last_error.argtypes = [P]

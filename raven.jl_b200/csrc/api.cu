@@ -56,6 +56,11 @@ struct rb200_handle {
     int use_graphs = 1;
     int pipe_grid = 0;            // CTAs of the pipelined kernel (0: not eligible)
     double pipe_S[64] = {0};      // D[a,id] w[a] / w[id] - D[id,a]
+    // mortars of an adapted grid (rb200_set_mortars)
+    int64_t nmortars = 0;
+    int64_t* d_mortars = nullptr;
+    double* d_ncflux = nullptr;
+    MortarArgs mortar{};
     std::string err;
 };
 
@@ -126,6 +131,10 @@ void free_all(rb200_handle* h) {
                     h->d_dq32,     h->d_hq,   h->d_hdq,     h->d_partial, h->d_sums, h->d_status};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    if (h->d_mortars) cudaFree(h->d_mortars);
+    if (h->d_ncflux) cudaFree(h->d_ncflux);
+    h->d_mortars = nullptr;
+    h->d_ncflux = nullptr;
     h->d_elem_geo = h->d_vgeo = h->d_sgeo = h->d_w = h->d_qtmp = h->d_hq = h->d_hdq = h->d_partial = h->d_sums =
         nullptr;
     h->d_nbr = nullptr;
@@ -138,6 +147,13 @@ bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 // One stage (or tendency) launch: the pipelined kernel when the configuration and the
 // pointers allow it, the generic stage kernel otherwise.
 cudaError_t launch_any(rb200_handle* h, const StageArgs& a, cudaStream_t st) {
+    if (h->nmortars > 0) {  // adapted grid: the mortar fluxes of this q, then the generic kernel
+        MortarArgs m = h->mortar;
+        m.q = a.q_in;
+        cudaError_t e = launch_mortars(h->dim, h->nq, h->law == RB200_LAW_EULER, h->prec, m, st);
+        if (e != cudaSuccess) return e;
+        return launch_stage(h->dim, h->nq, h->combo, h->geom, h->prec, a, st);
+    }
     const bool stage_mode = a.mode >= MODE_STAGE;
     const bool eligible = h->kernel_path == 0 && h->pipe_grid > 0 && aligned16(a.q_in) && aligned16(a.dq) &&
                           (!stage_mode || aligned16(a.q_out)) &&
@@ -170,6 +186,7 @@ StageArgs base_args(const rb200_handle* h) {
     a.vgeo = h->d_vgeo;
     a.sgeo = h->d_sgeo;
     a.nbr = h->d_nbr;
+    a.ncflux = h->d_ncflux;
     a.E = h->E;
     a.surface_rusanov = h->sflux == RB200_FLUX_RUSANOV ? 1 : 0;
     a.gamma = h->gamma;
@@ -586,6 +603,60 @@ rb200_status rb200_face_vmapP(rb200_handle* h, int64_t* vmapP_out, void* stream)
     DeviceGuard guard(h->device);
     cudaError_t e = launch_face_vmapP(h->d_nbr, h->dim, h->nq, h->E, vmapP_out, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "vmapP kernel launch");
+    return RB200_OK;
+}
+
+rb200_status rb200_set_mortars(rb200_handle* h, const int64_t* mortars, int64_t num_mortars, const double* IL,
+                               const double* IU, const double* PL, const double* PU) {
+    if (!h) return RB200_ERR_BAD_ARG;
+    if (num_mortars < 0 || (num_mortars > 0 && (!mortars || !IL || !IU || !PL || !PU))) return RB200_ERR_BAD_ARG;
+    if (h->nmortars > 0) return fail(h, RB200_ERR_BAD_ARG, "mortars are already set");
+    if (num_mortars == 0) return RB200_OK;
+    if (h->geom != GEOM_AFFINE)
+        return fail(h, RB200_ERR_UNSUPPORTED, "mortars are implemented for unwarped (affine) elements only");
+    const int nf = h->nf, mcols = 2 + (h->dim == 3 ? 4 : 2);
+    DeviceGuard guard(h->device);
+    std::vector<int32_t> nbr((size_t)nf * h->E);
+    cudaError_t ce = cudaMemcpy(nbr.data(), h->d_nbr, nbr.size() * sizeof(int32_t), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return cuda_fail(h, ce, "mortar set-up");
+    for (int64_t m = 0; m < num_mortars; ++m) {
+        const int64_t* col = mortars + (size_t)mcols * m;
+        if (col[0] < 0 || col[0] >= h->E || col[1] < 0 || col[1] >= nf)
+            return fail(h, RB200_ERR_BAD_ARG, "mortar: large element or face out of range");
+        // a hanging face is unconnected in the face maps (vmapP = vmapM)
+        if (nbr[(size_t)nf * col[0] + col[1]] != -1) return fail(h, RB200_ERR_SHAPE, "mortar: the large face is connected");
+        nbr[(size_t)nf * col[0] + col[1]] = -2;
+        for (int k = 2; k < mcols; ++k) {
+            if (col[k] < 0 || col[k] >= h->E) return fail(h, RB200_ERR_BAD_ARG, "mortar: small element out of range");
+            int32_t& v = nbr[(size_t)nf * col[k] + (col[1] ^ 1)];
+            if (v != -1) return fail(h, RB200_ERR_SHAPE, "mortar: a small face is connected or in two mortars");
+            v = -2;
+        }
+    }
+    const size_t nflux = (size_t)nf * h->E * h->ns * h->nfp;
+    rb200_status st;
+    if ((st = dev_alloc(h, &h->d_mortars, (size_t)mcols * num_mortars)) != RB200_OK) return st;
+    if ((st = dev_alloc(h, &h->d_ncflux, nflux)) != RB200_OK) return st;
+    ce = cudaMemcpy(h->d_mortars, mortars, (size_t)mcols * num_mortars * sizeof(int64_t), cudaMemcpyHostToDevice);
+    if (ce == cudaSuccess) ce = cudaMemset(h->d_ncflux, 0, nflux * sizeof(double));
+    if (ce == cudaSuccess) ce = cudaMemcpy(h->d_nbr, nbr.data(), nbr.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    if (ce != cudaSuccess) return cuda_fail(h, ce, "mortar upload");
+    MortarArgs& a = h->mortar;
+    std::memset(&a, 0, sizeof(a));
+    a.ncflux = h->d_ncflux;
+    a.mortars = h->d_mortars;
+    a.M = num_mortars;
+    a.surface_rusanov = h->sflux == RB200_FLUX_RUSANOV ? 1 : 0;
+    a.gamma = h->gamma;
+    for (int d = 0; d < 3; ++d) a.adv[d] = h->adv[d];
+    const int q2 = h->nq * h->nq;
+    std::memcpy(a.IL, IL, q2 * sizeof(double));
+    std::memcpy(a.IU, IU, q2 * sizeof(double));
+    std::memcpy(a.PL, PL, q2 * sizeof(double));
+    std::memcpy(a.PU, PU, q2 * sizeof(double));
+    h->nmortars = num_mortars;
+    h->pipe_grid = 0;  // the pipelined kernel has no mortar faces
+    free_graph(h);
     return RB200_OK;
 }
 

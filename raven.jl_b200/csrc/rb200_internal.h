@@ -40,7 +40,9 @@ struct StageArgs {
     const double* elem_geo;  // affine: (4, E): drdx, dsdy, dtdz, J
     const double* vgeo;      // curved: (Np, dim*dim+2, E): wJ*dRdX[dir,d] (dir-major), MJI, MJ
     const double* sgeo;      // curved: (dim+1, 2*dim*Nfp, E): n, wsJ
-    const int32_t* nbr;      // (2*dim, E): neighbour element across each face, -1 = boundary
+    const int32_t* nbr;      // (2*dim, E): neighbour element across each face, -1 = boundary,
+                             // -2 = a mortar face (its flux is in ncflux)
+    const double* ncflux;    // mortar face fluxes ((2*dim, E) faces x (Ns, Nfp)), or null
     int64_t E;
     int32_t mode;
     int32_t surface_rusanov;  // 1 Rusanov, 0 central
@@ -51,6 +53,20 @@ struct StageArgs {
     double D[kMaxNq * kMaxNq];  // D[i + nq*j] = l_j'(r_i)
     double w[kMaxNq];
 };
+
+// Mortars of an adapted grid (mortar.cu).
+struct MortarArgs {
+    const double* q;          // q_in (Np, Ns, E)
+    double* ncflux;           // (2*dim, E) faces x (Ns, Nfp)
+    const int64_t* mortars;   // (2 + 2^(dim-1), M): large element, its face, small elements
+    int64_t M;
+    int32_t surface_rusanov;
+    double gamma;
+    double adv[3];
+    double IL[kMaxNq * kMaxNq], IU[kMaxNq * kMaxNq];  // to the halves, [i*nq + j]
+    double PL[kMaxNq * kMaxNq], PU[kMaxNq * kMaxNq];  // projections back, [j*nq + i]
+};
+cudaError_t launch_mortars(int dim, int nq, int euler, int fp32, const MortarArgs& a, cudaStream_t s);
 
 // Serving loop: one running solve of a class, and one chunk of its elements.
 struct SolveDesc {

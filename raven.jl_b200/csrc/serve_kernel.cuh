@@ -44,6 +44,7 @@ __global__ void __launch_bounds__(Shape<DIM, NQ, EPBX>::THREADS, 1)
         P.sgeo = nullptr;
         P.nbr = sd.nbr;
         P.rkb_dt = B.rkb * sd.dt;
+        P.ncflux = nullptr;
         for (int g = 0; g < c.count; g += S::EPB) {
             const int64_t e = c.first + g + el;
             stage_element<DIM, NQ, COMBO, GEOM, T, EPBX>(B.base, P, e, g + el < c.count, smem_raw);

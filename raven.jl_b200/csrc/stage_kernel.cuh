@@ -100,10 +100,11 @@ struct ElemPtrs {
     const double* sgeo;
     const int32_t* nbr;
     double rkb_dt;
+    const double* ncflux;
 };
 
 __device__ __forceinline__ ElemPtrs elem_ptrs(const StageArgs& A) {
-    return ElemPtrs{A.q_in, A.q_out, A.dq, A.elem_geo, A.vgeo, A.sgeo, A.nbr, A.rkb_dt};
+    return ElemPtrs{A.q_in, A.q_out, A.dq, A.elem_geo, A.vgeo, A.sgeo, A.nbr, A.rkb_dt, A.ncflux};
 }
 
 // One element per group of Np threads: the whole fused stage for element e.  All
@@ -416,7 +417,10 @@ __device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs
                 wsJ = __ldg(sg + DIM);
             }
             T nf[NS];
-            if constexpr (C::ADV) {
+            if (ne == -2) {  // mortar face of an adapted grid: the flux comes from the mortar kernel
+#pragma unroll
+                for (int s = 0; s < NS; ++s) nf[s] = (T)__ldg(P.ncflux + (((size_t)e * NF + f) * NS + s) * NFP + j);
+            } else if constexpr (C::ADV) {
                 T an;
                 if constexpr (AFF) an = (T)A.adv[dir] * nv[dir];
                 else {

@@ -34,11 +34,8 @@ def _legendre(n, x):
     return p1, dp
 
 
-def lobatto_operators(nq):
-    """LGL points, weights and derivative matrix D[i, j] = l_j'(r_i) for nq points.
-
-    Computed with 80-digit decimal arithmetic and rounded once to double, as Raven does
-    with BigFloat (src/lobattocells.jl:1-47)."""
+def _lgl_decimal(nq):
+    """LGL points of nq nodes in 80-digit decimal arithmetic."""
     getcontext().prec = 80
     N = nq - 1
     x = [Decimal(-1)] + [None] * (N - 1) + [Decimal(1)]
@@ -57,6 +54,16 @@ def lobatto_operators(nq):
         x[j], x[N - j] = -s, s
     if nq % 2 == 1:
         x[N // 2] = Decimal(0)
+    return x
+
+
+def lobatto_operators(nq):
+    """LGL points, weights and derivative matrix D[i, j] = l_j'(r_i) for nq points.
+
+    Computed with 80-digit decimal arithmetic and rounded once to double, as Raven does
+    with BigFloat (src/lobattocells.jl:1-47)."""
+    x = _lgl_decimal(nq)
+    N = nq - 1
     w = []
     for j in range(nq):
         P, _ = _legendre(N, x[j])
@@ -78,6 +85,36 @@ def lobatto_operators(nq):
     D[0, 0] = -N * (N + 1) / 4
     D[N, N] = N * (N + 1) / 4
     return np.array([float(v) for v in x]), np.array([float(v) for v in w]), D
+
+
+def tohalves_operators(nq):
+    """Interpolation from the LGL nodes of [-1, 1] to those of the lower and upper halves
+    (tohalves of lobattooperators_1d, src/lobattocells.jl:16-17, 30), I[i, j] =
+    l_j((r_i -+ 1) / 2), and the matching lumped L2 projections back,
+    P[j, i] = I[i, j] w_i / (2 w_j).  All in 80-digit decimals, rounded once.
+
+    Returns (I_lower, I_upper, P_lower, P_upper), each (nq, nq)."""
+    x = _lgl_decimal(nq)
+    N = nq - 1
+    w = []
+    for j in range(nq):
+        P, _ = _legendre(N, x[j])
+        w.append(Decimal(2) / (N * (N + 1) * P * P))
+
+    def lagrange(j, t):
+        v = Decimal(1)
+        for k in range(nq):
+            if k != j:
+                v *= (t - x[k]) / (x[j] - x[k])
+        return v
+
+    out = []
+    for shift in (-1, 1):
+        Id = [[lagrange(j, (x[i] + shift) / 2) for j in range(nq)] for i in range(nq)]
+        I = np.array([[float(v) for v in row] for row in Id])
+        P = np.array([[float(Id[i][j] * w[i] / (2 * w[j])) for i in range(nq)] for j in range(nq)])
+        out.append((I, P))
+    return out[0][0], out[1][0], out[0][1], out[1][1]
 
 
 def jl_range(lo, hi, length):
