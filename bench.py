@@ -46,6 +46,10 @@ WORKLOADS = {
                                          warp=True),
     "adv2d_weak_n4_16_fp64": dict(dim=2, N=4, K=16, L=1.0, law="advection", vflux="weak", precision="fp64",
                                   warp=False),
+    # adapted: 4^3 trees on the periodic unit cube, refined twice within radius 0.25 of the
+    # centre (2:1 balanced, hanging faces coupled by mortars), N = 5, density pulse
+    "euler3d_kg_n5_adapted_fp32bulk": dict(dim=3, N=5, K=4, L=1.0, law="euler", vflux="kg", precision="fp32_bulk",
+                                           warp=False, adapted=True),
 }
 SERVE_WORKLOAD = "serve_poisson_mix_fp32bulk"
 DEFAULT = "euler3d_kg_n7_32_fp64"
@@ -65,7 +69,27 @@ def load_product():
     return mod
 
 
-def config_json(name, w):
+def config_json(name, w, grid=None):
+    if grid is not None and w.get("adapted"):
+        return {
+            "workload": name,
+            "equation": "euler",
+            "dim": w["dim"],
+            "polynomial_order": w["N"],
+            "elements": grid.E,
+            "nodes": grid.E * grid.np,
+            "trees": w["K"] ** w["dim"],
+            "refinement": "two rounds within radius 0.25 of the centre of the periodic unit cube, 2:1 face balance",
+            "mortars": int(grid.mortars.shape[1]),
+            "volume_form": "flux_differencing_kennedy_gruber",
+            "surface_flux": "rusanov",
+            "precision": w["precision"],
+            "geometry": "adapted brick (hanging faces coupled by mortars)",
+            "time_stepper": "LSRK54",
+            "initial_data": "density pulse 1 + 0.2 exp(-|x - c|^2 / 0.01) at rest, pressure 1",
+            "l2_flush": "none: the state (6.4 MB) is L2-resident",
+            "parallelism": "replicas",
+        }
     return {
         "workload": name,
         "equation": "euler" if w["law"] == "euler" else "advection",
@@ -103,10 +127,23 @@ def setup(rb, w, device):
 
     dim, N, K, L = w["dim"], w["N"], w["K"], w["L"]
     cell = rb.LobattoCell(*([N + 1] * dim))
-    cg = rb.brick(tuple(rb.jl_range(0.0, L, K + 1) for _ in range(dim)), (True,) * dim)
+    coords = tuple(rb.jl_range(0.0, L, K + 1) for _ in range(dim))
+    cg = rb.brick(coords, (True,) * dim)
     gm = rb.GridManager(cell, cg)
+    if w.get("adapted"):
+        from raven_b200.forest import sphere_refinement_flags
+
+        centre = (L / 2,) * dim
+        for _ in range(2):
+            rb.adapt(gm, sphere_refinement_flags(gm.forest, coords, centre, L / 4))
     grid = rb.generate(sine_warp(L, dim), gm) if w["warp"] else rb.generate(gm)
-    if w["law"] == "euler":
+    if w.get("adapted"):
+        # density pulse rho = 1 + 0.2 exp(-|x - c|^2 / 0.01) at rest, uniform pressure 1
+        law = rb.EulerLaw(dim)
+        q0 = ic.density_pulse(grid, law, center=(L / 2,) * dim, amplitude=0.2, width2=0.01)
+        form = rb.FluxDifferencingForm(rb.KennedyGruberFlux())
+        dt = 0.4 * grid.min_node_distance() / ic.max_wavespeed(grid, law, q0)
+    elif w["law"] == "euler":
         law = rb.EulerLaw(dim)
         u0 = 0.5 * math.sqrt(law.gamma)
         q0 = ic.isentropic_vortex(grid, law, beta=5.0, u0=u0, center=(L / 2, L / 2))
@@ -212,6 +249,31 @@ def stage_bytes_per_launch(w, nodes, ns):
     return per_step / 5.0
 
 
+def adapted_oracle(w):
+    """The adapted workload's grid and initial state for the oracle: the forest and its
+    arrays are generated on the host (setup, untimed), the oracle couples the hanging
+    faces with its own mortar restatement."""
+    import numpy as np
+
+    import oracle as O
+
+    rb = load_product()
+    from raven_b200 import initial_conditions as ic
+    from raven_b200.forest import sphere_refinement_flags
+
+    dim, N, K, L = w["dim"], w["N"], w["K"], w["L"]
+    coords = tuple(rb.jl_range(0.0, L, K + 1) for _ in range(dim))
+    gm = rb.GridManager(rb.LobattoCell(*([N + 1] * dim)), rb.brick(coords, (True,) * dim))
+    for _ in range(2):
+        rb.adapt(gm, sphere_refinement_flags(gm.forest, coords, (L / 2,) * dim, L / 4))
+    grid = rb.generate(gm)
+    og = O.Grid.from_arrays(dim, N + 1, grid.points, grid.volume_metrics, grid.surface_metrics, grid.vmapM,
+                            grid.vmapP, grid.boundarycodes, grid.mortars, grid.tohalves)
+    law = O.Law(O.LAW_EULER, dim, form=O.FORM_FLUXDIFF, volume_flux=O.FLUX_KG)
+    q = ic.density_pulse(grid, rb.EulerLaw(dim), center=(L / 2,) * dim, amplitude=0.2, width2=0.01)
+    return og, law, np.asfortranarray(q), f"the adapted grid itself ({grid.E} elements, {grid.mortars.shape[1]} mortars)"
+
+
 def cpu_sample(w, max_seconds=20.0):
     """The oracle (C++ FP64 restatement) on the host cores: LSRK(5,4) steps of the same
     element type, law and flux on a small brick, repeated for up to ~max_seconds."""
@@ -220,8 +282,14 @@ def cpu_sample(w, max_seconds=20.0):
     dim, N = w["dim"], w["N"]
     K = 8 if dim == 3 else 16
     warp = O.WARP_SINE if w["warp"] else O.WARP_NONE
-    og = O.Grid(dim, N + 1, [K] * dim, [0.0] * dim, [w["L"]] * dim, [True] * dim, warp, 0.1)
-    if w["law"] == "euler":
+    if w.get("adapted"):
+        og, law, q, where = adapted_oracle(w)
+    else:
+        og = O.Grid(dim, N + 1, [K] * dim, [0.0] * dim, [w["L"]] * dim, [True] * dim, warp, 0.1)
+        where = f"a {K}^{dim}-element periodic brick"
+    if w.get("adapted"):
+        pass
+    elif w["law"] == "euler":
         law = O.Law(O.LAW_EULER, dim, form=O.FORM_FLUXDIFF, volume_flux=O.FLUX_KG)
         q = og.initial_condition(law, 4, [5.0, 0.5 * math.sqrt(1.4), w["L"] / 2, w["L"] / 2])
     else:
@@ -243,7 +311,7 @@ def cpu_sample(w, max_seconds=20.0):
         "cores": O.num_threads(),
         "kind": "port",
         "sample": f"{steps} LSRK(5,4) steps of the same scheme (dim {dim}, N {N}, {w['vflux']}, "
-                  f"{'warped' if w['warp'] else 'brick'}) on a {K}^{dim}-element periodic brick, FP64, "
+                  f"{'warped' if w['warp'] else 'brick'}) on {where}, FP64, "
                   f"OpenMP over elements, {el:.1f} s",
     }
 
@@ -259,8 +327,14 @@ def run_reference(args, w):
     # per-step sample size: keep (warmup + steps) * step time within ~2 minutes
     K = {3: 4, 2: 8}[dim]
     warp = O.WARP_SINE if w["warp"] else O.WARP_NONE
-    og = O.Grid(dim, N + 1, [K] * dim, [0.0] * dim, [w["L"]] * dim, [True] * dim, warp, 0.1)
-    if w["law"] == "euler":
+    if w.get("adapted"):
+        og, law, q, where = adapted_oracle(w)
+    else:
+        og = O.Grid(dim, N + 1, [K] * dim, [0.0] * dim, [w["L"]] * dim, [True] * dim, warp, 0.1)
+        where = f"a {K}^{dim}-element periodic brick"
+    if w.get("adapted"):
+        pass
+    elif w["law"] == "euler":
         law = O.Law(O.LAW_EULER, dim, form=O.FORM_FLUXDIFF, volume_flux=O.FLUX_KG)
         q = og.initial_condition(law, 4, [5.0, 0.5 * math.sqrt(1.4), w["L"] / 2, w["L"] / 2])
     else:
@@ -296,7 +370,7 @@ def run_reference(args, w):
             "unit": UNIT,
             "cores": O.num_threads(),
             "kind": "port",
-            "sample": f"each step: one LSRK(5,4) step of the same scheme on a {K}^{dim}-element periodic brick "
+            "sample": f"each step: one LSRK(5,4) step of the same scheme on {where} "
                       f"(N {N}), FP64 C++ restatement of Raven's CPU path, OpenMP over elements",
         },
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -605,7 +679,30 @@ def main(argv=None):
 
     # accuracy of the run: L2 distance to the exactly advected vortex, and conservation
     l2_err = None
-    if w["law"] == "euler":
+    fp64_cmp = None
+    if w.get("adapted"):
+        # the FP32-bulk state against an FP64 run of the same steps (the FP64 path is
+        # parity-tested against the oracle), and the drift of the conserved integrals
+        dg64 = rb.DGSEM(law=law, grid=grid, volume_form=rb.FluxDifferencingForm(rb.KennedyGruberFlux()),
+                        surface_numericalflux=rb.RusanovFlux(), precision="fp64", device=local)
+        q64 = rb.GridArray.from_numpy(q0)
+        dq64 = q64.similar()
+        dg64.lsrk54_steps(q64, dq64, 0.0, dt, args.warmup + args.steps)
+        I0 = rb.integrals(dg64, rb.GridArray.from_numpy(q0))
+        I32, I64 = rb.integrals(dg, q), rb.integrals(dg64, q64)
+        diff = q64.copy()
+        diff.data.sub_(q.data)
+        fp64_cmp = {
+            "l2_diff_vs_fp64_relative": rb.weightednorm(dg64, diff) / rb.weightednorm(dg64, q64),
+            "max_diff_vs_fp64_relative": float(diff.data.abs().max().item() / q64.data.abs().max().item()),
+            "conservation_drift_fp32bulk": [abs(a - b) / max(abs(a), 1e-300) for a, b in zip(I32, I0)],
+            "conservation_drift_fp64": [abs(a - b) / max(abs(a), 1e-300) for a, b in zip(I64, I0)],
+            "elements": grid.E,
+            "mortars": int(grid.mortars.shape[1]),
+            "levels": [int(c) for c in np.bincount([L_[1] for L_ in grid.forest.leaves])],
+        }
+        del diff, q64, dq64, dg64
+    elif w["law"] == "euler":
         from raven_b200 import initial_conditions as ic
 
         T = (args.warmup + args.steps) * dt
@@ -672,13 +769,14 @@ def main(argv=None):
             "vs_baseline": None,
             "dtype": "f32+f64" if w["precision"] == "fp32_bulk" else "f64",
             "data": "synthetic",
-            "config": config_json(args.workload, w),
+            "config": config_json(args.workload, w, grid),
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": sampler.summary(),
             "l2_error_vs_exact": l2_err,
+            "adapted": fp64_cmp,
             "dt": dt,
         }
         print(json.dumps(line))
