@@ -695,8 +695,9 @@ def main(argv=None):
         fp64_cmp = {
             "l2_diff_vs_fp64_relative": rb.weightednorm(dg64, diff) / rb.weightednorm(dg64, q64),
             "max_diff_vs_fp64_relative": float(diff.data.abs().max().item() / q64.data.abs().max().item()),
-            "conservation_drift_fp32bulk": [abs(a - b) / max(abs(a), 1e-300) for a, b in zip(I32, I0)],
-            "conservation_drift_fp64": [abs(a - b) / max(abs(a), 1e-300) for a, b in zip(I64, I0)],
+            # |integral(t) - integral(0)| over max(|integral(0)|, mass): the momenta start at 0
+            "conservation_drift_fp32bulk": [abs(a - b) / max(abs(b), abs(I0[0])) for a, b in zip(I32, I0)],
+            "conservation_drift_fp64": [abs(a - b) / max(abs(b), abs(I0[0])) for a, b in zip(I64, I0)],
             "elements": grid.E,
             "mortars": int(grid.mortars.shape[1]),
             "levels": [int(c) for c in np.bincount([L_[1] for L_ in grid.forest.leaves])],
