@@ -43,12 +43,17 @@ typedef enum rb200_status {
 enum { RB200_LAW_ADVECTION = 0, RB200_LAW_EULER = 1 };
 /* Volume forms: WeakForm(), FluxDifferencingForm(flux) (dgsem.jl:5-17). */
 enum { RB200_FORM_WEAK = 0, RB200_FORM_FLUXDIFF = 1 };
-/* Numerical fluxes (numericalfluxes.jl:39-55, euler.jl:150-216). */
+/* Numerical fluxes (numericalfluxes.jl:39-55, euler.jl:93-300).  Surface fluxes:
+ * Rusanov and Central for every law and precision; Kennedy-Gruber, entropy conservative
+ * (their two-point flux contracted with the normal), Roe and matrix dissipation for the
+ * Euler law in FP64. */
 enum {
     RB200_FLUX_CENTRAL = 0,
     RB200_FLUX_KENNEDY_GRUBER = 1,
     RB200_FLUX_ENTROPY_CONSERVATIVE = 2,
-    RB200_FLUX_RUSANOV = 3
+    RB200_FLUX_RUSANOV = 3,
+    RB200_FLUX_ROE = 4,
+    RB200_FLUX_MATRIX = 5
 };
 /* Arithmetic of the volume/surface bulk.  FP32_BULK keeps the state q, the
  * geometry and all reductions in FP64 and the LSRK register dq in FP32. */
@@ -62,7 +67,7 @@ typedef struct rb200_desc {
     int64_t num_elements;     /* E (local elements; no ghosts on one rank) */
     int32_t volume_form;      /* RB200_FORM_* */
     int32_t volume_flux;      /* two-point flux of FluxDifferencingForm */
-    int32_t surface_flux;     /* RB200_FLUX_RUSANOV or RB200_FLUX_CENTRAL */
+    int32_t surface_flux;     /* RB200_FLUX_*; see the flux enum for what each law takes */
     int32_t precision;        /* RB200_PRECISION_* */
     double gamma;             /* Euler ratio of specific heats (Raven default 7//5) */
     double advection_velocity[3];
@@ -111,6 +116,23 @@ rb200_status rb200_weightednorm(rb200_handle* h, const double* q, double* out, v
 
 /* Conservation integrals out[s] = sum(MJ .* q_s)  (FP64, synchronous).  out: host, Ns. */
 rb200_status rb200_integrals(rb200_handle* h, const double* q, double* out, void* stream);
+
+/* entropyintegral(dg, q) = sum(MJ .* entropy.(q)) (measures.jl:23-27) into *out (host;
+ * FP64, deterministic, synchronous).  Replaces Raven.BalanceLaws.entropyintegral. */
+rb200_status rb200_entropy_integral(rb200_handle* h, const double* q, double* out, void* stream);
+
+/* entropyproduct(dg, p, q) = sum(MJ .* dot.(entropyvariables.(p), q)) (measures.jl:28-33)
+ * into *out (host; synchronous). */
+rb200_status rb200_entropy_product(rb200_handle* h, const double* p, const double* q, double* out, void* stream);
+
+/* `nsteps` steps of RLSRK54(dg, q, dt) (odesolvers.jl:73-161, 153-156): LSRK(5,4) stages
+ * with the entropy production of each stage, then the relaxation q = q0 + gamma (q - q0)
+ * with gamma solving eta(q) = eta0 + gamma deta.  dq: FP64 LSRK register (zero before the
+ * first step); *gamma: the relaxation parameter carried between steps (1 at the start),
+ * updated in place.  FP64 handles only.  Synchronous: the scalar solve reads two device
+ * sums per iterate on the host. */
+rb200_status rb200_rlsrk54_step(rb200_handle* h, double* q, double* dq, double* gamma, double time, double dt,
+                                int32_t nsteps, void* stream);
 
 /* Rebuilds vmapP (1-based, (2*dim*nq^(dim-1), E) int64) on the device from the
  * neighbour table the kernels use, for bit-exact comparison with facemaps(grid).vmapP. */

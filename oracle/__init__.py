@@ -23,7 +23,7 @@ LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 
 LAW_ADVECTION, LAW_EULER = 0, 1
 FORM_WEAK, FORM_FLUXDIFF = 0, 1
-FLUX_CENTRAL, FLUX_KG, FLUX_EC, FLUX_RUSANOV = 0, 1, 2, 3
+FLUX_CENTRAL, FLUX_KG, FLUX_EC, FLUX_RUSANOV, FLUX_ROE, FLUX_MATRIX = 0, 1, 2, 3, 4, 5
 WARP_NONE, WARP_SINE, WARP_IDENTITY_CURVED = 0, 1, 2
 
 
@@ -83,6 +83,11 @@ def lib():
         L.og_lsrk54_step.argtypes = [P, P, P, P, ctypes.c_double, ctypes.c_double]
         L.og_solve.restype = ctypes.c_int64
         L.og_solve.argtypes = [P, P, P, ctypes.c_double, ctypes.c_double]
+        L.og_entropy_sums.argtypes = [P, P, P, P, ctypes.c_double, P, P]
+        L.og_rlsrk54_step.restype = ctypes.c_int
+        L.og_rlsrk54_step.argtypes = [P, P, P, P, P, ctypes.c_double, ctypes.c_double]
+        L.og_solve_rlsrk.restype = ctypes.c_int64
+        L.og_solve_rlsrk.argtypes = [P, P, P, ctypes.c_double, ctypes.c_double, P]
         L.og_weightednorm.restype = ctypes.c_double
         L.og_weightednorm.argtypes = [P, P, ctypes.c_int, P]
         L.og_integrals.argtypes = [P, P, ctypes.c_int, P]
@@ -225,6 +230,26 @@ class Grid:
 
     def solve(self, law, q, dt, timeend):
         return lib().og_solve(self.h, ctypes.byref(law.c), _ptr(q), dt, timeend)
+
+    def entropy_sums(self, law, base, direction=None, c=0.0, k=None):
+        """(sum MJ eta(p), sum MJ v(p).k) for p = base + c * direction."""
+        out = np.zeros(2)
+        base = np.asfortranarray(base, dtype=np.float64)
+        d = None if direction is None else np.asfortranarray(direction, dtype=np.float64)
+        kk = None if k is None else np.asfortranarray(k, dtype=np.float64)
+        lib().og_entropy_sums(self.h, ctypes.byref(law.c), _ptr(base), None if d is None else _ptr(d), c,
+                              None if kk is None else _ptr(kk), _ptr(out))
+        return out
+
+    def rlsrk54_step(self, law, q, dq, gamma, time, dt):
+        """One RLSRK(5,4) step in place; gamma is a 1-element float64 array carried
+        between steps.  Returns the Newton iterations."""
+        return lib().og_rlsrk54_step(self.h, ctypes.byref(law.c), _ptr(q), _ptr(dq), _ptr(gamma), time, dt)
+
+    def solve_rlsrk(self, law, q, dt, timeend):
+        gamma = np.ones(1)
+        steps = lib().og_solve_rlsrk(self.h, ctypes.byref(law.c), _ptr(q), dt, timeend, _ptr(gamma))
+        return steps, gamma[0]
 
     def weightednorm(self, q, ns):
         comp = np.zeros(ns)

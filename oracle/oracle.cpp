@@ -775,17 +775,125 @@ static void twopointflux(const Phys& P, int which, const double* q1, const doubl
     }
 }
 
-// surfaceflux (numericalfluxes.jl:27-37, 44-50)
+// F' * n for a (dim, ns) flux
+static void contract(const Phys& P, const double* F, const double* n, double* nf) {
+    for (int s = 0; s < P.ns; ++s) {
+        double v = F[s] * n[0];
+        for (int d = 1; d < P.dim; ++d) v = v + F[d * MAXS + s] * n[d];
+        nf[s] = v;
+    }
+}
+
+// entropyvariables (euler.jl:79-91)
+static void entropyvariables(const Phys& P, const double* q, double* v) {
+    const int dim = P.dim;
+    const double g = P.L.gamma, rho = q[0], p = pressure(P, q);
+    const double sv = std::log(p / std::pow(rho, g)), b = rho / (2 * p);
+    double u[3];
+    for (int d = 0; d < dim; ++d) u[d] = q[1 + d] / rho;
+    v[0] = (g - sv) / (g - 1) - dotv(u, u, dim) * b;
+    for (int d = 0; d < dim; ++d) v[1 + d] = 2 * b * u[d];
+    v[dim + 1] = -2 * b;
+}
+
+// Roe flux (euler.jl:93-149)
+static void roeflux(const Phys& P, const double* n, const double* qm, const double* qp, double* nf) {
+    const int dim = P.dim, ns = P.ns;
+    const double g = P.L.gamma;
+    double Fm[3 * MAXS], Fp[3 * MAXS], fm[MAXS], fp[MAXS];
+    flux(P, qm, Fm);
+    flux(P, qp, Fp);
+    contract(P, Fm, n, fm);
+    contract(P, Fp, n, fp);
+    const double rm = qm[0], rp = qp[0], pm = pressure(P, qm), pp = pressure(P, qp);
+    double um[3], up[3];
+    for (int d = 0; d < dim; ++d) { um[d] = qm[1 + d] / rm; up[d] = qp[1 + d] / rp; }
+    const double hm = qm[dim + 1] / rm + pm / rm, hp = qp[dim + 1] / rp + pp / rp;
+    const double cm = std::sqrt(g * pm / rm), cp = std::sqrt(g * pp / rp);
+    const double sm = std::sqrt(rm), sp = std::sqrt(rp);
+    auto roe_avg = [&](double a, double b) { return (sm * a + sp * b) / (sm + sp); };  // numericalfluxes.jl:23
+    const double rho = std::sqrt(rm * rp), h = roe_avg(hm, hp), c = roe_avg(cm, cp);
+    double u[3], du[3];
+    for (int d = 0; d < dim; ++d) { u[d] = roe_avg(um[d], up[d]); du[d] = up[d] - um[d]; }
+    const double un = dotv(u, n, dim), dun = dotv(du, n, dim);
+    const double drho = rp - rm, dp = pp - pm, ci2 = 1 / (c * c);
+    const double w1 = std::fabs(un - c) * (dp - rho * c * dun) * ci2 / 2;
+    const double w2 = std::fabs(un + c) * (dp + rho * c * dun) * ci2 / 2;
+    const double w3 = std::fabs(un) * (drho - dp * ci2);
+    const double w4 = std::fabs(un) * rho;
+    double D[MAXS];
+    D[0] = (w1 + w2 + w3) / 2;
+    for (int k = 0; k < dim; ++k)
+        D[1 + k] = (w1 * (u[k] - c * n[k]) + w2 * (u[k] + c * n[k]) + w3 * u[k] + w4 * (du[k] - dun * n[k])) / 2;
+    D[dim + 1] = (w1 * (h - c * un) + w2 * (h + c * un) + w3 * dotv(u, u, dim) / 2 + w4 * (dotv(u, du, dim) - un * dun)) / 2;
+    for (int s = 0; s < ns; ++s) nf[s] = (fm[s] + fp[s]) / 2 - D[s];
+}
+
+// matrix-dissipation flux (euler.jl:218-300): the entropy-conservative flux minus a
+// dissipation built on the jump of the entropy variables
+static void matrixflux(const Phys& P, const double* n, const double* qm, const double* qp, double* nf) {
+    const int dim = P.dim, ns = P.ns;
+    const double g = P.L.gamma;
+    double F[3 * MAXS];
+    twopointflux(P, OG_FLUX_EC, qm, qp, F);
+    contract(P, F, n, nf);
+    const double rm = qm[0], rp = qp[0], pm = pressure(P, qm), pp = pressure(P, qp);
+    double um[3], up[3], ua[3];
+    for (int d = 0; d < dim; ++d) {
+        um[d] = qm[1 + d] / rm;
+        up[d] = qp[1 + d] / rp;
+        ua[d] = (um[d] + up[d]) / 2;
+    }
+    const double bm = rm / (2 * pm), bp = rp / (2 * pp);
+    const double rlog = logavg(rm, rp), blog = logavg(bm, bp);
+    const double pavg = ((rm + rp) / 2) / (2 * ((bm + bp) / 2));
+    const double u2bar = 2 * std::sqrt(dotv(ua, ua, dim)) - (std::sqrt(dotv(um, um, dim)) + std::sqrt(dotv(up, up, dim))) / 2;
+    const double hbar = g / (2 * blog * (g - 1)) + u2bar / 2;
+    const double cbar = std::sqrt(g * pavg / rlog);
+    const double un = dotv(ua, n, dim);
+    double umc[3], upc[3], ut[3], vm[MAXS], vp[MAXS], dv[MAXS];
+    for (int d = 0; d < dim; ++d) {
+        umc[d] = ua[d] - cbar * n[d];
+        upc[d] = ua[d] + cbar * n[d];
+        ut[d] = ua[d] - un * n[d];
+    }
+    entropyvariables(P, qm, vm);
+    entropyvariables(P, qp, vp);
+    for (int s = 0; s < ns; ++s) dv[s] = vp[s] - vm[s];
+    const double l1 = std::fabs(un - cbar) * rlog / (2 * g);
+    const double l2 = std::fabs(un) * rlog * (g - 1) / g;
+    const double l3 = std::fabs(un + cbar) * rlog / (2 * g);
+    const double l4 = std::fabs(un) * pavg;
+    const double* dvm = dv + 1;
+    const double dve = dv[dim + 1];
+    const double w1 = l1 * (dv[0] + dotv(umc, dvm, dim) + (hbar - cbar * un) * dve);
+    const double w2 = l2 * (dv[0] + dotv(ua, dvm, dim) + u2bar / 2 * dve);
+    const double w3 = l3 * (dv[0] + dotv(upc, dvm, dim) + (hbar + cbar * un) * dve);
+    const double ndv = dotv(n, dvm, dim);
+    double D[MAXS];
+    D[0] = w1 + w2 + w3;
+    for (int k = 0; k < dim; ++k)
+        D[1 + k] = w1 * umc[k] + w2 * ua[k] + w3 * upc[k] + l4 * (dvm[k] - ndv * n[k] + dve * ut[k]);
+    D[dim + 1] = w1 * (hbar - cbar * un) + w2 * u2bar / 2 + w3 * (hbar + cbar * un) +
+                 l4 * (dotv(ut, dvm, dim) + dve * (dotv(ua, ua, dim) - un * un));
+    for (int s = 0; s < ns; ++s) nf[s] = nf[s] - D[s] / 2;
+}
+
+// surfaceflux (numericalfluxes.jl:27-37, 44-50; euler.jl:93-149, 218-300)
 static void surfaceflux(const Phys& P, const double* n, const double* qm, const double* qp, double* nf) {
     const int dim = P.dim, ns = P.ns;
+    const int which = P.L.surface_flux;
+    if (P.L.law == OG_LAW_EULER && which == OG_FLUX_ROE) return roeflux(P, n, qm, qp, nf);
+    if (P.L.law == OG_LAW_EULER && which == OG_FLUX_MATRIX) return matrixflux(P, n, qm, qp, nf);
     double Fc[3 * MAXS];
-    twopointflux(P, OG_FLUX_CENTRAL, qm, qp, Fc);
+    // the default surfaceflux: the flux's two-point form contracted with n
+    twopointflux(P, which == OG_FLUX_RUSANOV ? OG_FLUX_CENTRAL : which, qm, qp, Fc);
     for (int s = 0; s < ns; ++s) {
         double v = Fc[s] * n[0];
         for (int d = 1; d < dim; ++d) v = v + Fc[d * MAXS + s] * n[d];
         nf[s] = v;
     }
-    if (P.L.surface_flux == OG_FLUX_RUSANOV) {
+    if (which == OG_FLUX_RUSANOV) {
         double wm = wavespeed(P, n, qm), wp = wavespeed(P, n, qp);
         double mx = std::max(wm, wp);
         for (int s = 0; s < ns; ++s) nf[s] = nf[s] - (mx * (qp[s] - qm[s])) / 2;
@@ -1159,6 +1267,132 @@ extern "C" void og_integrals(const og_grid* g, const double* q, int ns, double* 
             }
         out[s] = (double)acc;
     }
+}
+
+// ---------------------------------------------------------------------------------
+// Entropy measures and the relaxation Runge-Kutta step
+// (src/balancelaws/measures.jl:23-33, odesolvers.jl:73-161)
+// ---------------------------------------------------------------------------------
+
+static double entropy_at(const Phys& P, const double* q) {  // euler.jl:70-77, advection.jl:20
+    if (P.L.law == OG_LAW_ADVECTION) return q[0] * q[0] / 2;
+    const double g = P.L.gamma, rho = q[0], p = pressure(P, q);
+    const double sv = std::log(p / std::pow(rho, g));
+    return -rho * sv / (g - 1);
+}
+
+extern "C" void og_entropy_sums(const og_grid* g, const og_law* law, const double* base, const double* dir,
+                                double c, const double* k, double* out) {
+    Phys P{g->dim, num_states(g, law), *law};
+    const int np = g->np, ns = P.ns;
+    long double eta = 0, prod = 0;
+    for (int64_t e = 0; e < g->E; ++e)
+        for (int n = 0; n < np; ++n) {
+            const double mj = g->vmet[n + (size_t)np * (g->nvmet - 1 + (size_t)g->nvmet * e)];
+            double q[MAXS], v[MAXS];
+            for (int s = 0; s < ns; ++s) {
+                const size_t i = (size_t)np * ns * e + (size_t)np * s + n;
+                q[s] = dir ? base[i] + c * dir[i] : base[i];  // @. q = q0 + γ * k
+            }
+            eta += (long double)(mj * entropy_at(P, q));
+            if (k) {
+                if (P.L.law == OG_LAW_ADVECTION) v[0] = q[0];  // advection.jl:21
+                else entropyvariables(P, q, v);
+                double vk = v[0] * k[(size_t)np * ns * e + n];
+                for (int s = 1; s < ns; ++s) vk = vk + v[s] * k[(size_t)np * ns * e + (size_t)np * s + n];
+                prod += (long double)(mj * vk);
+            }
+        }
+    out[0] = (double)eta;
+    out[1] = (double)prod;
+}
+
+// rkb_full: the b coefficients of the standard Butcher form (odesolvers.jl:91-97)
+static void rkb_full(double* bf) {
+    bf[4] = RKB[4];
+    for (int i = 3; i >= 0; --i) bf[i] = RKA[i + 1] * bf[i + 1] + RKB[i];
+}
+
+// The relaxation solve r(γ) = η(q0 + γk) - η0 - γ dη = 0 with r'(γ) = v(q0 + γk).k - dη
+// (odesolvers.jl:137-148).  The reference calls NLsolve's default trust-region method
+// with ftol = 10 eps; for this scalar problem its steps are Newton steps, accepted when
+// they reduce r^2 by more than the 1e-4 fraction of the predicted reduction.  A rejected
+// step ends the solve here (the residual is at round-off), where NLsolve would retry
+// shorter steps until its 1000-iteration limit.
+template <class Eval>
+static int relaxation_newton(Eval eval, double* gamma) {
+    const double ftol = 10 * 2.220446049250313e-16;
+    double gm = *gamma, F, J;
+    eval(gm, &F, &J);
+    int it = 0;
+    if (std::fabs(F) <= ftol) return it;
+    while (it < 1000) {
+        ++it;
+        if (!(J != 0)) break;
+        const double step = -F / J;
+        const double gn = gm + step;
+        double Fn, Jn;
+        eval(gn, &Fn, &Jn);
+        if (!(Fn * Fn < F * F * (1 - 1e-4))) break;
+        gm = gn;
+        F = Fn;
+        J = Jn;
+        if (std::fabs(F) <= ftol || step == 0) break;
+    }
+    *gamma = gm;
+    return it;
+}
+
+extern "C" int og_rlsrk54_step(const og_grid* g, const og_law* law, double* q, double* dq, double* gamma,
+                               double time, double dt) {
+    (void)time;
+    const int64_t n = (int64_t)g->np * num_states(g, law) * g->E;
+    std::vector<double> q0(q, q + n), k(n);
+    double bf[5], sums[2];
+    rkb_full(bf);
+    og_entropy_sums(g, law, q0.data(), nullptr, 0.0, nullptr, sums);
+    const double eta0 = sums[0];
+    double deta = -0.0;
+    for (int st = 0; st < 5; ++st) {
+        const double a = RKA[st];
+        for (int64_t i = 0; i < n; ++i) dq[i] = dq[i] * a;
+        og_tendency(g, law, k.data(), q, time, 0, 0, g->E);
+        for (int64_t i = 0; i < n; ++i) dq[i] = dq[i] + k[i];
+        og_entropy_sums(g, law, q, nullptr, 0.0, k.data(), sums);
+        deta = deta + bf[st] * dt * sums[1];
+        const double c = RKB[st] * dt;
+        for (int64_t i = 0; i < n; ++i) q[i] = q[i] + c * dq[i];
+    }
+    for (int64_t i = 0; i < n; ++i) k[i] = q[i] - q0[i];
+    auto eval = [&](double gm, double* F, double* J) {
+        double s2[2];
+        og_entropy_sums(g, law, q0.data(), k.data(), gm, k.data(), s2);
+        *F = s2[0] - eta0 - gm * deta;
+        *J = s2[1] - deta;
+    };
+    const int its = relaxation_newton(eval, gamma);
+    for (int64_t i = 0; i < n; ++i) q[i] = q0[i] + *gamma * k[i];
+    return its;
+}
+
+extern "C" int64_t og_solve_rlsrk(const og_grid* g, const og_law* law, double* q, double dt, double timeend,
+                                  double* gamma) {
+    const int64_t n = (int64_t)g->np * num_states(g, law) * g->E;
+    std::vector<double> dq(n, 0.0);
+    double time = 0.0;
+    int64_t steps = 0;
+    while (true) {
+        ++steps;
+        bool final = false;
+        if (time + dt >= timeend) {
+            dt = timeend - time;
+            final = true;
+        }
+        og_rlsrk54_step(g, law, q, dq.data(), gamma, time, dt);
+        time += dt;
+        if (final) break;
+    }
+    return steps;
 }
 
 // ---------------------------------------------------------------------------------

@@ -25,14 +25,14 @@ typedef struct og_grid og_grid;
 /* Law / scheme selection (mirrors Raven's types; see oracle.cpp for citations). */
 enum { OG_LAW_ADVECTION = 0, OG_LAW_EULER = 1 };
 enum { OG_FORM_WEAK = 0, OG_FORM_FLUXDIFF = 1 };
-enum { OG_FLUX_CENTRAL = 0, OG_FLUX_KG = 1, OG_FLUX_EC = 2, OG_FLUX_RUSANOV = 3 };
+enum { OG_FLUX_CENTRAL = 0, OG_FLUX_KG = 1, OG_FLUX_EC = 2, OG_FLUX_RUSANOV = 3, OG_FLUX_ROE = 4, OG_FLUX_MATRIX = 5 };
 enum { OG_WARP_NONE = 0, OG_WARP_SINE = 1, OG_WARP_IDENTITY_CURVED = 2 };
 
 typedef struct {
     int law;          /* OG_LAW_* */
     int form;         /* OG_FORM_* */
     int volume_flux;  /* two-point flux for OG_FORM_FLUXDIFF */
-    int surface_flux; /* OG_FLUX_RUSANOV (or CENTRAL) */
+    int surface_flux; /* OG_FLUX_*: Rusanov, central, or (Euler) KG, EC, Roe, matrix */
     double gamma;     /* Euler */
     double adv[3];    /* advection velocity */
 } og_law;
@@ -101,6 +101,19 @@ double og_weightednorm(const og_grid* g, const double* q, int ns, double* compon
 
 /* sum(MJ .* q_s) per field (conservation integrals). */
 void og_integrals(const og_grid* g, const double* q, int ns, double* out);
+
+/* entropyintegral / entropyproduct (measures.jl:23-33) in one pass over p = base + c*dir
+ * (dir NULL: p = base): out[0] = sum MJ eta(p), out[1] = sum MJ v(p).k (0 when k is NULL). */
+void og_entropy_sums(const og_grid* g, const og_law* law, const double* base, const double* dir, double c,
+                     const double* k, double* out);
+
+/* One RLSRK(5,4) step (odesolvers.jl:118-151); *gamma carries the relaxation parameter
+ * between steps (1 at the start).  Returns the Newton iterations taken. */
+int og_rlsrk54_step(const og_grid* g, const og_law* law, double* q, double* dq, double* gamma, double time,
+                    double dt);
+
+/* solve!(q, timeend, RLSRK54(dg, q, dt)) with adjust_final; returns steps taken. */
+int64_t og_solve_rlsrk(const og_grid* g, const og_law* law, double* q, double dt, double timeend, double* gamma);
 
 int og_num_threads(void);
 void og_set_num_threads(int n);

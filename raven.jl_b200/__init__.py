@@ -37,8 +37,9 @@ from .grids import Grid, brick_tree_order, jl_range, lobatto_operators
 
 __all__ = [
     "LobattoCell", "brick", "BrickGrid", "GridManager", "generate", "Grid", "AdvectionLaw", "EulerLaw",
-    "RusanovFlux", "CentralFlux", "KennedyGruberFlux", "EntropyConservativeFlux", "WeakForm",
-    "FluxDifferencingForm", "GridArray", "DGSEM", "LSRK54", "solve", "weightednorm", "integrals",
+    "RusanovFlux", "CentralFlux", "KennedyGruberFlux", "EntropyConservativeFlux", "RoeFlux", "MatrixFlux", "WeakForm",
+    "FluxDifferencingForm", "GridArray", "DGSEM", "LSRK54", "RLSRK54", "solve", "weightednorm", "integrals",
+    "entropyintegral", "entropyproduct",
     "jl_range", "RB200Error", "brick_tree_order", "adapt", "AdaptRefine", "AdaptNone", "AdaptCoarsen",
     "ForestGrid",
 ]
@@ -185,6 +186,18 @@ class KennedyGruberFlux:
 
 class EntropyConservativeFlux:
     code = _lib.FLUX_ENTROPY_CONSERVATIVE
+
+
+class RoeFlux:
+    """Roe's approximate Riemann solver for the Euler law (balancelaws/euler.jl:93-149)."""
+
+    code = _lib.FLUX_ROE
+
+
+class MatrixFlux:
+    """Entropy-stable matrix-dissipation flux for the Euler law (balancelaws/euler.jl:218-300)."""
+
+    code = _lib.FLUX_MATRIX
 
 
 class WeakForm:
@@ -389,6 +402,29 @@ class LSRK54:
             self.time += self.dt
 
 
+class RLSRK54:
+    """RLSRK54(rhs!, q, dt; t0 = 0) (src/balancelaws/odesolvers.jl:73-161): LSRK(5,4) with
+    relaxation, so that the entropy integral changes by exactly the stages' entropy
+    production (entropy-conservative fluxes then conserve it to round-off).  `gamma` is
+    the relaxation parameter, carried between steps.  FP64 operators only."""
+
+    def __init__(self, dg, q, dt, t0=0.0):
+        self.dg = dg
+        self.dt = float(dt)
+        self.time = float(t0)
+        self.gamma = 1.0
+        self.dq = q.similar()  # fill!(dq, 0)
+
+    def dostep(self, q, nsteps=1):
+        """dostep!(q, rlsrk) (odesolvers.jl:118-151), `nsteps` times with the same dt."""
+        g = ctypes.c_double(self.gamma)
+        _lib.check(_lib.lib().rb200_rlsrk54_step(self.dg._h, q.ptr(), self.dq.ptr(), ctypes.byref(g), self.time,
+                                                 self.dt, int(nsteps), _stream_ptr()), self.dg._h)
+        self.gamma = g.value
+        for _ in range(nsteps):
+            self.time += self.dt
+
+
 def solve(q, timeend, solver, after_step=None, adjust_final=True):
     """solve!(q, timeend, solver; after_step, adjust_final) (odesolvers.jl:9-30).
 
@@ -429,6 +465,20 @@ def weightednorm(dg, q, p=2, componentwise=False):
     _lib.check(_lib.lib().rb200_weightednorm(dg._h, q.ptr(), out, _stream_ptr()), dg._h)
     vals = list(out)
     return vals[: q.ns] if componentwise else vals[q.ns]
+
+
+def entropyintegral(dg, q):
+    """entropyintegral(dg, q) = sum(MJ .* entropy(q)) (src/balancelaws/measures.jl:23-27)."""
+    out = ctypes.c_double()
+    _lib.check(_lib.lib().rb200_entropy_integral(dg._h, q.ptr(), ctypes.byref(out), _stream_ptr()), dg._h)
+    return out.value
+
+
+def entropyproduct(dg, p, q):
+    """entropyproduct(dg, p, q) = sum(MJ .* entropyvariables(p) . q) (measures.jl:28-33)."""
+    out = ctypes.c_double()
+    _lib.check(_lib.lib().rb200_entropy_product(dg._h, p.ptr(), q.ptr(), ctypes.byref(out), _stream_ptr()), dg._h)
+    return out.value
 
 
 def integrals(dg, q):

@@ -22,7 +22,7 @@ STATUS = {
 }
 LAW_ADVECTION, LAW_EULER = 0, 1
 FORM_WEAK, FORM_FLUXDIFF = 0, 1
-FLUX_CENTRAL, FLUX_KENNEDY_GRUBER, FLUX_ENTROPY_CONSERVATIVE, FLUX_RUSANOV = 0, 1, 2, 3
+FLUX_CENTRAL, FLUX_KENNEDY_GRUBER, FLUX_ENTROPY_CONSERVATIVE, FLUX_RUSANOV, FLUX_ROE, FLUX_MATRIX = 0, 1, 2, 3, 4, 5
 PRECISION_FP64, PRECISION_FP32_BULK = 0, 1
 
 EXPORTED = [
@@ -33,6 +33,9 @@ EXPORTED = [
     "rb200_lsrk54_step_host",
     "rb200_weightednorm",
     "rb200_integrals",
+    "rb200_entropy_integral",
+    "rb200_entropy_product",
+    "rb200_rlsrk54_step",
     "rb200_face_vmapP",
     "rb200_get_info",
     "rb200_set_mortars",
@@ -145,6 +148,9 @@ def lib():
     L.rb200_lsrk54_step_host.argtypes = [P, P, D, D, I32, P]
     L.rb200_weightednorm.argtypes = [P, P, P, P]
     L.rb200_integrals.argtypes = [P, P, P, P]
+    L.rb200_entropy_integral.argtypes = [P, P, P, P]
+    L.rb200_entropy_product.argtypes = [P, P, P, P, P]
+    L.rb200_rlsrk54_step.argtypes = [P, P, P, P, D, D, I32, P]
     L.rb200_face_vmapP.argtypes = [P, P, P]
     L.rb200_get_info.argtypes = [P, P, I32]
     L.rb200_set_kernel_path.argtypes = [P, I32]

@@ -61,6 +61,10 @@ struct rb200_handle {
     int64_t* d_mortars = nullptr;
     double* d_ncflux = nullptr;
     MortarArgs mortar{};
+    // RLSRK(5,4) workspace (rb200_rlsrk54_step): q0, the stage tendency k, and device sums
+    double* d_rq0 = nullptr;
+    double* d_rk = nullptr;
+    double* d_rsums = nullptr;  // (eta, prod) pairs: [0] eta0, [1..5] stages, [6] relaxation solve
     std::string err;
 };
 
@@ -135,6 +139,10 @@ void free_all(rb200_handle* h) {
     if (h->d_ncflux) cudaFree(h->d_ncflux);
     h->d_mortars = nullptr;
     h->d_ncflux = nullptr;
+    for (double** p : {&h->d_rq0, &h->d_rk, &h->d_rsums}) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
     h->d_elem_geo = h->d_vgeo = h->d_sgeo = h->d_w = h->d_qtmp = h->d_hq = h->d_hdq = h->d_partial = h->d_sums =
         nullptr;
     h->d_nbr = nullptr;
@@ -189,6 +197,7 @@ StageArgs base_args(const rb200_handle* h) {
     a.ncflux = h->d_ncflux;
     a.E = h->E;
     a.surface_rusanov = h->sflux == RB200_FLUX_RUSANOV ? 1 : 0;
+    a.surface_flux = h->sflux;
     a.gamma = h->gamma;
     for (int d = 0; d < 3; ++d) a.adv[d] = h->adv[d];
     std::memcpy(a.D, h->D, sizeof(a.D));
@@ -277,6 +286,105 @@ rb200_status run_steps(rb200_handle* h, double* q, void* dq, double dt, int32_t 
     return RB200_OK;
 }
 
+RelaxGeo relax_geo(const rb200_handle* h) {
+    RelaxGeo G;
+    std::memset(&G, 0, sizeof(G));
+    G.elem_geo = h->d_elem_geo;
+    G.vgeo = h->d_vgeo;
+    G.dim = h->dim;
+    G.nq = h->nq;
+    G.np = h->np;
+    G.geom = h->geom;
+    G.euler = h->law == RB200_LAW_EULER ? 1 : 0;
+    G.E = h->E;
+    G.gamma = h->gamma;
+    std::memcpy(G.w, h->w, sizeof(G.w));
+    return G;
+}
+
+// (sum MJ eta(base + c dir), sum MJ v(base + c dir).k) into host out[0..1]
+rb200_status entropy_sums_host(rb200_handle* h, const double* base, const double* dir, double c, const double* k,
+                               double* out, cudaStream_t s) {
+    cudaError_t e = launch_entropy_sums(relax_geo(h), base, dir, c, k, h->d_partial, h->red_blocks, h->d_sums, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, h->d_sums, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "entropy reduction");
+    return RB200_OK;
+}
+
+// rkb_full: the b coefficients of the standard Butcher form (odesolvers.jl:91-97)
+void rkb_full(double* bf) {
+    bf[4] = RKB[4];
+    for (int i = 3; i >= 0; --i) bf[i] = RKA[i + 1] * bf[i + 1] + RKB[i];
+}
+
+// One RLSRK(5,4) step (odesolvers.jl:118-151).  The relaxation solve r(gamma) = 0 with
+// r(gamma) = eta(q0 + gamma k) - eta0 - gamma deta and r'(gamma) = v(q0 + gamma k).k - deta
+// takes Newton steps from the previous gamma, as the reference's NLsolve trust-region
+// method does for a scalar problem whose steps stay inside the region: a step is kept
+// when it reduces r^2 by more than 1e-4 of the predicted reduction; the solve ends at
+// |r| <= 10 eps (the reference's ftol) or at the first step that is not kept (the
+// residual is then at round-off), after at most 1000 iterations.
+rb200_status rlsrk_step(rb200_handle* h, double* q, double* dq, double* gamma, double dt, cudaStream_t s) {
+    const int64_t n = (int64_t)h->np * h->ns * h->E;
+    const RelaxGeo G = relax_geo(h);
+    cudaError_t e = cudaMemcpyAsync(h->d_rq0, q, n * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess)
+        e = launch_entropy_sums(G, h->d_rq0, nullptr, 0.0, nullptr, h->d_partial, h->red_blocks, h->d_rsums, s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "relaxation set-up");
+    StageArgs a = base_args(h);
+    a.mode = MODE_TENDENCY_SET;
+    a.dq = h->d_rk;
+    for (int st = 0; st < 5; ++st) {
+        a.q_in = q;
+        e = launch_any(h, a, s);  // k = RHS(q)
+        if (e == cudaSuccess)
+            e = launch_rlsrk_stage(G, q, dq, h->d_rk, RKA[st], RKB[st] * dt, h->d_partial, h->red_blocks,
+                                   h->d_rsums + 2 * (1 + st), s);
+        if (e != cudaSuccess) return cuda_fail(h, e, "relaxation stage");
+    }
+    e = launch_state_diff(q, h->d_rq0, h->d_rk, n, s);  // k = q - q0
+    double sums[12];
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sums, h->d_rsums, sizeof(sums), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "relaxation stages");
+    double bf[5];
+    rkb_full(bf);
+    const double eta0 = sums[0];
+    double deta = -0.0;
+    for (int st = 0; st < 5; ++st) deta = deta + bf[st] * dt * sums[2 * (1 + st) + 1];
+    const double ftol = 10 * 2.220446049250313e-16;
+    auto eval = [&](double g, double* F, double* J) -> rb200_status {
+        double s2[2];
+        rb200_status rs = entropy_sums_host(h, h->d_rq0, h->d_rk, g, h->d_rk, s2, s);
+        *F = s2[0] - eta0 - g * deta;
+        *J = s2[1] - deta;
+        return rs;
+    };
+    double g = *gamma, F, J;
+    rb200_status rs = eval(g, &F, &J);
+    if (rs != RB200_OK) return rs;
+    if (!(std::fabs(F) <= ftol)) {
+        for (int it = 0; it < 1000; ++it) {
+            if (!(J != 0)) break;
+            const double step = -F / J;
+            const double gn = g + step;
+            double Fn, Jn;
+            if ((rs = eval(gn, &Fn, &Jn)) != RB200_OK) return rs;
+            if (!(Fn * Fn < F * F * (1 - 1e-4))) break;
+            g = gn;
+            F = Fn;
+            J = Jn;
+            if (std::fabs(F) <= ftol || step == 0) break;
+        }
+    }
+    if (!std::isfinite(g)) return fail(h, RB200_ERR_BAD_ARG, "relaxation parameter is not finite");
+    *gamma = g;
+    e = launch_relax(q, h->d_rq0, h->d_rk, g, n, s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "relaxation update");
+    return RB200_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -335,8 +443,13 @@ rb200_status rb200_create(const rb200_desc* d, rb200_handle** out) {
     for (int i = 0; i < 3; ++i) h->adv[i] = d->advection_velocity[i];
     if (h->prec != RB200_PRECISION_FP64 && h->prec != RB200_PRECISION_FP32_BULK)
         return bail(fail(h, RB200_ERR_BAD_ARG, "unknown precision"));
-    if (h->sflux != RB200_FLUX_RUSANOV && h->sflux != RB200_FLUX_CENTRAL)
-        return bail(fail(h, RB200_ERR_UNSUPPORTED, "surface flux must be Rusanov or Central"));
+    const bool entropy_flux = h->sflux == RB200_FLUX_KENNEDY_GRUBER || h->sflux == RB200_FLUX_ENTROPY_CONSERVATIVE ||
+                              h->sflux == RB200_FLUX_ROE || h->sflux == RB200_FLUX_MATRIX;
+    if (h->sflux != RB200_FLUX_RUSANOV && h->sflux != RB200_FLUX_CENTRAL && !entropy_flux)
+        return bail(fail(h, RB200_ERR_BAD_ARG, "unknown surface flux"));
+    if (entropy_flux && (h->law != RB200_LAW_EULER || h->prec != RB200_PRECISION_FP64))
+        return bail(fail(h, RB200_ERR_UNSUPPORTED,
+                         "the KG, EC, Roe and matrix surface fluxes are implemented for Euler in FP64"));
     if (h->law == RB200_LAW_ADVECTION) {
         h->ns = 1;
         if (h->form == RB200_FORM_WEAK) h->combo = ADV_WEAK;
@@ -483,7 +596,7 @@ rb200_status rb200_create(const rb200_desc* d, rb200_handle** out) {
     if ((st = dev_alloc(h, &h->d_status, 1)) != RB200_OK) return bail(st);
     ce = cudaMemset(h->d_status, 0, sizeof(int32_t));
     if (ce != cudaSuccess) return bail(cuda_fail(h, ce, "memset"));
-    if (dim == 3 && nq == 8 && affine && (h->combo == EUL_KG || h->combo == EUL_EC)) {
+    if (dim == 3 && nq == 8 && affine && (h->combo == EUL_KG || h->combo == EUL_EC) && !entropy_flux) {
         for (int a = 0; a < 8; ++a)
             for (int id = 0; id < 8; ++id)
                 h->pipe_S[a * 8 + id] = h->D[a + 8 * id] * (h->w[a] / h->w[id]) - h->D[id + 8 * a];
@@ -597,6 +710,46 @@ rb200_status rb200_integrals(rb200_handle* h, const double* q, double* out, void
     return RB200_OK;
 }
 
+rb200_status rb200_entropy_integral(rb200_handle* h, const double* q, double* out, void* stream) {
+    if (!h) return RB200_ERR_BAD_ARG;
+    if (!q || !out) return fail(h, RB200_ERR_BAD_ARG, "null pointer");
+    DeviceGuard guard(h->device);
+    double s2[2];
+    rb200_status st = entropy_sums_host(h, q, nullptr, 0.0, nullptr, s2, (cudaStream_t)stream);
+    if (st == RB200_OK) *out = s2[0];
+    return st;
+}
+
+rb200_status rb200_entropy_product(rb200_handle* h, const double* p, const double* q, double* out, void* stream) {
+    if (!h) return RB200_ERR_BAD_ARG;
+    if (!p || !q || !out) return fail(h, RB200_ERR_BAD_ARG, "null pointer");
+    DeviceGuard guard(h->device);
+    double s2[2];
+    rb200_status st = entropy_sums_host(h, p, nullptr, 0.0, q, s2, (cudaStream_t)stream);
+    if (st == RB200_OK) *out = s2[1];
+    return st;
+}
+
+rb200_status rb200_rlsrk54_step(rb200_handle* h, double* q, double* dq, double* gamma, double time, double dt,
+                                int32_t nsteps, void* stream) {
+    (void)time;
+    if (!h) return RB200_ERR_BAD_ARG;
+    if (!q || !dq || !gamma) return fail(h, RB200_ERR_BAD_ARG, "null pointer");
+    if (nsteps < 0 || !std::isfinite(dt) || !std::isfinite(*gamma)) return fail(h, RB200_ERR_BAD_ARG, "bad nsteps, dt or gamma");
+    if (h->prec != RB200_PRECISION_FP64)
+        return fail(h, RB200_ERR_UNSUPPORTED, "RLSRK54 keeps its LSRK register in FP64: create the handle in FP64");
+    if (h->E == 0 || nsteps == 0) return RB200_OK;
+    DeviceGuard guard(h->device);
+    const size_t n = (size_t)h->np * h->ns * h->E;
+    rb200_status st;
+    if (!h->d_rq0 && (st = dev_alloc(h, &h->d_rq0, n)) != RB200_OK) return st;
+    if (!h->d_rk && (st = dev_alloc(h, &h->d_rk, n)) != RB200_OK) return st;
+    if (!h->d_rsums && (st = dev_alloc(h, &h->d_rsums, 16)) != RB200_OK) return st;
+    for (int32_t i = 0; i < nsteps; ++i)
+        if ((st = rlsrk_step(h, q, dq, gamma, dt, (cudaStream_t)stream)) != RB200_OK) return st;
+    return RB200_OK;
+}
+
 rb200_status rb200_face_vmapP(rb200_handle* h, int64_t* vmapP_out, void* stream) {
     if (!h) return RB200_ERR_BAD_ARG;
     if (!vmapP_out) return fail(h, RB200_ERR_BAD_ARG, "null pointer");
@@ -647,6 +800,7 @@ rb200_status rb200_set_mortars(rb200_handle* h, const int64_t* mortars, int64_t 
     a.mortars = h->d_mortars;
     a.M = num_mortars;
     a.surface_rusanov = h->sflux == RB200_FLUX_RUSANOV ? 1 : 0;
+    a.surface_flux = h->sflux;
     a.gamma = h->gamma;
     for (int d = 0; d < 3; ++d) a.adv[d] = h->adv[d];
     const int q2 = h->nq * h->nq;

@@ -21,6 +21,7 @@
 #include <algorithm>
 
 #include "rb200_internal.h"
+#include "surface_fluxes.cuh"
 
 namespace rb200 {
 
@@ -48,6 +49,12 @@ __device__ __forceinline__ void face_flux(const MortarArgs& A, int dir, T sn, co
         const T an = (T)A.adv[dir] * sn;
         const T fc = (an * qm[0] + an * qp[0]) * T(0.5);
         nf[0] = A.surface_rusanov ? fc - (fabs(an) * (qp[0] - qm[0])) * T(0.5) : fc;
+    } else if (A.surface_flux == kFluxKG || A.surface_flux == kFluxEC || A.surface_flux == kFluxRoe ||
+               A.surface_flux == kFluxMatrix) {
+        T n[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) n[d] = d == dir ? sn : T(0);
+        euler_entropy_surface_flux<DIM, T>(A.surface_flux, n, qm, qp, (T)A.gamma, nf);
     } else {
         const T gm1 = (T)(A.gamma - 1.0);
         T Fn[2][NS], ws[2];

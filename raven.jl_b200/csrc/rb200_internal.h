@@ -32,6 +32,8 @@ enum Mode : int {
 
 constexpr int kMaxNq = 8;
 constexpr int32_t kStatusTimeout = 5;  // RB200_ERR_TIMEOUT
+// Numerical flux codes (RB200_FLUX_* of raven_b200.h)
+constexpr int kFluxCentral = 0, kFluxKG = 1, kFluxEC = 2, kFluxRusanov = 3, kFluxRoe = 4, kFluxMatrix = 5;
 
 struct StageArgs {
     const double* q_in;   // (Np, Ns, E)
@@ -45,7 +47,8 @@ struct StageArgs {
     const double* ncflux;    // mortar face fluxes ((2*dim, E) faces x (Ns, Nfp)), or null
     int64_t E;
     int32_t mode;
-    int32_t surface_rusanov;  // 1 Rusanov, 0 central
+    int32_t surface_rusanov;  // 1 Rusanov, 0 central (with surface_flux Rusanov or central)
+    int32_t surface_flux;     // kFlux*: the entropy family (EC, KG, Roe, matrix) runs its own kernels
     double rka;
     double rkb_dt;
     double gamma;
@@ -61,6 +64,7 @@ struct MortarArgs {
     const int64_t* mortars;   // (2 + 2^(dim-1), M): large element, its face, small elements
     int64_t M;
     int32_t surface_rusanov;
+    int32_t surface_flux;     // kFlux*: the Euler entropy family uses surface_fluxes.cuh
     double gamma;
     double adv[3];
     double IL[kMaxNq * kMaxNq], IU[kMaxNq * kMaxNq];  // to the halves, [i*nq + j]
@@ -105,5 +109,22 @@ cudaError_t launch_weighted_sums(const double* q, const double* elem_geo, const 
                                  int dim, int nq, int ns, int64_t E, int geom, double* partial, int nblocks,
                                  double* out_dev, cudaStream_t s);
 cudaError_t launch_face_vmapP(const int32_t* nbr, int dim, int nq, int64_t E, int64_t* out, cudaStream_t s);
+
+// Entropy measures and the RLSRK(5,4) step (relaxation.cu).  Sums land in out[0..1]
+// (device): (sum MJ eta, sum MJ v.k); the stage kernel writes only out[1].
+struct RelaxGeo {
+    const double* elem_geo;  // affine: (4, E)
+    const double* vgeo;      // curved: (Np, dim*dim+2, E), MJ at dim*dim+1
+    int dim, nq, np, geom, euler;
+    int64_t E;
+    double gamma;
+    double w[kMaxNq];
+};
+cudaError_t launch_entropy_sums(const RelaxGeo& G, const double* base, const double* dir, double c, const double* k,
+                                double* partial, int nblocks, double* out, cudaStream_t s);
+cudaError_t launch_rlsrk_stage(const RelaxGeo& G, double* q, double* dq, const double* k, double rka, double rkb_dt,
+                               double* partial, int nblocks, double* out, cudaStream_t s);
+cudaError_t launch_state_diff(const double* q, const double* q0, double* k, int64_t n, cudaStream_t s);
+cudaError_t launch_relax(double* q, const double* q0, const double* k, double gamma, int64_t n, cudaStream_t s);
 
 }  // namespace rb200

@@ -19,6 +19,12 @@ namespace rb200 {
 
 template <int COMBO, int GEOM>
 static cudaError_t launch_cg(int fp32, const StageArgs& a, cudaStream_t s) {
+    const bool entropy_family = a.surface_flux == kFluxEC || a.surface_flux == kFluxKG ||
+                                a.surface_flux == kFluxRoe || a.surface_flux == kFluxMatrix;
+    if (entropy_family) {  // Euler only, FP64 only (the host checks both)
+        if constexpr (COMBO == ADV_WEAK || COMBO == ADV_FDC) return cudaErrorInvalidValue;
+        else return fp32 ? cudaErrorInvalidValue : launch_one<RB_DIM, RB_NQ, COMBO, GEOM, double, 1>(a, s);
+    }
     return fp32 ? launch_one<RB_DIM, RB_NQ, COMBO, GEOM, float>(a, s)
                 : launch_one<RB_DIM, RB_NQ, COMBO, GEOM, double>(a, s);
 }

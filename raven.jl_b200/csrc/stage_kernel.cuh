@@ -19,6 +19,7 @@
 #include <stdint.h>
 
 #include "rb200_internal.h"
+#include "surface_fluxes.cuh"
 
 namespace rb200 {
 
@@ -109,8 +110,9 @@ __device__ __forceinline__ ElemPtrs elem_ptrs(const StageArgs& A) {
 
 // One element per group of Np threads: the whole fused stage for element e.  All
 // threads of the CTA must call it (it contains a barrier); inactive groups pass
-// active = false.
-template <int DIM, int NQ, int COMBO, int GEOM, typename T, int EPBX>
+// active = false.  SF = 1: the Euler surface flux is one of the entropy family
+// (entropy conservative, Kennedy-Gruber, Roe, matrix dissipation; A.surface_flux).
+template <int DIM, int NQ, int COMBO, int GEOM, typename T, int EPBX, int SF = 0>
 __device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs& P, const int64_t e,
                                               const bool active, unsigned char* smem_raw) {
     using S = Shape<DIM, NQ, EPBX>;
@@ -420,6 +422,8 @@ __device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs
             if (ne == -2) {  // mortar face of an adapted grid: the flux comes from the mortar kernel
 #pragma unroll
                 for (int s = 0; s < NS; ++s) nf[s] = (T)__ldg(P.ncflux + (((size_t)e * NF + f) * NS + s) * NFP + j);
+            } else if constexpr (SF == 1 && !C::ADV) {
+                euler_entropy_surface_flux<DIM, T>(A.surface_flux, nv, q, qp, (T)A.gamma, nf);
             } else if constexpr (C::ADV) {
                 T an;
                 if constexpr (AFF) an = (T)A.adv[dir] * nv[dir];
@@ -492,20 +496,20 @@ __device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs
     }
 }
 
-template <int DIM, int NQ, int COMBO, int GEOM, typename T>
+template <int DIM, int NQ, int COMBO, int GEOM, typename T, int SF>
 __global__ void __launch_bounds__(Shape<DIM, NQ>::THREADS, 1)
     stage_kernel(const __grid_constant__ StageArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using S = Shape<DIM, NQ>;
     const int64_t e = (int64_t)blockIdx.x * S::EPB + threadIdx.x / S::NP;
-    stage_element<DIM, NQ, COMBO, GEOM, T, 0>(A, elem_ptrs(A), e, e < A.E, smem_raw);
+    stage_element<DIM, NQ, COMBO, GEOM, T, 0, SF>(A, elem_ptrs(A), e, e < A.E, smem_raw);
 }
 
-template <int DIM, int NQ, int COMBO, int GEOM, typename T>
+template <int DIM, int NQ, int COMBO, int GEOM, typename T, int SF = 0>
 cudaError_t launch_one(const StageArgs& a, cudaStream_t st) {
     using S = Shape<DIM, NQ>;
     using K = KernelCfg<DIM, NQ, COMBO, GEOM, T>;
-    auto kern = stage_kernel<DIM, NQ, COMBO, GEOM, T>;
+    auto kern = stage_kernel<DIM, NQ, COMBO, GEOM, T, SF>;
     static bool configured = false;
     if (!configured) {
         cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::smem);

@@ -1,0 +1,138 @@
+"""The oracle's entropy-family surface fluxes, entropy measures and RLSRK(5,4) (no GPU).
+
+Pinned to the reference's own tests:
+  * test/balancelaws/euler/entropy_conservation_1d.jl: 1-D Euler, N = 4, K = 5, periodic,
+    FluxDifferencingForm(EntropyConservativeFlux()) with EntropyConservativeFlux() on the
+    faces, RLSRK54 at CFL 1/2 to t = 5: |eta_f - eta_0| / |eta_0| <= 40 eps;
+  * test/balancelaws/advection/entropy_conservation_1d.jl: 1-D advection, central volume
+    and surface fluxes, CFL 1/4: the same bound.
+The Roe and matrix fluxes have no reference test for the Euler law; they are checked by
+properties: free-stream preservation (1e-12 of the flux scale), conservation on periodic
+grids (1e-13 of sum |MJ dq|), semi-discrete entropy conservation of the EC pair (1e-13 of
+sum |MJ v.dq|) and entropy dissipation of the matrix flux (production <= 1e-13 of the scale).
+"""
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+EPS = np.finfo(float).eps
+
+
+def _square_1d(nq, K, law_kind, dim=1):
+    Ks = [K] + [1] * (dim - 1)
+    g = O.Grid(dim, nq, Ks, [-1.0] + [0.0] * (dim - 1), [1.0] + [1.0] * (dim - 1), [True] * dim)
+    x = g.points()
+    rho = np.where(np.abs(x[:, 0, :]) < 0.5, 2.0, 1.0)  # square(law, x) of the reference tests
+    if law_kind == "euler":
+        law = O.Law(O.LAW_EULER, dim, form=O.FORM_FLUXDIFF, volume_flux=O.FLUX_EC, surface_flux=O.FLUX_EC)
+        q = g.state(law)
+        q[:, 0, :] = rho
+        q[:, 1, :] = rho * 1.0
+        q[:, dim + 1, :] = 1.0 / (1.4 - 1) + (rho * rho) / (2 * rho)  # Euler.energy(law, rho, rho u, p = 1)
+        dt = 0.5 * (2.0 / K) / nq / np.sqrt(1.4 * 1.0 / 1.0)
+    else:
+        law = O.Law(O.LAW_ADVECTION, dim, form=O.FORM_FLUXDIFF, volume_flux=O.FLUX_CENTRAL,
+                    surface_flux=O.FLUX_CENTRAL)
+        q = g.state(law)
+        q[:, 0, :] = rho
+        dt = 0.25 * (2.0 / K) / nq / 1.0
+    return g, law, q, dt
+
+
+@pytest.mark.parametrize("law_kind", ["euler", "advection"])
+def test_rlsrk54_entropy_conservation_1d(law_kind):
+    g, law, q, dt = _square_1d(5, 5, law_kind)
+    eta0 = g.entropy_sums(law, q)[0]
+    steps, gamma = g.solve_rlsrk(law, q, dt, 5.0)
+    eta1 = g.entropy_sums(law, q)[0]
+    assert steps > 100 and abs(gamma - 1) < 1e-2
+    assert abs(eta1 - eta0) / abs(eta0) <= 40 * EPS
+
+
+def test_rlsrk54_relaxation_matters():
+    """Plain LSRK54 on the same problem drifts in entropy well above round-off."""
+    g, law, q, dt = _square_1d(5, 5, "euler")
+    eta0 = g.entropy_sums(law, q)[0]
+    g.solve(law, q, dt, 5.0)
+    assert abs(g.entropy_sums(law, q)[0] - eta0) / abs(eta0) > 1e3 * EPS
+
+
+def _entropy_numpy(law, q, dim, gamma=1.4):
+    if law.ns == 1:
+        return q[:, 0] ** 2 / 2, q.copy()
+    rho, m, rhoe = q[:, 0], q[:, 1:1 + dim], q[:, dim + 1]
+    p = (gamma - 1) * (rhoe - (m * m).sum(1) / (2 * rho))
+    s = np.log(p / rho ** gamma)
+    b = rho / (2 * p)
+    u = m / rho[:, None]
+    v = np.concatenate([((gamma - s) / (gamma - 1) - (u * u).sum(1) * b)[:, None], 2 * b[:, None] * u,
+                        (-2 * b)[:, None]], axis=1)
+    return -rho * s / (gamma - 1), v
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("law_kind", [O.LAW_EULER, O.LAW_ADVECTION])
+def test_entropy_sums_against_numpy(dim, law_kind):
+    g = O.Grid(dim, 4, [2] * dim, [0.0] * dim, [1.0] * dim, [True] * dim, O.WARP_SINE, 0.05)
+    law = O.Law(law_kind, dim)
+    q = g.initial_condition(law, 1 if law_kind == O.LAW_EULER else 0)
+    rng = np.random.default_rng(3)
+    k = np.asfortranarray(rng.standard_normal(q.shape))
+    d = np.asfortranarray(0.01 * rng.standard_normal(q.shape))
+    c = 0.7
+    got = g.entropy_sums(law, q, d, c, k)
+    p = q + c * d
+    MJ = g.volume_metrics()[:, dim * dim + 1, :]
+    eta, v = _entropy_numpy(law, np.moveaxis(p, 1, 2).reshape(-1, law.ns), dim)
+    kk = np.moveaxis(k, 1, 2).reshape(-1, law.ns)
+    mj = MJ.reshape(-1)
+    assert got[0] == pytest.approx((mj * eta).sum(), rel=1e-13)
+    assert got[1] == pytest.approx((mj * (v * kk).sum(1)).sum(), rel=1e-12)
+
+
+SURFACE = [O.FLUX_ROE, O.FLUX_MATRIX, O.FLUX_EC, O.FLUX_KG]
+
+
+def _euler_state(g, law, seed):
+    q = g.initial_condition(law, 1)
+    rng = np.random.default_rng(seed)
+    return np.asfortranarray(q * (1 + 0.05 * rng.standard_normal(q.shape)))
+
+
+@pytest.mark.parametrize("sflux", SURFACE, ids=["roe", "matrix", "ec", "kg"])
+@pytest.mark.parametrize("dim,warp", [(2, O.WARP_NONE), (2, O.WARP_SINE), (3, O.WARP_NONE)])
+def test_surface_flux_free_stream_and_conservation(dim, warp, sflux):
+    g = O.Grid(dim, 4, [3, 2, 2][:dim], [0.0] * dim, [1.0] * dim, [True] * dim, warp, 0.05)
+    law = O.Law(O.LAW_EULER, dim, form=O.FORM_FLUXDIFF, volume_flux=O.FLUX_KG, surface_flux=sflux)
+    q = g.state(law)
+    const = [1.3, 0.4, -0.2, 0.3][: dim + 1] + [2.9]
+    for s in range(law.ns):
+        q[:, s, :] = const[s]
+    assert np.abs(g.tendency(law, q)).max() <= 1e-12 * 10
+    q = _euler_state(g, law, 4)
+    dq = g.tendency(law, q)
+    MJ = g.volume_metrics()[:, dim * dim + 1, :]
+    for s in range(law.ns):
+        assert abs((MJ * dq[:, s, :]).sum()) <= 1e-13 * np.abs(MJ * dq[:, s, :]).sum()
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_entropy_production(dim):
+    """EC volume and surface fluxes conserve entropy semi-discretely; the matrix flux
+    dissipates it (and so does Roe's, on this smooth state)."""
+    g = O.Grid(dim, 5, [3, 2, 2][:dim], [0.0] * dim, [1.0] * dim, [True] * dim)
+    prods = {}
+    for sflux in (O.FLUX_EC, O.FLUX_MATRIX):
+        law = O.Law(O.LAW_EULER, dim, form=O.FORM_FLUXDIFF, volume_flux=O.FLUX_EC, surface_flux=sflux)
+        q = _euler_state(g, law, 5)
+        dq = g.tendency(law, q)
+        _, v = _entropy_numpy(law, np.moveaxis(q, 1, 2).reshape(-1, law.ns), dim)
+        MJ = g.volume_metrics()[:, dim * dim + 1, :].reshape(-1)
+        terms = MJ * (v * np.moveaxis(dq, 1, 2).reshape(-1, law.ns)).sum(1)
+        prods[sflux] = (terms.sum(), np.abs(terms).sum())
+    tot, scale = prods[O.FLUX_EC]
+    assert abs(tot) <= 1e-13 * scale
+    tot, scale = prods[O.FLUX_MATRIX]
+    assert tot <= 1e-13 * scale and tot < -1e-8 * scale
