@@ -134,6 +134,21 @@ rb200_status rb200_entropy_product(rb200_handle* h, const double* p, const doubl
 rb200_status rb200_rlsrk54_step(rb200_handle* h, double* q, double* dq, double* gamma, double time, double dt,
                                 int32_t nsteps, void* stream);
 
+/* Snapshot / resume of the time-stepper state.  The reference keeps (q, dq, time, dt)
+ * in its LSRK struct (odesolvers.jl:32-49; RLSRK adds gamma, :73-84) and has no
+ * checkpoint; these copy that state to a host buffer and back.  The buffer holds a
+ * 128-byte header (magic "RB200SNP", version, sizes, time, dt, gamma, a fingerprint of the
+ * discretization, checksums of the header and of the payload), then q (FP64) and dq (FP64,
+ * or FP32 for FP32_BULK handles, whose LSRK register is the handle's own and the dq
+ * argument is ignored).  rb200_restore checks the header, the fingerprint
+ * (RB200_ERR_SHAPE: another discretization) and the checksums (RB200_ERR_BAD_ARG:
+ * corrupted) before it copies anything.  Both are synchronous on `stream`. */
+rb200_status rb200_snapshot_bytes(const rb200_handle* h, size_t* bytes);
+rb200_status rb200_snapshot(rb200_handle* h, const double* q, const void* dq, double time, double dt, double gamma,
+                            void* host, size_t bytes, void* stream);
+rb200_status rb200_restore(rb200_handle* h, const void* host, size_t bytes, double* q, void* dq, double* time,
+                           double* dt, double* gamma, void* stream);
+
 /* Rebuilds vmapP (1-based, (2*dim*nq^(dim-1), E) int64) on the device from the
  * neighbour table the kernels use, for bit-exact comparison with facemaps(grid).vmapP. */
 rb200_status rb200_face_vmapP(rb200_handle* h, int64_t* vmapP_out, void* stream);

@@ -39,7 +39,7 @@ __all__ = [
     "LobattoCell", "brick", "BrickGrid", "GridManager", "generate", "Grid", "AdvectionLaw", "EulerLaw",
     "RusanovFlux", "CentralFlux", "KennedyGruberFlux", "EntropyConservativeFlux", "RoeFlux", "MatrixFlux", "WeakForm",
     "FluxDifferencingForm", "GridArray", "DGSEM", "LSRK54", "RLSRK54", "solve", "weightednorm", "integrals",
-    "entropyintegral", "entropyproduct",
+    "entropyintegral", "entropyproduct", "snapshot", "restore",
     "jl_range", "RB200Error", "brick_tree_order", "adapt", "AdaptRefine", "AdaptNone", "AdaptCoarsen",
     "ForestGrid",
 ]
@@ -452,6 +452,30 @@ def solve(q, timeend, solver, after_step=None, adjust_final=True):
             after_step(step, time, q)
         if final:
             return step
+
+
+# ------------------------------------------------------------------------- snapshot / resume
+
+
+def snapshot(dg, q, solver):
+    """The time-stepper state (q, dq, time, dt and, for RLSRK54, gamma) as bytes: a
+    checksummed header, then q and the LSRK register (see rb200_snapshot)."""
+    n = ctypes.c_size_t()
+    _lib.check(_lib.lib().rb200_snapshot_bytes(dg._h, ctypes.byref(n)), dg._h)
+    buf = ctypes.create_string_buffer(n.value)
+    _lib.check(_lib.lib().rb200_snapshot(dg._h, q.ptr(), solver.dq.ptr(), solver.time, solver.dt,
+                                         getattr(solver, "gamma", 1.0), buf, n.value, _stream_ptr()), dg._h)
+    return buf.raw
+
+
+def restore(dg, data, q, solver):
+    """Loads a snapshot taken with the same discretization into q and the solver."""
+    t, dt, g = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    _lib.check(_lib.lib().rb200_restore(dg._h, data, len(data), q.ptr(), solver.dq.ptr(), ctypes.byref(t),
+                                        ctypes.byref(dt), ctypes.byref(g), _stream_ptr()), dg._h)
+    solver.time, solver.dt = t.value, dt.value
+    if hasattr(solver, "gamma"):
+        solver.gamma = g.value
 
 
 # ------------------------------------------------------------------------------- measures

@@ -36,6 +36,9 @@ EXPORTED = [
     "rb200_entropy_integral",
     "rb200_entropy_product",
     "rb200_rlsrk54_step",
+    "rb200_snapshot_bytes",
+    "rb200_snapshot",
+    "rb200_restore",
     "rb200_face_vmapP",
     "rb200_get_info",
     "rb200_set_mortars",
@@ -151,6 +154,9 @@ def lib():
     L.rb200_entropy_integral.argtypes = [P, P, P, P]
     L.rb200_entropy_product.argtypes = [P, P, P, P, P]
     L.rb200_rlsrk54_step.argtypes = [P, P, P, P, D, D, I32, P]
+    L.rb200_snapshot_bytes.argtypes = [P, ctypes.POINTER(ctypes.c_size_t)]
+    L.rb200_snapshot.argtypes = [P, P, P, D, D, D, P, ctypes.c_size_t, P]
+    L.rb200_restore.argtypes = [P, P, ctypes.c_size_t, P, P, ctypes.POINTER(D), ctypes.POINTER(D), ctypes.POINTER(D), P]
     L.rb200_face_vmapP.argtypes = [P, P, P]
     L.rb200_get_info.argtypes = [P, P, I32]
     L.rb200_set_kernel_path.argtypes = [P, I32]

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -747,6 +748,136 @@ rb200_status rb200_rlsrk54_step(rb200_handle* h, double* q, double* dq, double* 
     if (!h->d_rsums && (st = dev_alloc(h, &h->d_rsums, 16)) != RB200_OK) return st;
     for (int32_t i = 0; i < nsteps; ++i)
         if ((st = rlsrk_step(h, q, dq, gamma, dt, (cudaStream_t)stream)) != RB200_OK) return st;
+    return RB200_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// Snapshot / resume of the time-stepper state (q, dq, time, dt, gamma)
+// ---------------------------------------------------------------------------------
+
+// 64-bit multiply-xor hash over little-endian 64-bit words (FNV-1a's prime and offset,
+// applied per word rather than per byte), then per byte for a ragged tail.
+static uint64_t snap_hash(const void* data, size_t bytes, uint64_t h = 0xcbf29ce484222325ull) {
+    const unsigned char* p = static_cast<const unsigned char*>(data);
+    const uint64_t prime = 0x100000001b3ull;
+    size_t i = 0;
+    for (; i + 8 <= bytes; i += 8) {
+        uint64_t w;
+        std::memcpy(&w, p + i, 8);
+        h = (h ^ w) * prime;
+    }
+    for (; i < bytes; ++i) h = (h ^ p[i]) * prime;
+    return h;
+}
+
+struct SnapHeader {
+    char magic[8];  // "RB200SNP"
+    uint32_t version;
+    uint32_t header_bytes;
+    int32_t dim, nq, ns, law, precision, combo;
+    int64_t E;
+    uint64_t q_bytes, dq_bytes;
+    double time, dt, gamma;
+    uint64_t fingerprint;  // the discretization: sizes, law, scheme, D, w, gamma, velocity
+    uint64_t payload_sum;  // hash of the q bytes, then the dq bytes
+    uint64_t reserved[2];
+    uint64_t header_sum;   // hash of every byte before this field
+};
+static_assert(sizeof(SnapHeader) == 128, "snapshot header layout");
+
+static uint64_t snap_fingerprint(const rb200_handle* h) {
+    const int32_t ints[9] = {h->dim, h->nq, h->ns, h->law, h->form, h->vflux, h->sflux, h->prec, h->combo};
+    uint64_t f = snap_hash(ints, sizeof(ints));
+    f = snap_hash(&h->E, sizeof(h->E), f);
+    f = snap_hash(h->D, sizeof(double) * h->nq * h->nq, f);
+    f = snap_hash(h->w, sizeof(double) * h->nq, f);
+    f = snap_hash(&h->gamma, sizeof(double), f);
+    return snap_hash(h->adv, sizeof(h->adv), f);
+}
+
+static size_t snap_dq_bytes(const rb200_handle* h) {
+    return (size_t)h->np * h->ns * h->E * (h->prec == RB200_PRECISION_FP32_BULK ? sizeof(float) : sizeof(double));
+}
+
+rb200_status rb200_snapshot_bytes(const rb200_handle* h, size_t* bytes) {
+    if (!h || !bytes) return RB200_ERR_BAD_ARG;
+    *bytes = sizeof(SnapHeader) + (size_t)h->np * h->ns * h->E * sizeof(double) + snap_dq_bytes(h);
+    return RB200_OK;
+}
+
+rb200_status rb200_snapshot(rb200_handle* h, const double* q, const void* dq, double time, double dt, double gamma,
+                            void* host, size_t bytes, void* stream) {
+    if (!h) return RB200_ERR_BAD_ARG;
+    size_t need = 0;
+    rb200_snapshot_bytes(h, &need);
+    const bool fp32 = h->prec == RB200_PRECISION_FP32_BULK;
+    if (!q || !host || (!dq && !fp32)) return fail(h, RB200_ERR_BAD_ARG, "null pointer");
+    if (bytes < need) return fail(h, RB200_ERR_SHAPE, "snapshot buffer is smaller than rb200_snapshot_bytes");
+    DeviceGuard guard(h->device);
+    const size_t qb = (size_t)h->np * h->ns * h->E * sizeof(double), db = snap_dq_bytes(h);
+    unsigned char* out = static_cast<unsigned char*>(host);
+    cudaStream_t s = (cudaStream_t)stream;
+    // the FP32-bulk LSRK register is the handle's own (rb200_lsrk54_step ignores dq there)
+    const void* dq_src = fp32 ? (const void*)h->d_dq32 : dq;
+    cudaError_t e = cudaSuccess;
+    if (qb) e = cudaMemcpyAsync(out + sizeof(SnapHeader), q, qb, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && db) e = cudaMemcpyAsync(out + sizeof(SnapHeader) + qb, dq_src, db, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "snapshot copy");
+    SnapHeader hd;
+    std::memset(&hd, 0, sizeof(hd));
+    std::memcpy(hd.magic, "RB200SNP", 8);
+    hd.version = 1;
+    hd.header_bytes = sizeof(SnapHeader);
+    hd.dim = h->dim;
+    hd.nq = h->nq;
+    hd.ns = h->ns;
+    hd.law = h->law;
+    hd.precision = h->prec;
+    hd.combo = h->combo;
+    hd.E = h->E;
+    hd.q_bytes = qb;
+    hd.dq_bytes = db;
+    hd.time = time;
+    hd.dt = dt;
+    hd.gamma = gamma;
+    hd.fingerprint = snap_fingerprint(h);
+    hd.payload_sum = snap_hash(out + sizeof(SnapHeader), qb + db);
+    hd.header_sum = snap_hash(&hd, offsetof(SnapHeader, header_sum));
+    std::memcpy(out, &hd, sizeof(hd));
+    return RB200_OK;
+}
+
+rb200_status rb200_restore(rb200_handle* h, const void* host, size_t bytes, double* q, void* dq, double* time,
+                           double* dt, double* gamma, void* stream) {
+    if (!h) return RB200_ERR_BAD_ARG;
+    const bool fp32 = h->prec == RB200_PRECISION_FP32_BULK;
+    if (!host || !q || (!dq && !fp32)) return fail(h, RB200_ERR_BAD_ARG, "null pointer");
+    if (bytes < sizeof(SnapHeader)) return fail(h, RB200_ERR_SHAPE, "snapshot is shorter than its header");
+    SnapHeader hd;
+    std::memcpy(&hd, host, sizeof(hd));
+    if (std::memcmp(hd.magic, "RB200SNP", 8) != 0 || hd.version != 1 || hd.header_bytes != sizeof(SnapHeader))
+        return fail(h, RB200_ERR_BAD_ARG, "not a snapshot of this format");
+    if (hd.header_sum != snap_hash(&hd, offsetof(SnapHeader, header_sum)))
+        return fail(h, RB200_ERR_BAD_ARG, "snapshot header checksum mismatch");
+    const size_t qb = (size_t)h->np * h->ns * h->E * sizeof(double), db = snap_dq_bytes(h);
+    if (hd.fingerprint != snap_fingerprint(h) || hd.q_bytes != qb || hd.dq_bytes != db)
+        return fail(h, RB200_ERR_SHAPE, "snapshot was taken with another discretization or precision");
+    if (bytes < sizeof(SnapHeader) + qb + db) return fail(h, RB200_ERR_SHAPE, "snapshot is truncated");
+    const unsigned char* in = static_cast<const unsigned char*>(host);
+    if (hd.payload_sum != snap_hash(in + sizeof(SnapHeader), qb + db))
+        return fail(h, RB200_ERR_BAD_ARG, "snapshot payload checksum mismatch");
+    DeviceGuard guard(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    void* dq_dst = fp32 ? (void*)h->d_dq32 : dq;
+    cudaError_t e = cudaSuccess;
+    if (qb) e = cudaMemcpyAsync(q, in + sizeof(SnapHeader), qb, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && db) e = cudaMemcpyAsync(dq_dst, in + sizeof(SnapHeader) + qb, db, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "restore copy");
+    if (time) *time = hd.time;
+    if (dt) *dt = hd.dt;
+    if (gamma) *gamma = hd.gamma;
     return RB200_OK;
 }
 

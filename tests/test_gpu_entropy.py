@@ -171,3 +171,37 @@ def test_unsupported_combinations(rb, cuda_ok):
     with pytest.raises(rb.RB200Error) as ei:
         rb.RLSRK54(dg, qg, 1e-3).dostep(qg, 1)
     assert ei.value.status == 6
+
+
+@pytest.mark.parametrize("precision,stepper", [("fp64", "lsrk"), ("fp32_bulk", "lsrk"), ("fp64", "rlsrk")])
+def test_snapshot_resume(rb, cuda_ok, precision, stepper):
+    """Resuming from a snapshot reproduces the uninterrupted run bit for bit."""
+    import struct
+
+    case = (3, 5, (2, 2, 2), (1, 1, 1), "eul_kg", O.WARP_NONE)
+    og, dg, olaw, law = _build(rb, *case, "ec" if stepper == "rlsrk" else "rusanov", precision=precision)
+    q0 = initial_state(og, olaw, "eul_kg", seed=16, amp=0.01)
+    qg = rb.GridArray.from_numpy(q0)
+    mk = rb.RLSRK54 if stepper == "rlsrk" else rb.LSRK54
+    solver = mk(dg, qg, 1e-2)
+    solver.dostep(qg, 3)
+    snap = rb.snapshot(dg, qg, solver)
+    magic, version, hbytes = struct.unpack_from("<8sII", snap, 0)
+    assert magic == b"RB200SNP" and version == 1 and hbytes == 128
+    solver.dostep(qg, 3)
+    want, want_t = qg.numpy(), solver.time
+    q2 = rb.GridArray.from_numpy(np.zeros_like(q0))
+    s2 = mk(dg, q2, 5.0)
+    rb.restore(dg, snap, q2, s2)
+    assert s2.dt == 1e-2 and s2.time == pytest.approx(3e-2, abs=0)
+    s2.dostep(q2, 3)
+    assert np.array_equal(q2.numpy(), want) and s2.time == want_t
+    bad = bytearray(snap)
+    bad[-3] ^= 0x10
+    with pytest.raises(rb.RB200Error) as ei:
+        rb.restore(dg, bytes(bad), q2, s2)
+    assert ei.value.status == 1
+    other = _build(rb, 3, 5, (2, 2, 3), (1, 1, 1), "eul_kg", O.WARP_NONE, "rusanov", precision=precision)[1]
+    with pytest.raises(rb.RB200Error) as ei:
+        rb.restore(other, snap, q2, s2)
+    assert ei.value.status == 2
