@@ -182,8 +182,9 @@ rb200_status rb200_sync_status(rb200_handle* h, void* stream);
 
 /* Handle properties: info[0]=dim, [1]=nq, [2]=Ns, [3]=E, [4]=geometry kind
  * (0 affine brick, 1 curved), [5]=precision, [6]=kernel launches per LSRK step,
- * [7]=algorithmic HBM bytes per node per stage, [8]=CTAs of the pipelined kernel
- * (0 when the handle's configuration does not use it). */
+ * [7]=algorithmic HBM bytes per node per stage, [8]=CTAs of the pipelined kernel of the
+ * handle's geometry (brick, or the FP32-bulk curved one; 0 when the configuration does
+ * not use one). */
 rb200_status rb200_get_info(const rb200_handle* h, int64_t* info, int32_t n);
 
 /* Weighted sums without any device allocation (no counterpart in the reference).

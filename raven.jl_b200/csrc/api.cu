@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/raven_b200.h"
+#include "pipelined_curved.cuh"
 #include "pipelined_kernel.cuh"
 #include "rb200_internal.h"
 
@@ -56,6 +57,7 @@ struct rb200_handle {
     double graph_dt = 0.0;
     int use_graphs = 1;
     int pipe_grid = 0;            // CTAs of the pipelined kernel (0: not eligible)
+    int pipe_curved_grid = 0;     // CTAs of the curved-grid pipelined kernel (0: not eligible)
     double pipe_S[64] = {0};      // D[a,id] w[a] / w[id] - D[id,a]
     // mortars of an adapted grid (rb200_set_mortars)
     int64_t nmortars = 0;
@@ -164,6 +166,26 @@ cudaError_t launch_any(rb200_handle* h, const StageArgs& a, cudaStream_t st) {
         return launch_stage(h->dim, h->nq, h->combo, h->geom, h->prec, a, st);
     }
     const bool stage_mode = a.mode >= MODE_STAGE;
+    if (h->pipe_curved_grid > 0 && h->kernel_path == 0 && stage_mode && aligned16(a.q_in) && aligned16(a.q_out) &&
+        aligned16(a.dq)) {
+        PipeCurvedArgs c;
+        std::memset(&c, 0, sizeof(c));
+        c.q_in = a.q_in;
+        c.q_out = a.q_out;
+        c.dq = static_cast<float*>(a.dq);
+        c.vgeo = h->d_vgeo;
+        c.sgeo = h->d_sgeo;
+        c.nbr = h->d_nbr;
+        c.status = h->d_status;
+        c.E = a.E;
+        c.mode = a.mode;
+        c.surface_rusanov = a.surface_rusanov;
+        c.rka = a.rka;
+        c.rkb_dt = a.rkb_dt;
+        c.gamma = a.gamma;
+        std::memcpy(c.D, h->D, sizeof(c.D));
+        return launch_pipelined_curved(c, (int)std::min<int64_t>(h->pipe_curved_grid, a.E), st);
+    }
     const bool eligible = h->kernel_path == 0 && h->pipe_grid > 0 && aligned16(a.q_in) && aligned16(a.dq) &&
                           (!stage_mode || aligned16(a.q_out)) &&
                           (h->prec == RB200_PRECISION_FP64 || stage_mode);
@@ -608,6 +630,15 @@ rb200_status rb200_create(const rb200_desc* d, rb200_handle** out) {
         h->pipe_grid = per_sm > 0 ? per_sm * nsm : 0;
         cudaGetLastError();
     }
+    if (dim == 3 && nq == 8 && !affine && h->combo == EUL_KG && h->prec == RB200_PRECISION_FP32_BULK && !entropy_flux &&
+        h->d_vgeo && h->d_sgeo && aligned16(h->d_vgeo) && aligned16(h->d_sgeo)) {
+        int dev = 0, nsm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        const int per_sm = pipelined_curved_blocks_per_sm();
+        h->pipe_curved_grid = per_sm > 0 ? per_sm * nsm : 0;
+        cudaGetLastError();
+    }
     h->red_blocks = 296;
     if ((st = dev_alloc(h, &h->d_partial, (size_t)h->red_blocks * 2 * h->ns)) != RB200_OK) return bail(st);
     if ((st = dev_alloc(h, &h->d_sums, (size_t)2 * h->ns)) != RB200_OK) return bail(st);
@@ -940,7 +971,8 @@ rb200_status rb200_set_mortars(rb200_handle* h, const int64_t* mortars, int64_t 
     std::memcpy(a.PL, PL, q2 * sizeof(double));
     std::memcpy(a.PU, PU, q2 * sizeof(double));
     h->nmortars = num_mortars;
-    h->pipe_grid = 0;  // the pipelined kernel has no mortar faces
+    h->pipe_grid = 0;  // the pipelined kernels have no mortar faces
+    h->pipe_curved_grid = 0;
     free_graph(h);
     return RB200_OK;
 }
@@ -968,7 +1000,8 @@ rb200_status rb200_get_info(const rb200_handle* h, int64_t* info, int32_t n) {
     int64_t per_node = h->ns * (2 * bytes_q + 2 * bytes_dq);
     if (h->geom == GEOM_CURVED)
         per_node += (h->dim * h->dim + 1) * 8 + (int64_t)h->nf * h->nfp * (h->dim + 1) * 8 / h->np;
-    const int64_t v[9] = {h->dim, h->nq, h->ns, h->E, h->geom, h->prec, 5, per_node, h->pipe_grid};
+    const int64_t v[9] = {h->dim, h->nq, h->ns, h->E, h->geom, h->prec, 5, per_node,
+                          h->geom == GEOM_CURVED ? h->pipe_curved_grid : h->pipe_grid};
     for (int i = 0; i < n && i < 9; ++i) info[i] = v[i];
     return RB200_OK;
 }

@@ -1,5 +1,6 @@
 // Instantiations and launch helpers of the pipelined 3-D Nq = 8 stage kernel: one state
 // (the DGSEM handle) or the chunks of a serving class (BATCH).
+#include "pipelined_curved.cuh"
 #include "pipelined_kernel.cuh"
 
 namespace rb200 {
@@ -60,6 +61,31 @@ int pipelined_blocks_per_sm(int combo, int fp32) {
 int pipelined_batch_blocks_per_sm(int combo, int fp32) {
     if (combo == EUL_KG) return fp32 ? occupancy_p<EUL_KG, float, true>() : occupancy_p<EUL_KG, double, true>();
     return 0;
+}
+
+// The curved-grid kernel (FP32 bulk, Kennedy-Gruber): two CTAs per SM.
+cudaError_t launch_pipelined_curved(const PipeCurvedArgs& a, int grid, cudaStream_t s) {
+    auto kern = pipelined_curved_kernel<EUL_KG>;
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t err =
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(pipec::Smem));
+        if (err != cudaSuccess) return err;
+        configured = true;
+    }
+    kern<<<grid, pipec::NT, sizeof(pipec::Smem), s>>>(a);
+    return cudaGetLastError();
+}
+
+int pipelined_curved_blocks_per_sm() {
+    auto kern = pipelined_curved_kernel<EUL_KG>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(pipec::Smem)) !=
+        cudaSuccess)
+        return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, pipec::NT, sizeof(pipec::Smem)) != cudaSuccess)
+        return 0;
+    return n;
 }
 
 }  // namespace rb200

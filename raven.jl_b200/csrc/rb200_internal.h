@@ -103,6 +103,10 @@ struct PipeBatch;  // pipelined_kernel.cuh
 cudaError_t launch_pipelined_batch(int combo, int fp32, const PipeArgs& a, const PipeBatch& b, int grid,
                                    cudaStream_t s);
 int pipelined_batch_blocks_per_sm(int combo, int fp32);
+struct PipeCurvedArgs;  // pipelined_curved.cuh
+// Persistent pipelined kernel for 3-D Nq = 8 curved grids (FP32 bulk, Kennedy-Gruber, stage modes).
+cudaError_t launch_pipelined_curved(const PipeCurvedArgs& a, int grid, cudaStream_t s);
+int pipelined_curved_blocks_per_sm();
 
 // Reductions and face-map expansion (reduce.cu).
 cudaError_t launch_weighted_sums(const double* q, const double* elem_geo, const double* vgeo, const double* w,

@@ -96,3 +96,35 @@ def test_misaligned_state_falls_back_to_generic_kernel(rb, cuda_ok):
     dqg = rb.GridArray.zeros(law, og)
     dg(dqg, qv, 0.0, increment=False)
     assert rel_err(dqg.numpy(), ref) <= 1e-12
+
+
+@pytest.mark.parametrize("warp,per", [(O.WARP_SINE, (1, 1, 1)), (O.WARP_SINE, (1, 0, 1)),
+                                      (O.WARP_IDENTITY_CURVED, (1, 1, 0))], ids=["sine", "sine-open-y", "identity"])
+def test_curved_pipelined_fp32_bulk_steps(rb, cuda_ok, warp, per):
+    """The curved-grid pipelined kernel (FP32 bulk, Kennedy-Gruber) against the oracle
+    after two steps (1e-6 relative, as for the brick kernel) and against the generic
+    kernel after five steps, the last three replayed from a CUDA graph (1e-6)."""
+    og = O.Grid(3, 8, (8, 8, 7), [0.0] * 3, [10.0] * 3, per, warp, 0.1 if warp == O.WARP_SINE else 0.0)
+    g = wrap_oracle_grid(og)
+    law, form = product_scheme(rb, "eul_kg", 3)
+    dg = rb.DGSEM(law=law, grid=g, volume_form=form, surface_numericalflux=rb.RusanovFlux(), precision="fp32_bulk")
+    olaw = oracle_law("eul_kg", 3)
+    assert dg.geometry == "curved" and dg.pipelined_ctas > 0 and og.E > dg.pipelined_ctas
+    q = initial_state(og, olaw, "eul_kg", seed=16, amp=0.01)
+    qo, dqo = q.copy(order="F"), og.state(olaw)
+    for i in range(2):
+        og.lsrk54_step(olaw, qo, dqo, i * 1e-3, 1e-3)
+    qg = rb.GridArray.from_numpy(q)
+    rb.LSRK54(dg, qg, 1e-3).dostep(qg, 2)
+    dg.sync_status()
+    for s in range(law.ns):
+        assert rel_err(qg.numpy()[:, s], qo[:, s]) <= 1e-6, s
+    qa = rb.GridArray.from_numpy(q)
+    rb.LSRK54(dg, qa, 1e-3).dostep(qa, 5)
+    dg.sync_status()
+    dg.set_kernel_path("generic")
+    qb = rb.GridArray.from_numpy(q)
+    rb.LSRK54(dg, qb, 1e-3).dostep(qb, 5)
+    dg.set_kernel_path("auto")
+    for s in range(law.ns):
+        assert rel_err(qa.numpy()[:, s], qb.numpy()[:, s]) <= 1e-6, s
