@@ -221,18 +221,27 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(name):
-    """dram bytes per launch of the stage kernel from the committed ncu summary, if any."""
+def profiled_figure(name, key):
+    """A figure of the stage kernel from the committed ncu summary of this workload
+    (`dram_bytes_per_launch`, `fp64_flops_per_node`), if any."""
     path = os.path.join(ROOT, "profiles", f"stage_kernel_{name}.md")
     if not os.path.exists(path):
         return None
     for line in open(path):
-        if line.startswith("dram_bytes_per_launch:"):
+        if line.startswith(key + ":"):
             try:
                 return float(line.split(":", 1)[1].strip().split()[0])
             except ValueError:
                 return None
     return None
+
+
+def profiled_traffic(name):
+    """dram bytes per launch of the stage kernel from the committed ncu summary, if any."""
+    return profiled_figure(name, "dram_bytes_per_launch")
+
+
+FP64_NOMINAL_TFLOPS = 37.0  # B200 datasheet FP64 (no measured FP64 peak is available)
 
 
 def stage_bytes_per_launch(w, nodes, ns):
@@ -719,6 +728,7 @@ def main(argv=None):
     # accuracy of the run: L2 distance to the exactly advected vortex, and conservation
     l2_err = None
     fp64_cmp = None
+    accuracy = None
     if w.get("adapted"):
         # the FP32-bulk state against an FP64 run of the same steps (the FP64 path is
         # parity-tested against the oracle), and the drift of the conserved integrals
@@ -751,8 +761,17 @@ def main(argv=None):
         T = (args.warmup + args.steps) * dt
         qe = rb.GridArray.from_numpy(ic.isentropic_vortex(grid, law, beta=5.0, u0=0.5 * math.sqrt(law.gamma),
                                                           center=(w["L"] / 2, w["L"] / 2), t=T))
+        qmax = float(qe.data.abs().max().item())
         qe.data.sub_(q.data)
         l2_err = rb.weightednorm(dg, qe)
+        I0, I1 = rb.integrals(dg, rb.GridArray.from_numpy(q0)), rb.integrals(dg, q)
+        accuracy = {
+            "l2_error_vs_exact": l2_err,
+            "max_error_vs_exact_relative": float(qe.data.abs().max().item()) / qmax,
+            # |integral(t) - integral(0)| over max(|integral(0)|, mass): the vortex's z momentum is 0
+            "conservation_drift": [abs(a - b) / max(abs(b), abs(I0[0])) for a, b in zip(I1, I0)],
+            "steps": args.warmup + args.steps,
+        }
         del qe
 
     # end to end through the C ABI with host buffers: every step copies the state in from
@@ -795,6 +814,14 @@ def main(argv=None):
         "kernel": kernel_name(w, dg),
         "algorithmic_bytes_per_launch": bytes_launch,
     }
+    fp64_pipe = None
+    flops_node = profiled_figure(args.workload, "fp64_flops_per_node")
+    if flops_node and w["precision"] == "fp64":
+        # the second roofline of the FP64 path: FP64 flops the kernel executes (ncu counters
+        # of the committed summary, DFMA = 2) per launch over the launch time
+        tf = flops_node * nodes / (ms / 1e3 / launches) / 1e12
+        fp64_pipe = {"achieved": tf, "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s", "frac": tf / FP64_NOMINAL_TFLOPS,
+                     "peak_source": "nominal (datasheet)", "flops_per_node_stage": flops_node}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample(w)
@@ -814,11 +841,13 @@ def main(argv=None):
             "data": "synthetic",
             "config": config_json(args.workload, w, grid),
             "roofline": roofline,
+            "fp64_roofline": fp64_pipe,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": sampler.summary(),
             "l2_error_vs_exact": l2_err,
+            "accuracy": accuracy,
             "vs_fp64": fp64_cmp,
             "dt": dt,
         }
