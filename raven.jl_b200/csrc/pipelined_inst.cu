@@ -13,13 +13,9 @@ constexpr int kNPT = RB200_PIPE_NPT;
 template <int COMBO, typename T, bool BATCH>
 static cudaError_t launch_p(const PipeArgs& a, const PipeBatch& b, int grid, cudaStream_t s) {
     auto kern = pipelined_stage_kernel<COMBO, T, kNPT, BATCH>;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)sizeof(pipe::Smem<T>));
-        if (err != cudaSuccess) return err;
-        configured = true;
-    }
+    static std::atomic<uint64_t> configured{0};
+    cudaError_t err = ensure_smem_limit(kern, (int)sizeof(pipe::Smem<T>), configured);
+    if (err != cudaSuccess) return err;
     kern<<<grid, 512 / kNPT, sizeof(pipe::Smem<T>), s>>>(a, b);
     return cudaGetLastError();
 }
@@ -66,13 +62,9 @@ int pipelined_batch_blocks_per_sm(int combo, int fp32) {
 // The curved-grid kernel (FP32 bulk, Kennedy-Gruber): two CTAs per SM.
 cudaError_t launch_pipelined_curved(const PipeCurvedArgs& a, int grid, cudaStream_t s) {
     auto kern = pipelined_curved_kernel<EUL_KG>;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t err =
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(pipec::Smem));
-        if (err != cudaSuccess) return err;
-        configured = true;
-    }
+    static std::atomic<uint64_t> configured{0};
+    cudaError_t err = ensure_smem_limit(kern, (int)sizeof(pipec::Smem), configured);
+    if (err != cudaSuccess) return err;
     kern<<<grid, pipec::NT, sizeof(pipec::Smem), s>>>(a);
     return cudaGetLastError();
 }

@@ -5,9 +5,25 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 
 namespace rb200 {
+
+// Raises a kernel's dynamic shared-memory limit once per device: the attribute belongs
+// to the kernel's instance in the current device's context.  `done` holds one bit per
+// device ordinal (devices beyond 63 set the attribute on every call).
+template <typename Kernel>
+cudaError_t ensure_smem_limit(Kernel kern, int bytes, std::atomic<uint64_t>& done) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const uint64_t bit = (dev >= 0 && dev < 64) ? (uint64_t{1} << dev) : 0;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_acq_rel);
+    return e;
+}
 
 // Physics + volume-form combination (template parameter of the stage kernel).
 enum Combo : int {

@@ -20,12 +20,9 @@ cudaError_t launch_t(const BatchArgs& b, int grid, cudaStream_t s, int* blocks_p
     auto kern = batched_stage_kernel<RB_SERVE_DIM, NQ, COMBO, GEOM_AFFINE, T, EPB>;
     using K = KernelCfg<RB_SERVE_DIM, NQ, COMBO, GEOM_AFFINE, T, EPB>;
     using S = Shape<RB_SERVE_DIM, NQ, EPB>;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::smem);
-        if (err != cudaSuccess) return err;
-        configured = true;
-    }
+    static std::atomic<uint64_t> configured{0};
+    cudaError_t err = ensure_smem_limit(kern, (int)K::smem, configured);
+    if (err != cudaSuccess) return err;
     if (blocks_per_sm) {  // occupancy query only
         return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kern, S::THREADS, K::smem);
     }

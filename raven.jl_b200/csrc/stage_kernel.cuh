@@ -510,12 +510,9 @@ cudaError_t launch_one(const StageArgs& a, cudaStream_t st) {
     using S = Shape<DIM, NQ>;
     using K = KernelCfg<DIM, NQ, COMBO, GEOM, T>;
     auto kern = stage_kernel<DIM, NQ, COMBO, GEOM, T, SF>;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::smem);
-        if (err != cudaSuccess) return err;
-        configured = true;
-    }
+    static std::atomic<uint64_t> configured{0};
+    cudaError_t err = ensure_smem_limit(kern, (int)K::smem, configured);
+    if (err != cudaSuccess) return err;
     const int64_t blocks = (a.E + S::EPB - 1) / S::EPB;
     if (blocks <= 0) return cudaSuccess;
     kern<<<(unsigned)blocks, S::THREADS, K::smem, st>>>(a);
