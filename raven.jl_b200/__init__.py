@@ -208,9 +208,17 @@ class WeakForm:
 class FluxDifferencingForm:
     code = _lib.FORM_FLUXDIFF
 
+    # The reference's three loop organisations of the same flux-differencing sum
+    # (dgsem.jl:163-255: :naive, :per_dir, :per_dir_symmetric).  They differ only in the
+    # order of the floating-point sums; one device kernel family serves all three.
+    KERNEL_TYPES = ("naive", "per_dir", "per_dir_symmetric")
+
     def __init__(self, volume_numericalflux, kernel_type="per_dir"):
+        kt = str(kernel_type).lstrip(":")
+        if kt not in self.KERNEL_TYPES:
+            raise ValueError(f"Unknown kernel type {kernel_type}")  # dgsem.jl:253
         self.volume_numericalflux = volume_numericalflux
-        self.kernel_type = kernel_type
+        self.kernel_type = kt
 
 
 # ------------------------------------------------------------------------------ GridArray

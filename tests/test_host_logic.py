@@ -111,3 +111,12 @@ def test_warped_grid_matches_oracle(rb, dim, nq, K):
     assert np.abs(g.volume_metrics - vm).max() <= 1e-13 * np.abs(vm).max()
     assert np.abs(g.surface_metrics - og.surface_metrics()).max() <= 1e-11
     assert np.array_equal(g.vmapP, og.vmapP())
+
+
+def test_flux_differencing_kernel_types(rb):
+    """FluxDifferencingForm takes the reference's three kernel types (dgsem.jl:163-255),
+    with or without the Julia symbol colon, and rejects others as the reference does."""
+    for kt in ("naive", "per_dir", ":per_dir_symmetric"):
+        assert rb.FluxDifferencingForm(rb.KennedyGruberFlux(), kt).kernel_type == kt.lstrip(":")
+    with pytest.raises(ValueError, match="Unknown kernel type"):
+        rb.FluxDifferencingForm(rb.KennedyGruberFlux(), "per_node")
