@@ -18,15 +18,15 @@ namespace {
 template <int NQ, int COMBO, typename T, int EPB>
 cudaError_t launch_t(const BatchArgs& b, int grid, cudaStream_t s, int* blocks_per_sm) {
     auto kern = batched_stage_kernel<RB_SERVE_DIM, NQ, COMBO, GEOM_AFFINE, T, EPB>;
-    using K = KernelCfg<RB_SERVE_DIM, NQ, COMBO, GEOM_AFFINE, T, EPB>;
     using S = Shape<RB_SERVE_DIM, NQ, EPB>;
+    using PC = PersistentCfg<RB_SERVE_DIM, NQ, COMBO, GEOM_AFFINE, T, EPB>;
     static std::atomic<uint64_t> configured{0};
-    cudaError_t err = ensure_smem_limit(kern, (int)K::smem, configured);
+    cudaError_t err = ensure_smem_limit(kern, (int)PC::smem, configured);
     if (err != cudaSuccess) return err;
     if (blocks_per_sm) {  // occupancy query only
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kern, S::THREADS, K::smem);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kern, S::THREADS, PC::smem);
     }
-    kern<<<grid, S::THREADS, K::smem, s>>>(b);
+    kern<<<grid, S::THREADS, PC::smem, s>>>(b);
     return cudaGetLastError();
 }
 

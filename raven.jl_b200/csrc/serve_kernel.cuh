@@ -22,20 +22,32 @@ struct BatchArgs {
     double rkb;                   // LSRK b coefficient of this stage (times each solve's dt)
 };
 
+// The CTA walks chunk slots blockIdx.x + k*gridDim.x and, within a chunk, groups of EPB
+// elements.  Where the generic kernel prefetches (3-D, FP32 bulk), every thread copies
+// its node's state and register in the CTA's next group (possibly the next chunk's) into
+// its own shared-memory slots with cp.async while the current group runs.
 template <int DIM, int NQ, int COMBO, int GEOM, typename T, int EPBX>
-__global__ void __launch_bounds__(Shape<DIM, NQ, EPBX>::THREADS, 1)
+__global__ void __launch_bounds__(Shape<DIM, NQ, EPBX>::THREADS,
+                                  (PersistentCfg<DIM, NQ, COMBO, GEOM, T, EPBX>::MIN_CTAS))
     batched_stage_kernel(const __grid_constant__ BatchArgs B) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using S = Shape<DIM, NQ, EPBX>;
+    using PC = PersistentCfg<DIM, NQ, COMBO, GEOM, T, EPBX>;
+    constexpr int NS = PC::NS, TH = S::THREADS, NP = S::NP;
+    double* qs = reinterpret_cast<double*>(smem_raw + PC::off_q);  // [2][NS][TH]
+    T* dqs = reinterpret_cast<T*>(smem_raw + PC::off_dq);           // [2][NS][TH]
     const int nch = *B.nchunks;
     const int64_t tick = *B.tick;
-    const int el = threadIdx.x / S::NP;
-    for (int ci = blockIdx.x; ci < nch; ci += gridDim.x) {
+    const int tid = threadIdx.x, el = tid / NP, n = tid - el * NP;
+    const bool pf_dq = PC::PF && B.base.mode == MODE_STAGE;
+    auto live = [&](int ci) {
+        while (ci < nch && (B.chunks[ci].solve < 0 || B.chunks[ci].count <= 0)) ci += gridDim.x;
+        return ci;
+    };
+    auto elem = [&](int ci, int g, ElemPtrs& P, int64_t& e, bool& active) {
         const Chunk c = B.chunks[ci];
-        if (c.solve < 0 || c.count <= 0) continue;
         const SolveDesc& sd = B.solves[c.solve];
         const int par = (int)((tick - sd.start_tick + B.stage) & 1);
-        ElemPtrs P;
         P.q_in = sd.q[par];
         P.q_out = sd.q[par ^ 1];
         P.dq = sd.dq;
@@ -45,12 +57,56 @@ __global__ void __launch_bounds__(Shape<DIM, NQ, EPBX>::THREADS, 1)
         P.nbr = sd.nbr;
         P.rkb_dt = B.rkb * sd.dt;
         P.ncflux = nullptr;
-        for (int g = 0; g < c.count; g += S::EPB) {
-            const int64_t e = c.first + g + el;
-            stage_element<DIM, NQ, COMBO, GEOM, T, EPBX>(B.base, P, e, g + el < c.count, smem_raw);
-            __syncthreads();  // the shared partner values are reused by the next group
+        e = c.first + g + el;
+        active = g + el < c.count;
+    };
+    auto prefetch = [&](int ci, int g, int b) {
+        if (PC::PF && ci < nch) {
+            ElemPtrs P;
+            int64_t e;
+            bool active;
+            elem(ci, g, P, e, active);
+            if (active) {
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    const size_t gi = ((size_t)e * NS + s) * NP + n;
+                    cpa8(qs + (b * NS + s) * TH + tid, P.q_in + gi);
+                    if (pf_dq) {
+                        if constexpr (sizeof(T) == 4) cpa4(dqs + (b * NS + s) * TH + tid, static_cast<const float*>(P.dq) + gi);
+                        else cpa8(dqs + (b * NS + s) * TH + tid, static_cast<const double*>(P.dq) + gi);
+                    }
+                }
+            }
         }
+        cpa_commit();
+    };
+    int ci = live(blockIdx.x), g = 0, b = 0;
+    prefetch(ci, 0, 0);
+    while (ci < nch) {
+        int ci2 = ci, g2 = g + S::EPB;  // the CTA's next group
+        if (g2 >= B.chunks[ci].count) {
+            ci2 = live(ci + gridDim.x);
+            g2 = 0;
+        }
+        cpa_wait_all();
+        prefetch(ci2, g2, b ^ 1);
+        ElemPtrs P;
+        int64_t e;
+        bool active;
+        elem(ci, g, P, e, active);
+        Prefetched pf;
+        if (PC::PF) {
+            pf.q = qs + b * NS * TH + tid;
+            pf.dq = pf_dq ? static_cast<const void*>(dqs + b * NS * TH + tid) : nullptr;
+            pf.stride = TH;
+        }
+        stage_element<DIM, NQ, COMBO, GEOM, T, EPBX>(B.base, P, e, active, smem_raw, pf);
+        __syncthreads();  // the shared partner values are reused by the next group
+        ci = ci2;
+        g = g2;
+        b ^= 1;
     }
+    cpa_wait_all();
 }
 
 // Initial data of a brick solve evaluated on the device at its LGL nodes:

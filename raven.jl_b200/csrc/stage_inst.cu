@@ -49,10 +49,10 @@ cudaError_t RB_LAUNCH_NAME(int combo, int geom, int fp32, const StageArgs& a, cu
 template <int COMBO>
 static size_t smem_c(int geom, int fp32) {
     if (geom == GEOM_AFFINE)
-        return fp32 ? KernelCfg<RB_DIM, RB_NQ, COMBO, GEOM_AFFINE, float>::smem
-                    : KernelCfg<RB_DIM, RB_NQ, COMBO, GEOM_AFFINE, double>::smem;
-    return fp32 ? KernelCfg<RB_DIM, RB_NQ, COMBO, GEOM_CURVED, float>::smem
-                : KernelCfg<RB_DIM, RB_NQ, COMBO, GEOM_CURVED, double>::smem;
+        return fp32 ? PersistentCfg<RB_DIM, RB_NQ, COMBO, GEOM_AFFINE, float>::smem
+                    : PersistentCfg<RB_DIM, RB_NQ, COMBO, GEOM_AFFINE, double>::smem;
+    return fp32 ? PersistentCfg<RB_DIM, RB_NQ, COMBO, GEOM_CURVED, float>::smem
+                : PersistentCfg<RB_DIM, RB_NQ, COMBO, GEOM_CURVED, double>::smem;
 }
 
 size_t RB_SMEM_NAME(int combo, int geom, int fp32) {

@@ -69,6 +69,26 @@ __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+// cp.async of one value into shared memory (the persistent kernels' prefetch)
+__device__ __forceinline__ void cpa8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cpa4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cpa_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// A thread's own state and LSRK register, already copied into shared memory by the
+// thread itself (field s at q[s * stride]); null pointers: read them from global memory.
+struct Prefetched {
+    const double* q = nullptr;
+    const void* dq = nullptr;
+    int stride = 0;
+};
+
 __device__ __forceinline__ double dev_log(double x) { return log(x); }
 __device__ __forceinline__ float dev_log(float x) { return logf(x); }
 __device__ __forceinline__ double dev_sqrt(double x) { return sqrt(x); }
@@ -114,7 +134,8 @@ __device__ __forceinline__ ElemPtrs elem_ptrs(const StageArgs& A) {
 // (entropy conservative, Kennedy-Gruber, Roe, matrix dissipation; A.surface_flux).
 template <int DIM, int NQ, int COMBO, int GEOM, typename T, int EPBX, int SF = 0>
 __device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs& P, const int64_t e,
-                                              const bool active, unsigned char* smem_raw) {
+                                              const bool active, unsigned char* smem_raw,
+                                              const Prefetched pf = Prefetched{}) {
     using S = Shape<DIM, NQ, EPBX>;
     using C = CSize<COMBO, DIM>;
     using K = KernelCfg<DIM, NQ, COMBO, GEOM, T, EPBX>;
@@ -146,7 +167,7 @@ __device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs
         const double* qe = P.q_in + (size_t)e * NS * NP;
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
-            qd[s] = __ldg(qe + s * NP + n);
+            qd[s] = pf.q ? pf.q[s * pf.stride] : __ldg(qe + s * NP + n);
             q[s] = (T)qd[s];
         }
         if constexpr (AFF) {
@@ -364,7 +385,8 @@ __device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs
         T v = acc[s] * mjiT;
         if (A.mode == MODE_STAGE) {
             T old;
-            if (sizeof(T) == 4) old = (T) reinterpret_cast<const float*>(P.dq)[node0 + s * NP];
+            if (pf.dq) old = static_cast<const T*>(pf.dq)[s * pf.stride];
+            else if (sizeof(T) == 4) old = (T) reinterpret_cast<const float*>(P.dq)[node0 + s * NP];
             else old = (T) reinterpret_cast<const double*>(P.dq)[node0 + s * NP];
             v = (T)A.rka * old + v;
         } else if (A.mode == MODE_TENDENCY_INC) {
@@ -496,26 +518,108 @@ __device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs
     }
 }
 
+// Shared memory of the generic kernels: stage_element's arrays and, where the state and
+// register are prefetched (PF), two buffers of per-thread slots (FP64 state, T register).
+// Prefetching pays on 3-D elements in FP32 bulk (measured: 1.2-1.4x at Nq = 4 and 6);
+// 2-D elements and FP64 keep one group per CTA with direct loads, which measured faster.
+template <int DIM, int NQ, int COMBO, int GEOM, typename T, int EPBX = 0>
+struct PersistentCfg {
+    using S = Shape<DIM, NQ, EPBX>;
+    using K = KernelCfg<DIM, NQ, COMBO, GEOM, T, EPBX>;
+    static constexpr bool PF = DIM == 3 && sizeof(T) == 4;
+    static constexpr int NS = CSize<COMBO, DIM>::NS;
+    static constexpr size_t off_q = (K::smem + 15) / 16 * 16;
+    static constexpr size_t off_dq = off_q + (size_t)2 * NS * S::THREADS * sizeof(double);
+    static constexpr size_t smem = PF ? off_dq + (size_t)2 * NS * S::THREADS * sizeof(T) : K::smem;
+    // CTAs per SM the registers are sized for: about 768 resident threads per SM when the
+    // kernel loops over groups with prefetches (the loop otherwise lets the compiler keep
+    // more values live than one group needs, at the cost of residency)
+    static constexpr int MIN_CTAS = PF && S::THREADS < 768 ? 768 / S::THREADS : 1;
+};
+
+// Generic stage kernel.  Without prefetch (PC::PF false) one CTA runs one group of EPB
+// elements.  With it, each CTA walks element groups blockIdx.x + k*gridDim.x; while a
+// group runs, every thread copies the state (and, in stage mode, the LSRK register) of
+// its node in the CTA's next group into its own shared-memory slots with cp.async, so
+// those loads overlap the current group's arithmetic.  A thread reads only slots it
+// filled itself, so the copies need no barrier.
 template <int DIM, int NQ, int COMBO, int GEOM, typename T, int SF>
-__global__ void __launch_bounds__(Shape<DIM, NQ>::THREADS, 1)
+__global__ void __launch_bounds__(Shape<DIM, NQ>::THREADS, (PersistentCfg<DIM, NQ, COMBO, GEOM, T>::MIN_CTAS))
     stage_kernel(const __grid_constant__ StageArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using S = Shape<DIM, NQ>;
-    const int64_t e = (int64_t)blockIdx.x * S::EPB + threadIdx.x / S::NP;
-    stage_element<DIM, NQ, COMBO, GEOM, T, 0, SF>(A, elem_ptrs(A), e, e < A.E, smem_raw);
+    using PC = PersistentCfg<DIM, NQ, COMBO, GEOM, T>;
+    if constexpr (!PC::PF) {
+        const int64_t e = (int64_t)blockIdx.x * S::EPB + threadIdx.x / S::NP;
+        stage_element<DIM, NQ, COMBO, GEOM, T, 0, SF>(A, elem_ptrs(A), e, e < A.E, smem_raw);
+        return;
+    }
+    constexpr int NS = PC::NS, TH = S::THREADS, NP = S::NP;
+    double* qs = reinterpret_cast<double*>(smem_raw + PC::off_q);  // [2][NS][TH]
+    T* dqs = reinterpret_cast<T*>(smem_raw + PC::off_dq);           // [2][NS][TH]
+    const int tid = threadIdx.x, el = tid / NP, n = tid - el * NP;
+    const bool pf_dq = A.mode == MODE_STAGE;
+    const int64_t ngroups = (A.E + S::EPB - 1) / S::EPB;
+    const ElemPtrs P = elem_ptrs(A);
+    auto prefetch = [&](int64_t g, int b) {
+        const int64_t e = g * S::EPB + el;
+        if (g < ngroups && e < A.E) {
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                const size_t gi = ((size_t)e * NS + s) * NP + n;
+                cpa8(qs + (b * NS + s) * TH + tid, A.q_in + gi);
+                if (pf_dq) {
+                    if constexpr (sizeof(T) == 4) cpa4(dqs + (b * NS + s) * TH + tid, static_cast<const float*>(A.dq) + gi);
+                    else cpa8(dqs + (b * NS + s) * TH + tid, static_cast<const double*>(A.dq) + gi);
+                }
+            }
+        }
+        cpa_commit();
+    };
+    prefetch(blockIdx.x, 0);
+    int b = 0;
+    for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x, b ^= 1) {
+        cpa_wait_all();                  // this group's values (issued one iteration ago)
+        prefetch(g + gridDim.x, b ^ 1);  // the next group's, into the other buffer
+        const int64_t e = g * S::EPB + el;
+        Prefetched pf;
+        pf.q = qs + b * NS * TH + tid;
+        pf.dq = pf_dq ? static_cast<const void*>(dqs + b * NS * TH + tid) : nullptr;
+        pf.stride = TH;
+        stage_element<DIM, NQ, COMBO, GEOM, T, 0, SF>(A, P, e, e < A.E, smem_raw, pf);
+        __syncthreads();  // the shared partner values are reused by the next group
+    }
+    cpa_wait_all();
 }
 
 template <int DIM, int NQ, int COMBO, int GEOM, typename T, int SF = 0>
 cudaError_t launch_one(const StageArgs& a, cudaStream_t st) {
     using S = Shape<DIM, NQ>;
-    using K = KernelCfg<DIM, NQ, COMBO, GEOM, T>;
+    using PC = PersistentCfg<DIM, NQ, COMBO, GEOM, T>;
     auto kern = stage_kernel<DIM, NQ, COMBO, GEOM, T, SF>;
     static std::atomic<uint64_t> configured{0};
-    cudaError_t err = ensure_smem_limit(kern, (int)K::smem, configured);
+    cudaError_t err = ensure_smem_limit(kern, (int)PC::smem, configured);
     if (err != cudaSuccess) return err;
-    const int64_t blocks = (a.E + S::EPB - 1) / S::EPB;
-    if (blocks <= 0) return cudaSuccess;
-    kern<<<(unsigned)blocks, S::THREADS, K::smem, st>>>(a);
+    const int64_t groups = (a.E + S::EPB - 1) / S::EPB;
+    if (groups <= 0) return cudaSuccess;
+    if constexpr (!PC::PF) {
+        kern<<<(unsigned)groups, S::THREADS, PC::smem, st>>>(a);
+        return cudaGetLastError();
+    }
+    // persistent grid: the resident CTAs of every SM, cached per device
+    static std::atomic<int> grid_of_device[64];
+    int dev = 0;
+    if ((err = cudaGetDevice(&dev)) != cudaSuccess) return err;
+    int grid = (dev >= 0 && dev < 64) ? grid_of_device[dev].load(std::memory_order_relaxed) : 0;
+    if (grid <= 0) {
+        int per_sm = 0, nsm = 0;
+        if ((err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, S::THREADS, PC::smem)) != cudaSuccess)
+            return err;
+        if ((err = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return err;
+        grid = per_sm > 0 ? per_sm * nsm : 1;
+        if (dev >= 0 && dev < 64) grid_of_device[dev].store(grid, std::memory_order_relaxed);
+    }
+    kern<<<(unsigned)std::min<int64_t>(grid, groups), S::THREADS, PC::smem, st>>>(a);
     return cudaGetLastError();
 }
 
