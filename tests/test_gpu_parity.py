@@ -203,3 +203,29 @@ def test_graph_replay_equals_eager_steps(rb, cuda_ok, case):
             sb.dostep(qb, 1)
         assert np.array_equal(qa.numpy(), qb.numpy())
         assert np.array_equal(sa.dq.numpy(), sb.dq.numpy())
+
+
+@pytest.mark.parametrize("nq,K", [(4, (12, 12, 13)), (6, (10, 10, 9)), (5, (12, 12, 10))], ids=["nq4", "nq6", "nq5"])
+def test_generic_fp32_bulk_steps_walk_groups(rb, cuda_ok, nq, K):
+    """3-D FP32-bulk stages on the generic kernel, whose CTAs walk several element groups
+    each (more elements than resident CTAs) and prefetch the next group's state and
+    register: two steps against the oracle (1e-6 relative on the state), and five steps,
+    the last three graph-replayed, against a run restarted from a snapshot after two."""
+    og, g, dg, olaw, law = _build(rb, 3, nq, K, (1, 1, 1), "eul_kg", O.WARP_NONE, precision="fp32_bulk")
+    assert dg.pipelined_ctas == 0
+    q = initial_state(og, olaw, "eul_kg", seed=21, amp=0.01)
+    qo, dqo = q.copy(order="F"), og.state(olaw)
+    for i in range(2):
+        og.lsrk54_step(olaw, qo, dqo, i * 1e-3, 1e-3)
+    qg = rb.GridArray.from_numpy(q)
+    solver = rb.LSRK54(dg, qg, 1e-3)
+    solver.dostep(qg, 2)
+    for s in range(law.ns):
+        assert rel_err(qg.numpy()[:, s], qo[:, s]) <= 1e-6, s
+    snap = rb.snapshot(dg, qg, solver)
+    solver.dostep(qg, 3)
+    q2 = rb.GridArray.from_numpy(np.zeros_like(q))
+    s2 = rb.LSRK54(dg, q2, 1.0)
+    rb.restore(dg, snap, q2, s2)
+    s2.dostep(q2, 3)
+    assert np.array_equal(q2.numpy(), qg.numpy())
