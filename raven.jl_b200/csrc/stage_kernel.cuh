@@ -60,7 +60,11 @@ struct KernelCfg {
     using S = Shape<DIM, NQ, EPBX>;
     using C = CSize<COMBO, DIM>;
     static constexpr int NLG = GEOM == GEOM_AFFINE ? DIM : DIM * DIM;
-    static constexpr size_t smem = (size_t)S::EPB * (C::NAUX + NLG) * S::NP * sizeof(T);
+    // partner values and metric rows of the CTA's elements, then the derivative matrix D
+    // (read per pair with thread-dependent indices: from shared memory rather than the
+    // kernel parameters, whose constant cache serialises distinct addresses in a warp)
+    static constexpr size_t off_D = (size_t)S::EPB * (C::NAUX + NLG) * S::NP * sizeof(T);
+    static constexpr size_t smem = off_D + (size_t)NQ * NQ * sizeof(T);
 };
 
 // Products and differences that must not be contracted into an FMA (they make the
@@ -145,6 +149,7 @@ __device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs
 
     T* s_aux = reinterpret_cast<T*>(smem_raw);
     T* s_lg = s_aux + EPB * NAUX * NP;
+    T* sD = reinterpret_cast<T*>(smem_raw + K::off_D);  // D[i + NQ j] = l_j'(r_i)
 
     const int tid = threadIdx.x;
     const int el = tid / NP;
@@ -271,6 +276,7 @@ __device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs
 #pragma unroll
         for (int k = 0; k < NAUX; ++k) aux[k * NP + n] = own[k];
     }
+    for (int i = tid; i < NQ * NQ; i += S::THREADS) sD[i] = (T)A.D[i];
     __syncthreads();
     if (!active) return;
 
@@ -287,14 +293,15 @@ __device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs
 #pragma unroll
         for (int a = 0; a < NQ; ++a) {
             const int na = base + a * stride;
-            const T Dai = (T)A.D[a + NQ * idd];  // D[a, id]
+            // D[a, id]: FP32 from shared memory (measured faster), FP64 from the parameters
+            const T Dai = sizeof(T) == 4 ? sD[a + NQ * idd] : (T)A.D[a + NQ * idd];
             if constexpr (COMBO == ADV_WEAK) {
                 acc[0] += Dai * aux[dir * NP + na];
             } else if constexpr (COMBO == EUL_WEAK) {
 #pragma unroll
                 for (int s = 0; s < NS; ++s) acc[s] += Dai * aux[(dir * NS + s) * NP + na];
             } else {
-                const T Dia = (T)A.D[idd + NQ * a];  // D[id, a]
+                const T Dia = sizeof(T) == 4 ? sD[idd + NQ * a] : (T)A.D[idd + NQ * a];  // D[id, a]
                 // metric combination G_d = D[a,id] l_g[a][d] - D[id,a] l_g[i][d]
                 T G[DIM];
                 if constexpr (AFF) {
@@ -534,7 +541,11 @@ struct PersistentCfg {
     // CTAs per SM the registers are sized for: about 768 resident threads per SM when the
     // kernel loops over groups with prefetches (the loop otherwise lets the compiler keep
     // more values live than one group needs, at the cost of residency)
-    static constexpr int MIN_CTAS = PF && S::THREADS < 768 ? 768 / S::THREADS : 1;
+#ifndef RB200_ADV_TARGET
+#define RB200_ADV_TARGET 2048
+#endif
+    static constexpr int TARGET = NS == 1 ? RB200_ADV_TARGET : 768;
+    static constexpr int MIN_CTAS = PF && S::THREADS < TARGET ? TARGET / S::THREADS : 1;
 };
 
 // Generic stage kernel.  Without prefetch (PC::PF false) one CTA runs one group of EPB
