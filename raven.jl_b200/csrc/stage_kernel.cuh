@@ -132,6 +132,110 @@ __device__ __forceinline__ ElemPtrs elem_ptrs(const StageArgs& A) {
     return ElemPtrs{A.q_in, A.q_out, A.dq, A.elem_geo, A.vgeo, A.sgeo, A.nbr, A.rkb_dt, A.ncflux};
 }
 
+// Weak-form advection on an unwarped element (the stage of stage_element, refactored for
+// bricks).  Along a line in direction dir the metric and mass factors of volumeterm!
+// (dgsem.jl:299-308, 326-343) reduce to MJI_i wJ_a drdx = (w_a / w_i) drdx, so
+//     dq_i += sum_dir drdx_dir a_dir sum_a W[a][i] q_a,    W[a][i] = D[a,i] w_a / w_i,
+// and on a face (wsJ MJI) = |drdx_dir| / w_0 (lobattocells.jl:3285-3291; LGL weights are
+// symmetric).  One field: the partner values are the state itself.
+template <int DIM, int NQ, typename T, int EPBX>
+__device__ __forceinline__ void stage_element_adv_brick(const StageArgs& A, const ElemPtrs& P, const int64_t e,
+                                                        const bool active, unsigned char* smem_raw,
+                                                        const Prefetched pf) {
+    using S = Shape<DIM, NQ, EPBX>;
+    constexpr int NP = S::NP, NFP = S::NFP, NF = S::NF, EPB = S::EPB;
+    T* sq = reinterpret_cast<T*>(smem_raw);  // q of the CTA's elements
+    T* sW = sq + EPB * NP;                   // W[a + NQ i]
+    const int tid = threadIdx.x;
+    const int el = tid / NP;
+    const int n = tid - el * NP;
+    int id[3];
+    id[0] = n % NQ;
+    id[1] = DIM > 1 ? (n / NQ) % NQ : 0;
+    id[2] = DIM > 2 ? n / (NQ * NQ) : 0;
+    double qd = 0.0, drdx[3] = {0.0, 0.0, 0.0};
+    T q0 = T(0);
+    if (active) {
+        qd = pf.q ? pf.q[0] : __ldg(P.q_in + (size_t)e * NP + n);
+        q0 = (T)qd;
+        const double* eg = P.elem_geo + 4 * e;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) drdx[d] = __ldg(eg + d);
+        sq[el * NP + n] = q0;
+    }
+    for (int i = tid; i < NQ * NQ; i += S::THREADS) {
+        const int a = i % NQ, ii = i / NQ;
+        sW[i] = (T)(A.D[a + NQ * ii] * (A.w[a] / A.w[ii]));
+    }
+    __syncthreads();
+    if (!active) return;
+
+    // ---- volume term
+    const T* qe = sq + el * NP;
+    T acc = T(0);
+#pragma unroll
+    for (int dir = 0; dir < DIM; ++dir) {
+        const int stride = dir == 0 ? 1 : (dir == 1 ? NQ : NQ * NQ);
+        const int idd = id[dir];
+        const int base = n - idd * stride;
+        T sum = T(0);
+#pragma unroll
+        for (int a = 0; a < NQ; ++a) sum += sW[a + NQ * idd] * qe[base + a * stride];
+        acc += ((T)drdx[dir] * (T)A.adv[dir]) * sum;
+    }
+
+    // ---- combine with dq
+    const bool stage = A.mode >= MODE_STAGE;
+    const size_t node0 = (size_t)e * NP + n;
+    T v = acc;
+    if (A.mode == MODE_STAGE) {
+        T old;
+        if (pf.dq) old = static_cast<const T*>(pf.dq)[0];
+        else if (sizeof(T) == 4) old = (T) reinterpret_cast<const float*>(P.dq)[node0];
+        else old = (T) reinterpret_cast<const double*>(P.dq)[node0];
+        v = (T)A.rka * old + v;
+    } else if (A.mode == MODE_TENDENCY_INC) {
+        v = (T)(reinterpret_cast<const double*>(P.dq)[node0] + (double)v);
+    }
+
+    // ---- surface term, faces in the order x-, x+, y-, y+, z-, z+ (dgsem.jl:756-782)
+#pragma unroll
+    for (int dir = 0; dir < DIM; ++dir) {
+        const int idd = id[dir];
+        if (idd != 0 && idd != NQ - 1) continue;
+        const int side = idd == 0 ? 0 : 1;
+        const int f = 2 * dir + side;
+        const int stride = dir == 0 ? 1 : (dir == 1 ? NQ : NQ * NQ);
+        const int ne = __ldg(P.nbr + (size_t)NF * e + f);
+        T nf;
+        if (ne == -2) {  // mortar face: the flux comes from the mortar kernel
+            int j;
+            if (DIM == 2) j = (dir == 0) ? id[1] : id[0];
+            else j = (dir == 0) ? id[1] + NQ * id[2] : (dir == 1 ? id[0] + NQ * id[2] : id[0] + NQ * id[1]);
+            nf = (T)__ldg(P.ncflux + ((size_t)e * NF + f) * NFP + j);
+        } else {
+            T qp = q0;  // default boundarystate (balancelaw.jl:77)
+            if (ne >= 0) {
+                const int nn = n + (side == 0 ? (NQ - 1) * stride : -(NQ - 1) * stride);
+                qp = (T)__ldg(P.q_in + (size_t)ne * NP + nn);
+            }
+            const T an = (T)A.adv[dir] * (side == 0 ? T(-1) : T(1));
+            const T fc = (an * q0 + an * qp) * T(0.5);
+            nf = A.surface_rusanov ? fc - (fabs(an) * (qp - q0)) * T(0.5) : fc;
+        }
+        v = v - nf * (T)(fabs(drdx[dir]) / A.w[0]);
+    }
+
+    // ---- write back
+    if (stage) {
+        if (sizeof(T) == 4) reinterpret_cast<float*>(P.dq)[node0] = (float)v;
+        else reinterpret_cast<double*>(P.dq)[node0] = (double)v;
+        P.q_out[node0] = qd + P.rkb_dt * (double)v;
+    } else {
+        reinterpret_cast<double*>(P.dq)[node0] = (double)v;
+    }
+}
+
 // One element per group of Np threads: the whole fused stage for element e.  All
 // threads of the CTA must call it (it contains a barrier); inactive groups pass
 // active = false.  SF = 1: the Euler surface flux is one of the entropy family
@@ -146,6 +250,10 @@ __device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs
     constexpr int NP = S::NP, NFP = S::NFP, NF = S::NF, EPB = S::EPB;
     constexpr int NS = C::NS, NAUX = C::NAUX, NLG = K::NLG;
     constexpr bool AFF = GEOM == GEOM_AFFINE;
+    if constexpr (COMBO == ADV_WEAK && AFF) {
+        stage_element_adv_brick<DIM, NQ, T, EPBX>(A, P, e, active, smem_raw, pf);
+        return;
+    }
 
     T* s_aux = reinterpret_cast<T*>(smem_raw);
     T* s_lg = s_aux + EPB * NAUX * NP;
