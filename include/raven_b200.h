@@ -180,6 +180,13 @@ rb200_status rb200_set_kernel_path(rb200_handle* h, int32_t path);
  * up a bounded wait since the handle was created, RB200_OK otherwise. */
 rb200_status rb200_sync_status(rb200_handle* h, void* stream);
 
+/* Diagnostics of the bounded waits: launches one CTA that polls an mbarrier nothing
+ * completes, with the stage kernels' try_wait loop limited to `polls` polls
+ * (1..2^30).  Returns RB200_ERR_TIMEOUT when the kernel gave up and recorded it (the
+ * expected outcome; the context stays usable), RB200_OK if the wait ended otherwise.
+ * Synchronous on `stream`; allocates and frees 4 bytes of device memory. */
+rb200_status rb200_probe_bounded_wait(int64_t polls, void* stream);
+
 /* Handle properties: info[0]=dim, [1]=nq, [2]=Ns, [3]=E, [4]=geometry kind
  * (0 affine brick, 1 curved), [5]=precision, [6]=kernel launches per LSRK step,
  * [7]=algorithmic HBM bytes per node per stage, [8]=CTAs of the pipelined kernel of the

@@ -40,7 +40,8 @@ def _sources():
     for d in (2, 3):
         units.append((os.path.join(CSRC, "serve_inst.cu"), os.path.join(BUILD, f"serve_d{d}.o"),
                       [f"-DRB_SERVE_DIM={d}"]))
-    for name in ("dispatch", "reduce", "pipelined_inst", "serve", "utilities", "mortar", "relaxation", "api"):
+    for name in ("dispatch", "reduce", "pipelined_inst", "serve", "utilities", "mortar", "relaxation", "diagnostics",
+                 "api"):
         units.append((os.path.join(CSRC, f"{name}.cu"), os.path.join(BUILD, f"{name}.o"), []))
     return units
 

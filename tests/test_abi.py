@@ -121,3 +121,9 @@ def test_status_strings(rb):
     assert L.rb200_status_string(0) == b"ok"
     assert L.rb200_status_string(6) == b"unsupported"
     assert L.rb200_last_error(None) == b"null handle"
+
+
+def test_bounded_wait_probe_validates_before_the_device(rb):
+    L = rb._lib.lib()
+    assert L.rb200_probe_bounded_wait(0, None) == 1  # RB200_ERR_BAD_ARG, no device call
+    assert L.rb200_probe_bounded_wait(1 << 31, None) == 1
