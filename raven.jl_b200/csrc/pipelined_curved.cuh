@@ -186,9 +186,10 @@ __global__ void __launch_bounds__(256, 2) pipelined_curved_kernel(const __grid_c
         auto pair = [&](float (&ac)[NS], const float (&o)[NAUX], const float4 pa, const float2 pb, const float4 lp,
                         const float* lo, const float Dai, const float Dia) {
             float G[3];
-            G[0] = __fsub_rn(__fmul_rn(Dai, lp.x), __fmul_rn(Dia, lo[0]));
-            G[1] = __fsub_rn(__fmul_rn(Dai, lp.y), __fmul_rn(Dia, lo[1]));
-            G[2] = __fsub_rn(__fmul_rn(Dai, lp.z), __fmul_rn(Dia, lo[2]));
+            // the self pair, whose G must cancel exactly, is never formed (a != i)
+            G[0] = fmaf(Dai, lp.x, -(Dia * lo[0]));
+            G[1] = fmaf(Dai, lp.y, -(Dia * lo[1]));
+            G[2] = fmaf(Dai, lp.z, -(Dia * lo[2]));
             const float rb = o[0] + pa.x;
             const float ub0 = o[1] + pa.y, ub1 = o[2] + pa.z, ub2 = o[3] + pa.w;
             const float eb = o[4] + pb.x, pbar = o[5] + pb.y;
