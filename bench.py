@@ -527,6 +527,7 @@ def run_serving(args):
     sampler.stop()
     st = srv.stats()
     tiles = srv.class_tiles()
+    class_stats = srv.class_stats()
     srv.close()
     lat = res["latencies"]
     dof = float(sum(a.spec.dof_updates() for a in arrivals))
@@ -588,6 +589,9 @@ def run_serving(args):
                 "total_dof_updates": dof,
                 "arena_peak_bytes": st["arena_peak"],
                 "class_tiles": [list(t) for t in tiles],
+                # per class: device time of its ticks (classes overlap) and DOF updates/s there
+                "classes": [dict(r, dof_per_s=r["dof_updates"] / (r["device_ms"] / 1e3) if r["device_ms"] else None)
+                            for r in class_stats],
             },
             "roofline": {
                 "bound": "hbm",

@@ -293,6 +293,12 @@ rb200_status rb200_server_stats(rb200_server* s, double* out, int32_t n);
  * autotuner chose (0 while it is still timing).  Unused entries are 0. */
 rb200_status rb200_server_class_tiles(rb200_server* s, int32_t* out, int32_t n);
 
+/* Per class, 6 values: dim, nq, internal kernel combination, completed ticks, device
+ * milliseconds of those ticks (from events around each tick on the class's stream;
+ * classes run concurrently, so the times of different classes overlap), DOF updates of
+ * those ticks (elements x Np x Ns x 5 stages).  Unused entries are 0. */
+rb200_status rb200_server_class_stats(rb200_server* s, double* out, int32_t n);
+
 /* Message of the error that stopped the server (empty if none).  Valid until destroy. */
 const char* rb200_server_last_error(rb200_server* s);
 

@@ -51,6 +51,7 @@ EXPORTED = [
     "rb200_server_wait",
     "rb200_server_stats",
     "rb200_server_class_tiles",
+    "rb200_server_class_stats",
     "rb200_server_last_error",
     "rb200_server_destroy",
     "rb200_kron_apply",
@@ -174,6 +175,7 @@ def lib():
     L.rb200_server_wait.argtypes = [P, ctypes.c_uint64, D, ctypes.POINTER(D)]
     L.rb200_server_stats.argtypes = [P, P, I32]
     L.rb200_server_class_tiles.argtypes = [P, P, I32]
+    L.rb200_server_class_stats.argtypes = [P, P, I32]
     L.rb200_server_last_error.argtypes = [P]
     L.rb200_server_last_error.restype = ctypes.c_char_p
     L.rb200_server_destroy.argtypes = [P]

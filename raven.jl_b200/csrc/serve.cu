@@ -218,7 +218,11 @@ struct Class {
     double tune_ms[3] = {0, 0, 0};
     int tune_n[3] = {0, 0, 0};
     int last_tile = 1;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // tick start (while tuning) and end
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // tick start and end
+    // totals of the completed ticks: device time between the tick's events (classes run
+    // concurrently, so these overlap across classes) and DOF updates
+    int64_t ticks_done = 0;
+    double busy_ms = 0.0, dof_updates = 0.0;
     bool pipelined = false;                      // 3-D Nq=8 Euler KG: the pipelined kernel
     int32_t* d_status = nullptr;                 // its bounded waits report here
     int active = 0;
@@ -508,7 +512,7 @@ cudaError_t launch_tick(Class& c) {
     // autotuner: the first 2*ntiles ticks cycle through the tiles, then the fastest stays
     const bool tuning = c.tune_done < 2 * c.ntiles;
     c.last_tile = tuning ? c.tune_done % c.ntiles : c.tile;
-    if (tuning) e = cudaEventRecord(c.ev0, c.stream);
+    e = cudaEventRecord(c.ev0, c.stream);
     if (e == cudaSuccess) e = cudaGraphLaunch(c.graph[c.last_tile], c.stream);
     if (e == cudaSuccess) e = cudaEventRecord(c.ev1, c.stream);  // completion of the tick
     c.launched = e == cudaSuccess;
@@ -519,13 +523,16 @@ cudaError_t launch_tick(Class& c) {
 cudaError_t finish_tick(rb200_server* s, Class& c) {
     c.launched = false;
     const int64_t done_tick = c.tick;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c.ev0, c.ev1);
+    int64_t elems = 0;  // elements of the solves the tick advanced
+    for (auto* sv : c.slots)
+        if (sv && sv->desc.start_tick <= done_tick) elems += sv->desc.E;
+    c.ticks_done += 1;
+    c.busy_ms += ms;
+    c.dof_updates += (double)elems * c.np * c.ns * 5.0;
     if (c.tune_done < 2 * c.ntiles) {
-        float ms = 0;
-        cudaEventElapsedTime(&ms, c.ev0, c.ev1);
         // normalise by the elements of the tick so that ticks of different batches compare
-        int64_t elems = 0;
-        for (auto* sv : c.slots)
-            if (sv && sv->desc.start_tick <= done_tick) elems += sv->desc.E;
         c.tune_ms[c.last_tile] += elems > 0 ? ms / (double)elems : ms;
         c.tune_n[c.last_tile] += 1;
         if (++c.tune_done == 2 * c.ntiles) {
@@ -776,6 +783,24 @@ rb200_status rb200_server_class_tiles(rb200_server* s, int32_t* out, int32_t n) 
         out[i++] = c.nq;
         out[i++] = c.combo;
         out[i++] = c.tune_done >= 2 * c.ntiles ? c.epb[c.tile] : 0;
+    }
+    return RB200_OK;
+}
+
+rb200_status rb200_server_class_stats(rb200_server* s, double* out, int32_t n) {
+    if (!s || !out) return RB200_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (int i = 0; i < n; ++i) out[i] = 0.0;
+    int i = 0;
+    for (auto& kv : s->classes) {
+        if (i + 6 > n) break;
+        const Class& c = *kv.second;
+        out[i++] = c.dim;
+        out[i++] = c.nq;
+        out[i++] = c.combo;
+        out[i++] = (double)c.ticks_done;
+        out[i++] = c.busy_ms;
+        out[i++] = c.dof_updates;
     }
     return RB200_OK;
 }

@@ -254,6 +254,23 @@ class Server:
         vals = list(buf)
         return [tuple(vals[i:i + 4]) for i in range(0, 256, 4) if vals[i] != 0]
 
+    def class_stats(self):
+        """Per class: dim, nq, kernel combination, completed ticks, device milliseconds of
+        those ticks (classes overlap on the device) and their DOF updates."""
+        buf = (ctypes.c_double * 384)()
+        _lib.check(_lib.lib().rb200_server_class_stats(self._h, buf, 384))
+        vals = list(buf)
+        keys = ("dim", "nq", "combo", "ticks", "device_ms", "dof_updates")
+        rows = []
+        for i in range(0, 384, 6):
+            if vals[i] == 0:
+                continue
+            r = dict(zip(keys, vals[i:i + 6]))
+            for k in ("dim", "nq", "combo", "ticks"):
+                r[k] = int(r[k])
+            rows.append(r)
+        return rows
+
     def last_error(self):
         return _lib.lib().rb200_server_last_error(self._h).decode()
 
