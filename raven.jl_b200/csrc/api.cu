@@ -207,7 +207,7 @@ cudaError_t launch_any(rb200_handle* h, const StageArgs& a, cudaStream_t st) {
     std::memcpy(p.S, h->pipe_S, sizeof(p.S));
     std::memcpy(p.w, h->w, sizeof(p.w));
     const int grid = (int)std::min<int64_t>(h->pipe_grid, a.E);
-    return launch_pipelined(h->combo, h->prec, p, grid, st);
+    return launch_pipelined(h->nq, h->combo, h->prec, p, grid, st);
 }
 
 StageArgs base_args(const rb200_handle* h) {
@@ -619,14 +619,15 @@ rb200_status rb200_create(const rb200_desc* d, rb200_handle** out) {
     if ((st = dev_alloc(h, &h->d_status, 1)) != RB200_OK) return bail(st);
     ce = cudaMemset(h->d_status, 0, sizeof(int32_t));
     if (ce != cudaSuccess) return bail(cuda_fail(h, ce, "memset"));
-    if (dim == 3 && nq == 8 && affine && (h->combo == EUL_KG || h->combo == EUL_EC) && !entropy_flux) {
-        for (int a = 0; a < 8; ++a)
-            for (int id = 0; id < 8; ++id)
-                h->pipe_S[a * 8 + id] = h->D[a + 8 * id] * (h->w[a] / h->w[id]) - h->D[id + 8 * a];
+    if (dim == 3 && (nq == 4 || nq == 6 || nq == 8) && affine && (h->combo == EUL_KG || h->combo == EUL_EC) &&
+        !entropy_flux) {
+        for (int a = 0; a < nq; ++a)
+            for (int id = 0; id < nq; ++id)
+                h->pipe_S[a * nq + id] = h->D[a + nq * id] * (h->w[a] / h->w[id]) - h->D[id + nq * a];
         int dev = 0, nsm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        const int per_sm = pipelined_blocks_per_sm(h->combo, h->prec);
+        const int per_sm = pipelined_blocks_per_sm(nq, h->combo, h->prec);
         h->pipe_grid = per_sm > 0 ? per_sm * nsm : 0;
         cudaGetLastError();
     }

@@ -10,52 +10,75 @@ namespace rb200 {
 #endif
 constexpr int kNPT = RB200_PIPE_NPT;
 
-template <int COMBO, typename T, bool BATCH>
+template <int COMBO, typename T, bool BATCH, int Q>
 static cudaError_t launch_p(const PipeArgs& a, const PipeBatch& b, int grid, cudaStream_t s) {
-    auto kern = pipelined_stage_kernel<COMBO, T, kNPT, BATCH>;
+    auto kern = pipelined_stage_kernel<COMBO, T, kNPT, BATCH, Q>;
     static std::atomic<uint64_t> configured{0};
-    cudaError_t err = ensure_smem_limit(kern, (int)sizeof(pipe::Smem<T>), configured);
+    cudaError_t err = ensure_smem_limit(kern, (int)sizeof(pipe::Smem<T, Q>), configured);
     if (err != cudaSuccess) return err;
-    kern<<<grid, 512 / kNPT, sizeof(pipe::Smem<T>), s>>>(a, b);
+    kern<<<grid, Q * Q * Q / kNPT, sizeof(pipe::Smem<T, Q>), s>>>(a, b);
     return cudaGetLastError();
 }
 
-cudaError_t launch_pipelined(int combo, int fp32, const PipeArgs& a, int grid, cudaStream_t s) {
+template <int COMBO, typename T, bool BATCH>
+static cudaError_t launch_q(int nq, const PipeArgs& a, const PipeBatch& b, int grid, cudaStream_t s) {
+    switch (nq) {
+        case 4: return launch_p<COMBO, T, BATCH, 4>(a, b, grid, s);
+        case 6: return launch_p<COMBO, T, BATCH, 6>(a, b, grid, s);
+        case 8: return launch_p<COMBO, T, BATCH, 8>(a, b, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_pipelined(int nq, int combo, int fp32, const PipeArgs& a, int grid, cudaStream_t s) {
     const PipeBatch none{};
     if (combo == EUL_KG)
-        return fp32 ? launch_p<EUL_KG, float, false>(a, none, grid, s) : launch_p<EUL_KG, double, false>(a, none, grid, s);
+        return fp32 ? launch_q<EUL_KG, float, false>(nq, a, none, grid, s)
+                    : launch_q<EUL_KG, double, false>(nq, a, none, grid, s);
     if (combo == EUL_EC)
-        return fp32 ? launch_p<EUL_EC, float, false>(a, none, grid, s) : launch_p<EUL_EC, double, false>(a, none, grid, s);
+        return fp32 ? launch_q<EUL_EC, float, false>(nq, a, none, grid, s)
+                    : launch_q<EUL_EC, double, false>(nq, a, none, grid, s);
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_pipelined_batch(int combo, int fp32, const PipeArgs& a, const PipeBatch& b, int grid,
+cudaError_t launch_pipelined_batch(int nq, int combo, int fp32, const PipeArgs& a, const PipeBatch& b, int grid,
                                    cudaStream_t s) {
     if (combo == EUL_KG)
-        return fp32 ? launch_p<EUL_KG, float, true>(a, b, grid, s) : launch_p<EUL_KG, double, true>(a, b, grid, s);
+        return fp32 ? launch_q<EUL_KG, float, true>(nq, a, b, grid, s) : launch_q<EUL_KG, double, true>(nq, a, b, grid, s);
     return cudaErrorInvalidValue;
 }
 
-template <int COMBO, typename T, bool BATCH>
+template <int COMBO, typename T, bool BATCH, int Q>
 static int occupancy_p() {
-    auto kern = pipelined_stage_kernel<COMBO, T, kNPT, BATCH>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(pipe::Smem<T>)) !=
+    auto kern = pipelined_stage_kernel<COMBO, T, kNPT, BATCH, Q>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(pipe::Smem<T, Q>)) !=
         cudaSuccess)
         return 0;
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, 512 / kNPT, sizeof(pipe::Smem<T>)) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, Q * Q * Q / kNPT, sizeof(pipe::Smem<T, Q>)) !=
+        cudaSuccess)
         return 0;
     return n;
 }
 
-int pipelined_blocks_per_sm(int combo, int fp32) {
-    if (combo == EUL_KG) return fp32 ? occupancy_p<EUL_KG, float, false>() : occupancy_p<EUL_KG, double, false>();
-    if (combo == EUL_EC) return fp32 ? occupancy_p<EUL_EC, float, false>() : occupancy_p<EUL_EC, double, false>();
+template <int COMBO, typename T, bool BATCH>
+static int occupancy_q(int nq) {
+    switch (nq) {
+        case 4: return occupancy_p<COMBO, T, BATCH, 4>();
+        case 6: return occupancy_p<COMBO, T, BATCH, 6>();
+        case 8: return occupancy_p<COMBO, T, BATCH, 8>();
+        default: return 0;
+    }
+}
+
+int pipelined_blocks_per_sm(int nq, int combo, int fp32) {
+    if (combo == EUL_KG) return fp32 ? occupancy_q<EUL_KG, float, false>(nq) : occupancy_q<EUL_KG, double, false>(nq);
+    if (combo == EUL_EC) return fp32 ? occupancy_q<EUL_EC, float, false>(nq) : occupancy_q<EUL_EC, double, false>(nq);
     return 0;
 }
 
-int pipelined_batch_blocks_per_sm(int combo, int fp32) {
-    if (combo == EUL_KG) return fp32 ? occupancy_p<EUL_KG, float, true>() : occupancy_p<EUL_KG, double, true>();
+int pipelined_batch_blocks_per_sm(int nq, int combo, int fp32) {
+    if (combo == EUL_KG) return fp32 ? occupancy_q<EUL_KG, float, true>(nq) : occupancy_q<EUL_KG, double, true>(nq);
     return 0;
 }
 

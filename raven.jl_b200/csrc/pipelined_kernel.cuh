@@ -1,5 +1,5 @@
-// Persistent, TMA-pipelined stage kernel for 3-D hexahedra with Nq = 8 on unwarped
-// bricks, flux-differencing volume forms (Kennedy-Gruber, entropy conservative).
+// Persistent, TMA-pipelined stage kernel for 3-D hexahedra on unwarped bricks (Nq = 4, 6
+// or 8), flux-differencing volume forms (Kennedy-Gruber, entropy conservative).
 //
 // Each CTA owns a strided set of elements (e = blockIdx.x + k*gridDim.x); two CTAs share
 // an SM in FP64, three in FP32 bulk.
@@ -44,7 +44,7 @@ struct PipeArgs {
     int32_t mode;
     int32_t surface_rusanov;
     double rka, rkb_dt, gamma;
-    double S[64];  // S[a*8 + id] = D[a,id] * w[a] / w[id] - D[id,a]
+    double S[64];  // S[a*Nq + id] = D[a,id] * w[a] / w[id] - D[id,a]
     double w[8];
 };
 
@@ -72,9 +72,17 @@ struct ElemRef {
 
 namespace pipe {
 
-constexpr int NQ = 8, NP = 512, NS = 5, NAUX = 6, NSLOT = 384;
+constexpr int NQ = 8, NP = 512, NS = 5, NAUX = 6, NSLOT = 384;  // the Nq = 8 element
 constexpr int PAD(int n) { return n + (n >> 3); }  // one vector slot of padding every 8 nodes
 constexpr int NPP = PAD(NP);                       // padded plane length
+
+// Sizes of an element with Q nodes per direction (Q even: an element's state is then a
+// whole number of 16-byte units, as the bulk copies need).
+template <int Q>
+struct Geo {
+    static_assert(Q % 2 == 0 && Q >= 4 && Q <= 8, "Nq = 4, 6 or 8");
+    static constexpr int NQ = Q, NP = Q * Q * Q, NFP = Q * Q, NSLOT = 6 * Q * Q, NPP = PAD(Q * Q * Q);
+};
 constexpr long kWaitLimit = 1L << 26;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -127,11 +135,11 @@ __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier
 
 // Per-node partner values (6 per node), read as vectors: three 16-byte loads in FP64, one
 // 16-byte and one 8-byte load in FP32.
-template <typename T>
+template <typename T, int NPP_ = NPP>
 struct AuxBuf;
-template <>
-struct AuxBuf<double> {
-    double2 v[NAUX / 2][NPP];
+template <int NPP_>
+struct AuxBuf<double, NPP_> {
+    double2 v[NAUX / 2][NPP_];
     __device__ __forceinline__ void put(int i, const double (&o)[NAUX]) {
 #pragma unroll
         for (int c = 0; c < NAUX / 2; ++c) v[c][i] = make_double2(o[2 * c], o[2 * c + 1]);
@@ -145,10 +153,10 @@ struct AuxBuf<double> {
         }
     }
 };
-template <>
-struct AuxBuf<float> {
-    float4 a[NPP];
-    float2 b[NPP];
+template <int NPP_>
+struct AuxBuf<float, NPP_> {
+    float4 a[NPP_];
+    float2 b[NPP_];
     __device__ __forceinline__ void put(int i, const float (&o)[NAUX]) {
         a[i] = make_float4(o[0], o[1], o[2], o[3]);
         b[i] = make_float2(o[4], o[5]);
@@ -165,16 +173,17 @@ struct AuxBuf<float> {
     }
 };
 
-template <typename T>
+template <typename T, int Q = 8>
 struct Smem {
-    double q[NS][NP];                           // state of the element (TMA destination)
-    AuxBuf<T> aux;                              // per-node partner values
-    double slot[NS][NSLOT];                     // neighbour trace, then (wsJ * nf) * MJI, per face slot
-    T S[3][NQ][NQ];                             // S_dir[a][id] * drdx_dir of the current element
+    using G = Geo<Q>;
+    double q[NS][G::NP];                        // state of the element (TMA destination)
+    AuxBuf<T, G::NPP> aux;                      // per-node partner values
+    double slot[NS][G::NSLOT];                  // neighbour trace, then (wsJ * nf) * MJI, per face slot
+    T S[3][Q][Q];                               // S_dir[a][id] * drdx_dir of the current element
     // FP32 LSRK register of the element, staged during the volume term (FP64 reads it at
     // the end instead: the larger shared footprint costs more than the exposed latency)
-    __align__(16) T dqs[sizeof(T) == 4 ? NS : 1][sizeof(T) == 4 ? NP : 1];
-    T rs[3][NQ];                                // sum_a S[dir][a][id]
+    __align__(16) T dqs[sizeof(T) == 4 ? NS : 1][sizeof(T) == 4 ? G::NP : 1];
+    T rs[3][Q];                                 // sum_a S[dir][a][id]
     double geo[2][4];                           // elem_geo of the current / next element
     int32_t nb[2][8];                           // neighbours of the current / next element
     ElemRef ref[2];                             // the current / next element
@@ -189,21 +198,22 @@ __device__ __forceinline__ bool bounded_wait(uint64_t* bar, uint32_t parity) {
     return true;
 }
 
-// 0-based volume node of face slot `slot` (faces x-, x+, y-, y+, z-, z+; 64 slots each)
+// 0-based volume node of face slot `slot` (faces x-, x+, y-, y+, z-, z+; Q*Q slots each)
 // and the node of the opposite face with the same in-face index.
+template <int Q = 8>
 __device__ __forceinline__ void slot_nodes(int slot, int& vn, int& opp) {
-    const int f = slot >> 6, jf = slot & 63;
+    const int f = slot / (Q * Q), jf = slot % (Q * Q);
     const int dir = f >> 1, side = f & 1;
-    const int j1 = jf & 7, j2 = jf >> 3, c = side ? NQ - 1 : 0;
+    const int j1 = jf % Q, j2 = jf / Q, c = side ? Q - 1 : 0;
     if (dir == 0) {
-        vn = c + 8 * (j1 + 8 * j2);
-        opp = (NQ - 1 - c) + 8 * (j1 + 8 * j2);
+        vn = c + Q * (j1 + Q * j2);
+        opp = (Q - 1 - c) + Q * (j1 + Q * j2);
     } else if (dir == 1) {
-        vn = j1 + 8 * (c + 8 * j2);
-        opp = j1 + 8 * ((NQ - 1 - c) + 8 * j2);
+        vn = j1 + Q * (c + Q * j2);
+        opp = j1 + Q * ((Q - 1 - c) + Q * j2);
     } else {
-        vn = j1 + 8 * (j2 + 8 * c);
-        opp = j1 + 8 * (j2 + 8 * (NQ - 1 - c));
+        vn = j1 + Q * (j2 + Q * c);
+        opp = j1 + Q * (j2 + Q * (Q - 1 - c));
     }
 }
 
@@ -270,17 +280,20 @@ constexpr int pipe_min_ctas() {
     return sizeof(T) == 4 ? 3 : 2;
 }
 
-// NPT nodes per thread: thread t owns nodes t + (512/NPT)*h, h < NPT, which share i, j
-// (k = k0 + (8/NPT)*h), so their z-partners are loaded once.
-template <int COMBO, typename T, int NPT, bool BATCH>
-__global__ void __launch_bounds__(512 / NPT, pipe_min_ctas<T>())
+// NPT nodes per thread: thread t owns nodes t + (Np/NPT)*h, h < NPT, which share i, j
+// (k = k0 + (Nq/NPT)*h), so their z-partners are loaded once.
+template <int COMBO, typename T, int NPT, bool BATCH, int Q = 8>
+__global__ void __launch_bounds__(Q * Q * Q / NPT, pipe_min_ctas<T>())
     pipelined_stage_kernel(const __grid_constant__ PipeArgs A, const __grid_constant__ PipeBatch B) {
     using namespace pipe;
-    constexpr int NT = 512 / NPT, KS = 8 / NPT;
+    using G = Geo<Q>;
+    constexpr int NQ = Q, NP = G::NP, NFP = G::NFP, NSLOT = G::NSLOT;
+    static_assert(Q % NPT == 0, "a thread's nodes share (i, j)");
+    constexpr int NT = NP / NPT, KS = Q / NPT;
     extern __shared__ __align__(128) unsigned char pipe_smem_raw[];
-    Smem<T>& sm = *reinterpret_cast<Smem<T>*>(pipe_smem_raw);
+    Smem<T, Q>& sm = *reinterpret_cast<Smem<T, Q>*>(pipe_smem_raw);
     const int t = threadIdx.x;
-    const int ii = t & 7, jj = (t >> 3) & 7, k0 = t >> 6;
+    const int ii = t % Q, jj = (t / Q) % Q, k0 = t / (Q * Q);
     const bool stage = A.mode >= MODE_STAGE;
     const bool dq_is_f32 = stage && sizeof(T) == 4;
     constexpr bool kStageDq = sizeof(T) == 4;
@@ -313,18 +326,20 @@ __global__ void __launch_bounds__(512 / NPT, pipe_min_ctas<T>())
         const int64_t e = BATCH ? sm.ref[buf].e : (es < A.E ? es : -1);
         if (e < 0) break;
         const double drdx[3] = {sm.geo[buf][0], sm.geo[buf][1], sm.geo[buf][2]};
-        for (int q = t; q < 192; q += NT) {
-            const int dir = q >> 6, a = (q >> 3) & 7, id = q & 7;
+        for (int q = t; q < 3 * Q * Q; q += NT) {
+            const int dir = q / (Q * Q), a = (q / Q) % Q, id = q % Q;
             const double dd = dir == 0 ? drdx[0] : (dir == 1 ? drdx[1] : drdx[2]);
-            sm.S[dir][a][id] = (T)(A.S[a * 8 + id] * dd);
+            sm.S[dir][a][id] = (T)(A.S[a * Q + id] * dd);
         }
-        if (COMBO == EUL_KG && t < 24) {
-            const int dir = t >> 3, id = t & 7;
-            const double dd = dir == 0 ? drdx[0] : (dir == 1 ? drdx[1] : drdx[2]);
-            T r = T(0);
+        if constexpr (COMBO == EUL_KG) {
+            for (int q = t; q < 3 * Q; q += NT) {
+                const int dir = q / Q, id = q % Q;
+                const double dd = dir == 0 ? drdx[0] : (dir == 1 ? drdx[1] : drdx[2]);
+                T r = T(0);
 #pragma unroll
-            for (int a = 0; a < NQ; ++a) r += (T)(A.S[a * 8 + id] * dd);
-            sm.rs[dir][id] = r;
+                for (int a = 0; a < NQ; ++a) r += (T)(A.S[a * Q + id] * dd);
+                sm.rs[dir][id] = r;
+            }
         }
         // ---- this element's state
         if (__syncthreads_or(!bounded_wait(&sm.bar, phase))) {
@@ -384,8 +399,8 @@ __global__ void __launch_bounds__(512 / NPT, pipe_min_ctas<T>())
             const int slot = t + NT * sl;
             if (slot >= NSLOT) continue;
             int vn, opp;
-            slot_nodes(slot, vn, opp);
-            const int ne = sm.nb[buf][slot >> 6];
+            slot_nodes<Q>(slot, vn, opp);
+            const int ne = sm.nb[buf][slot / NFP];
             if (ne >= 0) {
                 const double* qn = qin_e + (size_t)ne * NS * NP + opp;
 #pragma unroll
@@ -455,13 +470,13 @@ __global__ void __launch_bounds__(512 / NPT, pipe_min_ctas<T>())
             for (int h = 0; h < NPT; ++h) {
                 const int kk = k0 + KS * h;
                 T pv[NAUX];
-                load_aux(pv, a + 8 * (jj + 8 * kk));
+                load_aux(pv, a + Q * (jj + Q * kk));
                 pair(acc[h], accu[h], own[h], pv, sx, 0);
-                load_aux(pv, ii + 8 * (a + 8 * kk));
+                load_aux(pv, ii + Q * (a + Q * kk));
                 pair(acc[h], accu[h], own[h], pv, sy, 1);
             }
             T pv[NAUX];
-            load_aux(pv, ii + 8 * (jj + 8 * a));
+            load_aux(pv, ii + Q * (jj + Q * a));
 #pragma unroll
             for (int h = 0; h < NPT; ++h)
                 if (a != k0 + KS * h) pair(acc[h], accu[h], own[h], pv, sm.S[2][a][k0 + KS * h], 2);  // S_aa = 0
@@ -487,9 +502,9 @@ __global__ void __launch_bounds__(512 / NPT, pipe_min_ctas<T>())
         for (int sl = 0; sl < (NSLOT + NT - 1) / NT; ++sl) {
             const int slot = t + NT * sl;
             if (slot >= NSLOT) continue;
-            const int f = slot >> 6, dir = f >> 1, side = f & 1;
+            const int f = slot / NFP, dir = f >> 1, side = f & 1;
             int vn, opp;
-            slot_nodes(slot, vn, opp);
+            slot_nodes<Q>(slot, vn, opp);
             const bool open_face = sm.nb[buf][f] >= 0;
             // q- and its primitives from the staged partner values of the element
             T qm[NS], u0, u1, u2, p, rinv;
@@ -591,12 +606,12 @@ __global__ void __launch_bounds__(512 / NPT, pipe_min_ctas<T>())
         for (int h = 0; h < NPT; ++h) {
             const int kk = k0 + KS * h;
             int slots[3] = {-1, -1, -1};
-            if (ii == 0) slots[0] = jj + 8 * kk;
-            else if (ii == NQ - 1) slots[0] = 64 + jj + 8 * kk;
-            if (jj == 0) slots[1] = 128 + ii + 8 * kk;
-            else if (jj == NQ - 1) slots[1] = 192 + ii + 8 * kk;
-            if (kk == 0) slots[2] = 256 + ii + 8 * jj;
-            else if (kk == NQ - 1) slots[2] = 320 + ii + 8 * jj;
+            if (ii == 0) slots[0] = jj + Q * kk;
+            else if (ii == NQ - 1) slots[0] = NFP + jj + Q * kk;
+            if (jj == 0) slots[1] = 2 * NFP + ii + Q * kk;
+            else if (jj == NQ - 1) slots[1] = 3 * NFP + ii + Q * kk;
+            if (kk == 0) slots[2] = 4 * NFP + ii + Q * jj;
+            else if (kk == NQ - 1) slots[2] = 5 * NFP + ii + Q * jj;
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
                 T v = acc[h][s];

@@ -112,13 +112,13 @@ size_t stage_smem_bytes(int dim, int nq, int combo, int geom, int fp32);
 
 struct PipeArgs;  // pipelined_kernel.cuh
 // Persistent TMA-pipelined kernel for 3-D Nq = 8 affine flux differencing (KG, EC).
-cudaError_t launch_pipelined(int combo, int fp32, const PipeArgs& a, int grid, cudaStream_t s);
-int pipelined_blocks_per_sm(int combo, int fp32);
+cudaError_t launch_pipelined(int nq, int combo, int fp32, const PipeArgs& a, int grid, cudaStream_t s);
+int pipelined_blocks_per_sm(int nq, int combo, int fp32);
 struct PipeBatch;  // pipelined_kernel.cuh
 // The same kernel over the chunks of a serving class (Euler KG only).
-cudaError_t launch_pipelined_batch(int combo, int fp32, const PipeArgs& a, const PipeBatch& b, int grid,
+cudaError_t launch_pipelined_batch(int nq, int combo, int fp32, const PipeArgs& a, const PipeBatch& b, int grid,
                                    cudaStream_t s);
-int pipelined_batch_blocks_per_sm(int combo, int fp32);
+int pipelined_batch_blocks_per_sm(int nq, int combo, int fp32);
 struct PipeCurvedArgs;  // pipelined_curved.cuh
 // Persistent pipelined kernel for 3-D Nq = 8 curved grids (FP32 bulk, Kennedy-Gruber, stage modes).
 cudaError_t launch_pipelined_curved(const PipeCurvedArgs& a, int grid, cudaStream_t s);

@@ -318,16 +318,17 @@ cudaError_t make_class(rb200_server* s, Class& c, const Req& r) {
         // one configuration (the persistent TMA-pipelined kernel): nothing to tune
         c.ntiles = 1;
         c.tile = 0;
-        const int bps = pipelined_batch_blocks_per_sm(c.combo, c.prec);
+        const int bps = pipelined_batch_blocks_per_sm(c.nq, c.combo, c.prec);
         if (bps <= 0) return cudaErrorInvalidConfiguration;
         PipeArgs pa{};
         pa.status = c.d_status;
         pa.surface_rusanov = c.base.surface_rusanov;
         pa.gamma = c.base.gamma;
-        for (int a = 0; a < 8; ++a)
-            for (int id = 0; id < 8; ++id)
-                pa.S[a * 8 + id] = c.base.D[a + 8 * id] * (c.base.w[a] / c.base.w[id]) - c.base.D[id + 8 * a];
-        for (int i = 0; i < 8; ++i) pa.w[i] = c.base.w[i];
+        const int q = c.nq;
+        for (int a = 0; a < q; ++a)
+            for (int id = 0; id < q; ++id)
+                pa.S[a * q + id] = c.base.D[a + q * id] * (c.base.w[a] / c.base.w[id]) - c.base.D[id + q * a];
+        for (int i = 0; i < q; ++i) pa.w[i] = c.base.w[i];
         cudaGraph_t g = nullptr;
         e = cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return e;
@@ -335,7 +336,7 @@ cudaError_t make_class(rb200_server* s, Class& c, const Req& r) {
             pa.mode = kRKA[st] == 0.0 ? MODE_STAGE_FIRST : MODE_STAGE;
             pa.rka = kRKA[st];
             const PipeBatch b{c.d_solves, c.d_chunks, c.d_nchunks, c.d_tick, st, kRKB[st]};
-            e = launch_pipelined_batch(c.combo, c.prec, pa, b, bps * nsm, c.stream);
+            e = launch_pipelined_batch(c.nq, c.combo, c.prec, pa, b, bps * nsm, c.stream);
         }
         if (e == cudaSuccess) {
             advance_tick_kernel<<<1, 1, 0, c.stream>>>(c.d_tick);

@@ -1,4 +1,4 @@
-"""The persistent TMA-pipelined kernel (3-D, Nq = 8, unwarped brick, Kennedy-Gruber /
+"""The persistent TMA-pipelined kernel (3-D, Nq = 4, 6 and 8, unwarped brick, Kennedy-Gruber /
 entropy-conservative flux differencing) against the oracle and against the generic
 stage kernel.  The grids have more elements than the kernel has CTAs, so every CTA
 walks several elements through both halves of its shared-memory double buffer.
@@ -20,21 +20,26 @@ pytestmark = pytest.mark.gpu
 SCHEMES = ["eul_kg", "eul_ec"]
 
 
-def _build(rb, scheme, K=(8, 8, 7), per=(1, 1, 0), precision="fp64"):
-    og = O.Grid(3, 8, K, [0.0] * 3, [10.0] * 3, per)
+# Nq and a grid with more elements than the kernel has CTAs at that Nq
+NQS = [(8, (8, 8, 7)), (6, (12, 12, 10)), (4, (20, 20, 16))]
+
+
+def _build(rb, scheme, K=(8, 8, 7), per=(1, 1, 0), precision="fp64", nq=8):
+    og = O.Grid(3, nq, K, [0.0] * 3, [10.0] * 3, per)
     g = wrap_oracle_grid(og)
     law, form = product_scheme(rb, scheme, 3)
     dg = rb.DGSEM(law=law, grid=g, volume_form=form, surface_numericalflux=rb.RusanovFlux(), precision=precision)
     return og, dg, oracle_law(scheme, 3), law
 
 
+@pytest.mark.parametrize("nqk", NQS, ids=lambda c: f"nq{c[0]}")
 @pytest.mark.parametrize("scheme", SCHEMES)
 @pytest.mark.parametrize("increment", [False, True])
-def test_pipelined_tendency_fp64(rb, cuda_ok, scheme, increment):
-    og, dg, olaw, law = _build(rb, scheme)
+def test_pipelined_tendency_fp64(rb, cuda_ok, scheme, increment, nqk):
+    og, dg, olaw, law = _build(rb, scheme, K=nqk[1], nq=nqk[0])
     assert dg.pipelined_ctas > 0 and og.E > dg.pipelined_ctas
-    q = initial_state(og, olaw, scheme, seed=11)
-    dq0 = initial_state(og, olaw, scheme, seed=12) if increment else og.state(olaw)
+    q = initial_state(og, olaw, scheme, seed=11, amp=0.01)
+    dq0 = initial_state(og, olaw, scheme, seed=12, amp=0.01) if increment else og.state(olaw)
     ref = og.tendency(olaw, q, dq=np.asfortranarray(dq0.copy()), increment=increment)
     qg, dqg = rb.GridArray.from_numpy(q), rb.GridArray.from_numpy(dq0)
     dg(dqg, qg, 0.0, increment=increment)
@@ -44,9 +49,10 @@ def test_pipelined_tendency_fp64(rb, cuda_ok, scheme, increment):
         assert rel_err(got[:, s], ref[:, s]) <= 1e-12
 
 
+@pytest.mark.parametrize("nqk", NQS, ids=lambda c: f"nq{c[0]}")
 @pytest.mark.parametrize("scheme", SCHEMES)
-def test_pipelined_steps_fp64_and_paths_agree(rb, cuda_ok, scheme):
-    og, dg, olaw, law = _build(rb, scheme)
+def test_pipelined_steps_fp64_and_paths_agree(rb, cuda_ok, scheme, nqk):
+    og, dg, olaw, law = _build(rb, scheme, K=nqk[1], nq=nqk[0])
     q = initial_state(og, olaw, scheme, seed=13, amp=0.01)
     qo, dqo = q.copy(order="F"), og.state(olaw)
     for i in range(2):
@@ -63,9 +69,10 @@ def test_pipelined_steps_fp64_and_paths_agree(rb, cuda_ok, scheme):
     assert rel_err(qa.numpy(), qb.numpy()) <= 1e-13
 
 
+@pytest.mark.parametrize("nqk", NQS, ids=lambda c: f"nq{c[0]}")
 @pytest.mark.parametrize("scheme", SCHEMES)
-def test_pipelined_fp32_bulk_steps(rb, cuda_ok, scheme):
-    og, dg, olaw, law = _build(rb, scheme, precision="fp32_bulk")
+def test_pipelined_fp32_bulk_steps(rb, cuda_ok, scheme, nqk):
+    og, dg, olaw, law = _build(rb, scheme, precision="fp32_bulk", K=nqk[1], nq=nqk[0])
     q = initial_state(og, olaw, scheme, seed=14, amp=0.01)
     qo, dqo = q.copy(order="F"), og.state(olaw)
     for i in range(2):
