@@ -273,17 +273,25 @@ __device__ __forceinline__ void fetch_part(const ElemRef& r, int t, double (&geo
 
 }  // namespace pipe
 
-// CTAs per SM the register allocation is sized for: 2 for FP64 (128 registers a
-// thread), 3 for FP32 bulk (80 registers a thread)
-template <typename T>
+// CTAs per SM the register allocation is sized for.  Nq = 8: 2 for FP64 (128 registers a
+// thread), 3 for FP32 bulk (80).  Smaller elements have fewer threads a CTA, so more CTAs
+// share an SM at about the same registers a thread.
+#ifndef RB200_PIPE_MIN6
+#define RB200_PIPE_MIN6 4, 6
+#endif
+#ifndef RB200_PIPE_MIN4
+#define RB200_PIPE_MIN4 14, 20
+#endif
+template <typename T, int Q = 8>
 constexpr int pipe_min_ctas() {
-    return sizeof(T) == 4 ? 3 : 2;
+    constexpr int m6[2] = {RB200_PIPE_MIN6}, m4[2] = {RB200_PIPE_MIN4};
+    return Q == 8 ? (sizeof(T) == 4 ? 3 : 2) : Q == 6 ? m6[sizeof(T) == 4] : m4[sizeof(T) == 4];
 }
 
 // NPT nodes per thread: thread t owns nodes t + (Np/NPT)*h, h < NPT, which share i, j
 // (k = k0 + (Nq/NPT)*h), so their z-partners are loaded once.
 template <int COMBO, typename T, int NPT, bool BATCH, int Q = 8>
-__global__ void __launch_bounds__(Q * Q * Q / NPT, pipe_min_ctas<T>())
+__global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q>()))
     pipelined_stage_kernel(const __grid_constant__ PipeArgs A, const __grid_constant__ PipeBatch B) {
     using namespace pipe;
     using G = Geo<Q>;
