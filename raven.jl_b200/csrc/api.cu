@@ -158,12 +158,11 @@ bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 // One stage (or tendency) launch: the pipelined kernel when the configuration and the
 // pointers allow it, the generic stage kernel otherwise.
 cudaError_t launch_any(rb200_handle* h, const StageArgs& a, cudaStream_t st) {
-    if (h->nmortars > 0) {  // adapted grid: the mortar fluxes of this q, then the generic kernel
+    if (h->nmortars > 0) {  // adapted grid: the mortar fluxes of this q, then the stage
         MortarArgs m = h->mortar;
         m.q = a.q_in;
         cudaError_t e = launch_mortars(h->dim, h->nq, h->law == RB200_LAW_EULER, h->prec, m, st);
         if (e != cudaSuccess) return e;
-        return launch_stage(h->dim, h->nq, h->combo, h->geom, h->prec, a, st);
     }
     const bool stage_mode = a.mode >= MODE_STAGE;
     if (h->pipe_curved_grid > 0 && h->kernel_path == 0 && stage_mode && aligned16(a.q_in) && aligned16(a.q_out) &&
@@ -197,6 +196,7 @@ cudaError_t launch_any(rb200_handle* h, const StageArgs& a, cudaStream_t st) {
     p.dq = a.dq;
     p.elem_geo = a.elem_geo;
     p.nbr = a.nbr;
+    p.ncflux = h->d_ncflux;
     p.status = h->d_status;
     p.E = a.E;
     p.mode = a.mode;
@@ -972,8 +972,7 @@ rb200_status rb200_set_mortars(rb200_handle* h, const int64_t* mortars, int64_t 
     std::memcpy(a.PL, PL, q2 * sizeof(double));
     std::memcpy(a.PU, PU, q2 * sizeof(double));
     h->nmortars = num_mortars;
-    h->pipe_grid = 0;  // the pipelined kernels have no mortar faces
-    h->pipe_curved_grid = 0;
+    h->pipe_curved_grid = 0;  // the curved kernel has no mortar faces (mortars need affine grids anyway)
     free_graph(h);
     return RB200_OK;
 }

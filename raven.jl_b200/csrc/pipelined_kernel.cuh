@@ -38,7 +38,8 @@ struct PipeArgs {
     double* q_out;
     void* dq;
     const double* elem_geo;  // (4, E)
-    const int32_t* nbr;      // (6, E)
+    const int32_t* nbr;      // (6, E); -2 marks a mortar face of an adapted grid
+    const double* ncflux;    // mortar face fluxes ((6, E) faces x (Ns, Nfp)), or null
     int32_t* status;         // device status word (0 = ok)
     int64_t E;
     int32_t mode;
@@ -513,7 +514,15 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q>()))
             const int f = slot / NFP, dir = f >> 1, side = f & 1;
             int vn, opp;
             slot_nodes<Q>(slot, vn, opp);
-            const bool open_face = sm.nb[buf][f] >= 0;
+            const int nbf = sm.nb[buf][f];
+            const bool open_face = nbf >= 0;
+            if (nbf == -2) {  // mortar face: its flux comes from the mortar kernel
+                const T fsc = (T)(fabs(dir == 0 ? drdx[0] : (dir == 1 ? drdx[1] : drdx[2])) / A.w[0]);
+                const double* nfp = A.ncflux + (((size_t)e * 6 + f) * NS) * NFP + (slot - f * NFP);
+#pragma unroll
+                for (int s = 0; s < NS; ++s) sm.slot[s][slot] = (double)((T)nfp[s * NFP] * fsc);
+                continue;
+            }
             // q- and its primitives from the staged partner values of the element
             T qm[NS], u0, u1, u2, p, rinv;
             {
