@@ -82,6 +82,7 @@ __global__ void __launch_bounds__(Shape<DIM, NQ, EPBX>::THREADS,
     };
     int ci = live(blockIdx.x), g = 0, b = 0;
     prefetch(ci, 0, 0);
+    bool tables_ready = false;
     while (ci < nch) {
         int ci2 = ci, g2 = g + S::EPB;  // the CTA's next group
         if (g2 >= B.chunks[ci].count) {
@@ -100,7 +101,9 @@ __global__ void __launch_bounds__(Shape<DIM, NQ, EPBX>::THREADS,
             pf.dq = pf_dq ? static_cast<const void*>(dqs + b * NS * TH + tid) : nullptr;
             pf.stride = TH;
         }
+        pf.tables_ready = tables_ready;
         stage_element<DIM, NQ, COMBO, GEOM, T, EPBX>(B.base, P, e, active, smem_raw, pf);
+        tables_ready = true;
         __syncthreads();  // the shared partner values are reused by the next group
         ci = ci2;
         g = g2;

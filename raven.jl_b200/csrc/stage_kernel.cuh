@@ -87,10 +87,13 @@ __device__ __forceinline__ void cpa_wait_all() { asm volatile("cp.async.wait_gro
 
 // A thread's own state and LSRK register, already copied into shared memory by the
 // thread itself (field s at q[s * stride]); null pointers: read them from global memory.
+// tables_ready: the element-independent shared tables (D, or W of the brick advection
+// stage) already hold this CTA's values from an earlier group.
 struct Prefetched {
     const double* q = nullptr;
     const void* dq = nullptr;
     int stride = 0;
+    bool tables_ready = false;
 };
 
 __device__ __forceinline__ double dev_log(double x) { return log(x); }
@@ -163,10 +166,11 @@ __device__ __forceinline__ void stage_element_adv_brick(const StageArgs& A, cons
         for (int d = 0; d < DIM; ++d) drdx[d] = __ldg(eg + d);
         sq[el * NP + n] = q0;
     }
-    for (int i = tid; i < NQ * NQ; i += S::THREADS) {
-        const int a = i % NQ, ii = i / NQ;
-        sW[i] = (T)(A.D[a + NQ * ii] * (A.w[a] / A.w[ii]));
-    }
+    if (!pf.tables_ready)
+        for (int i = tid; i < NQ * NQ; i += S::THREADS) {
+            const int a = i % NQ, ii = i / NQ;
+            sW[i] = (T)(A.D[a + NQ * ii] * (A.w[a] / A.w[ii]));
+        }
     __syncthreads();
     if (!active) return;
 
@@ -384,7 +388,8 @@ __device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs
 #pragma unroll
         for (int k = 0; k < NAUX; ++k) aux[k * NP + n] = own[k];
     }
-    for (int i = tid; i < NQ * NQ; i += S::THREADS) sD[i] = (T)A.D[i];
+    if (!pf.tables_ready)
+        for (int i = tid; i < NQ * NQ; i += S::THREADS) sD[i] = (T)A.D[i];
     __syncthreads();
     if (!active) return;
 
@@ -705,6 +710,7 @@ __global__ void __launch_bounds__(Shape<DIM, NQ>::THREADS, (PersistentCfg<DIM, N
         pf.q = qs + b * NS * TH + tid;
         pf.dq = pf_dq ? static_cast<const void*>(dqs + b * NS * TH + tid) : nullptr;
         pf.stride = TH;
+        pf.tables_ready = g != blockIdx.x;
         stage_element<DIM, NQ, COMBO, GEOM, T, 0, SF>(A, P, e, e < A.E, smem_raw, pf);
         __syncthreads();  // the shared partner values are reused by the next group
     }
