@@ -266,6 +266,8 @@ def kernel_name(w, dg):
         if dg.geometry == "curved":
             return "pipelined_curved_kernel (3-D Nq=8 curved, FP32 bulk, fused volume + surface + LSRK stage)"
         extra = " with mortar fluxes" if w.get("adapted") else ""
+        if w.get("law") == "advection":
+            return f"pipelined_adv_kernel (3-D Nq={w['N'] + 1} brick{extra}, weak-form advection, fused stage)"
         return f"pipelined_stage_kernel (3-D Nq={w['N'] + 1} brick{extra}, fused volume + surface + LSRK stage)"
     return "stage_kernel (fused volume + surface + LSRK stage)"
 

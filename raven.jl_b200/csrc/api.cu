@@ -58,7 +58,7 @@ struct rb200_handle {
     int use_graphs = 1;
     int pipe_grid = 0;            // CTAs of the pipelined kernel (0: not eligible)
     int pipe_curved_grid = 0;     // CTAs of the curved-grid pipelined kernel (0: not eligible)
-    double pipe_S[64] = {0};      // D[a,id] w[a] / w[id] - D[id,a]
+    double pipe_S[64] = {0};      // D[a,id] w[a] / w[id] - D[id,a] (advection: D[a,id] w[a] / w[id])
     // mortars of an adapted grid (rb200_set_mortars)
     int64_t nmortars = 0;
     int64_t* d_mortars = nullptr;
@@ -206,6 +206,7 @@ cudaError_t launch_any(rb200_handle* h, const StageArgs& a, cudaStream_t st) {
     p.gamma = a.gamma;
     std::memcpy(p.S, h->pipe_S, sizeof(p.S));
     std::memcpy(p.w, h->w, sizeof(p.w));
+    std::memcpy(p.adv, a.adv, sizeof(p.adv));
     const int grid = (int)std::min<int64_t>(h->pipe_grid, a.E);
     return launch_pipelined(h->nq, h->combo, h->prec, p, grid, st);
 }
@@ -619,11 +620,15 @@ rb200_status rb200_create(const rb200_desc* d, rb200_handle** out) {
     if ((st = dev_alloc(h, &h->d_status, 1)) != RB200_OK) return bail(st);
     ce = cudaMemset(h->d_status, 0, sizeof(int32_t));
     if (ce != cudaSuccess) return bail(cuda_fail(h, ce, "memset"));
-    if (dim == 3 && (nq == 4 || nq == 6 || nq == 8) && affine && (h->combo == EUL_KG || h->combo == EUL_EC) &&
-        !entropy_flux) {
+    if (dim == 3 && (nq == 4 || nq == 6 || nq == 8) && affine &&
+        (h->combo == EUL_KG || h->combo == EUL_EC || h->combo == ADV_WEAK) && !entropy_flux) {
+        // flux differencing: S[a, id] = D[a,id] w[a] / w[id] - D[id,a]; weak-form
+        // advection: W[a, id] = D[a,id] w[a] / w[id]
         for (int a = 0; a < nq; ++a)
             for (int id = 0; id < nq; ++id)
-                h->pipe_S[a * nq + id] = h->D[a + nq * id] * (h->w[a] / h->w[id]) - h->D[id + nq * a];
+                h->pipe_S[a * nq + id] = h->combo == ADV_WEAK
+                                             ? h->D[a + nq * id] * (h->w[a] / h->w[id])
+                                             : h->D[a + nq * id] * (h->w[a] / h->w[id]) - h->D[id + nq * a];
         int dev = 0, nsm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);

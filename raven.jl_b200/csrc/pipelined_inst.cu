@@ -1,5 +1,7 @@
-// Instantiations and launch helpers of the pipelined 3-D Nq = 8 stage kernel: one state
-// (the DGSEM handle) or the chunks of a serving class (BATCH).
+// Instantiations and launch helpers of the pipelined 3-D stage kernels (Euler flux
+// differencing and weak-form advection, Nq = 4, 6, 8): one state (the DGSEM handle) or
+// the chunks of a serving class (BATCH).
+#include "pipelined_adv.cuh"
 #include "pipelined_curved.cuh"
 #include "pipelined_kernel.cuh"
 
@@ -20,8 +22,27 @@ static cudaError_t launch_p(const PipeArgs& a, const PipeBatch& b, int grid, cud
     return cudaGetLastError();
 }
 
+// The advection law: one field, two nodes a thread.
+template <typename T, bool BATCH, int Q>
+static cudaError_t launch_a(const PipeArgs& a, const PipeBatch& b, int grid, cudaStream_t s) {
+    auto kern = pipelined_adv_kernel<T, BATCH, Q>;
+    static std::atomic<uint64_t> configured{0};
+    cudaError_t err = ensure_smem_limit(kern, (int)sizeof(pipea::Smem<T, Q>), configured);
+    if (err != cudaSuccess) return err;
+    kern<<<grid, Q * Q * Q / 2, sizeof(pipea::Smem<T, Q>), s>>>(a, b);
+    return cudaGetLastError();
+}
+
 template <int COMBO, typename T, bool BATCH>
 static cudaError_t launch_q(int nq, const PipeArgs& a, const PipeBatch& b, int grid, cudaStream_t s) {
+    if constexpr (COMBO == ADV_WEAK) {
+        switch (nq) {
+            case 4: return launch_a<T, BATCH, 4>(a, b, grid, s);
+            case 6: return launch_a<T, BATCH, 6>(a, b, grid, s);
+            case 8: return launch_a<T, BATCH, 8>(a, b, grid, s);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     switch (nq) {
         case 4: return launch_p<COMBO, T, BATCH, 4>(a, b, grid, s);
         case 6: return launch_p<COMBO, T, BATCH, 6>(a, b, grid, s);
@@ -38,6 +59,9 @@ cudaError_t launch_pipelined(int nq, int combo, int fp32, const PipeArgs& a, int
     if (combo == EUL_EC)
         return fp32 ? launch_q<EUL_EC, float, false>(nq, a, none, grid, s)
                     : launch_q<EUL_EC, double, false>(nq, a, none, grid, s);
+    if (combo == ADV_WEAK)
+        return fp32 ? launch_q<ADV_WEAK, float, false>(nq, a, none, grid, s)
+                    : launch_q<ADV_WEAK, double, false>(nq, a, none, grid, s);
     return cudaErrorInvalidValue;
 }
 
@@ -45,6 +69,9 @@ cudaError_t launch_pipelined_batch(int nq, int combo, int fp32, const PipeArgs& 
                                    cudaStream_t s) {
     if (combo == EUL_KG)
         return fp32 ? launch_q<EUL_KG, float, true>(nq, a, b, grid, s) : launch_q<EUL_KG, double, true>(nq, a, b, grid, s);
+    if (combo == ADV_WEAK)
+        return fp32 ? launch_q<ADV_WEAK, float, true>(nq, a, b, grid, s)
+                    : launch_q<ADV_WEAK, double, true>(nq, a, b, grid, s);
     return cudaErrorInvalidValue;
 }
 
@@ -61,8 +88,29 @@ static int occupancy_p() {
     return n;
 }
 
+template <typename T, bool BATCH, int Q>
+static int occupancy_a() {
+    auto kern = pipelined_adv_kernel<T, BATCH, Q>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(pipea::Smem<T, Q>)) !=
+        cudaSuccess)
+        return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, Q * Q * Q / 2, sizeof(pipea::Smem<T, Q>)) !=
+        cudaSuccess)
+        return 0;
+    return n;
+}
+
 template <int COMBO, typename T, bool BATCH>
 static int occupancy_q(int nq) {
+    if constexpr (COMBO == ADV_WEAK) {
+        switch (nq) {
+            case 4: return occupancy_a<T, BATCH, 4>();
+            case 6: return occupancy_a<T, BATCH, 6>();
+            case 8: return occupancy_a<T, BATCH, 8>();
+            default: return 0;
+        }
+    }
     switch (nq) {
         case 4: return occupancy_p<COMBO, T, BATCH, 4>();
         case 6: return occupancy_p<COMBO, T, BATCH, 6>();
@@ -74,11 +122,15 @@ static int occupancy_q(int nq) {
 int pipelined_blocks_per_sm(int nq, int combo, int fp32) {
     if (combo == EUL_KG) return fp32 ? occupancy_q<EUL_KG, float, false>(nq) : occupancy_q<EUL_KG, double, false>(nq);
     if (combo == EUL_EC) return fp32 ? occupancy_q<EUL_EC, float, false>(nq) : occupancy_q<EUL_EC, double, false>(nq);
+    if (combo == ADV_WEAK)
+        return fp32 ? occupancy_q<ADV_WEAK, float, false>(nq) : occupancy_q<ADV_WEAK, double, false>(nq);
     return 0;
 }
 
 int pipelined_batch_blocks_per_sm(int nq, int combo, int fp32) {
     if (combo == EUL_KG) return fp32 ? occupancy_q<EUL_KG, float, true>(nq) : occupancy_q<EUL_KG, double, true>(nq);
+    if (combo == ADV_WEAK)
+        return fp32 ? occupancy_q<ADV_WEAK, float, true>(nq) : occupancy_q<ADV_WEAK, double, true>(nq);
     return 0;
 }
 

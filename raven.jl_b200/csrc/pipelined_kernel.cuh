@@ -45,8 +45,9 @@ struct PipeArgs {
     int32_t mode;
     int32_t surface_rusanov;
     double rka, rkb_dt, gamma;
-    double S[64];  // S[a*Nq + id] = D[a,id] * w[a] / w[id] - D[id,a]
+    double S[64];  // S[a*Nq + id] = D[a,id] * w[a] / w[id] - D[id,a] (advection: D[a,id] * w[a] / w[id])
     double w[8];
+    double adv[3];  // advection velocity (advection law only)
 };
 
 // Serving loop: the elements of a launch are the chunks of a class's running solves

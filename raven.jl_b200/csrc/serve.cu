@@ -223,7 +223,7 @@ struct Class {
     // concurrently, so these overlap across classes) and DOF updates
     int64_t ticks_done = 0;
     double busy_ms = 0.0, dof_updates = 0.0;
-    bool pipelined = false;                      // 3-D Nq=4, 6, 8 Euler KG: the pipelined kernel
+    bool pipelined = false;                      // 3-D Nq=4, 6, 8 Euler KG or advection: the pipelined kernel
     int32_t* d_status = nullptr;                 // its bounded waits report here
     int active = 0;
     bool launched = false;
@@ -313,7 +313,7 @@ cudaError_t make_class(rb200_server* s, Class& c, const Req& r) {
     c.chunk_elems = 8 * c.epb[1];
     int nsm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, s->device);
-    c.pipelined = c.dim == 3 && (c.nq == 4 || c.nq == 6 || c.nq == 8) && c.combo == EUL_KG;
+    c.pipelined = c.dim == 3 && (c.nq == 4 || c.nq == 6 || c.nq == 8) && (c.combo == EUL_KG || c.combo == ADV_WEAK);
     if (c.pipelined) {
         // one configuration (the persistent TMA-pipelined kernel): nothing to tune
         c.ntiles = 1;
@@ -327,8 +327,11 @@ cudaError_t make_class(rb200_server* s, Class& c, const Req& r) {
         const int q = c.nq;
         for (int a = 0; a < q; ++a)
             for (int id = 0; id < q; ++id)
-                pa.S[a * q + id] = c.base.D[a + q * id] * (c.base.w[a] / c.base.w[id]) - c.base.D[id + q * a];
+                pa.S[a * q + id] = c.combo == ADV_WEAK
+                                       ? c.base.D[a + q * id] * (c.base.w[a] / c.base.w[id])
+                                       : c.base.D[a + q * id] * (c.base.w[a] / c.base.w[id]) - c.base.D[id + q * a];
         for (int i = 0; i < q; ++i) pa.w[i] = c.base.w[i];
+        for (int d = 0; d < 3; ++d) pa.adv[d] = c.base.adv[d];
         cudaGraph_t g = nullptr;
         e = cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return e;

@@ -1,6 +1,6 @@
-"""The persistent TMA-pipelined kernel (3-D, Nq = 4, 6 and 8, unwarped brick, Kennedy-Gruber /
-entropy-conservative flux differencing) against the oracle and against the generic
-stage kernel.  The grids have more elements than the kernel has CTAs, so every CTA
+"""The persistent TMA-pipelined kernels (3-D, Nq = 4, 6 and 8, unwarped brick: Kennedy-Gruber /
+entropy-conservative flux differencing, and weak-form advection) against the oracle and
+against the generic stage kernel.  The grids have more elements than the kernel has CTAs, so every CTA
 walks several elements through both halves of its shared-memory double buffer.
 
 Tolerances: FP64 1e-12 relative (max norm per field); FP32 bulk 5e-5 for a tendency
@@ -88,6 +88,65 @@ def test_pipelined_fp32_bulk_steps(rb, cuda_ok, scheme, nqk):
     dg(dqg, rb.GridArray.from_numpy(q), 0.0, increment=False)
     for s in range(law.ns):
         assert rel_err(dqg.numpy()[:, s], ref[:, s]) <= 5e-5
+
+
+ADV = [1.0, 0.5, -0.25]
+# the advection kernel runs more CTAs per SM, so its grids are larger
+ADV_NQS = [(8, (10, 10, 8)), (6, (12, 12, 10)), (4, (20, 20, 16))]
+
+
+def _build_adv(rb, nq, K, per=(1, 1, 0), precision="fp64", surface="rusanov"):
+    og = O.Grid(3, nq, K, [0.0] * 3, [1.0] * 3, per)
+    g = wrap_oracle_grid(og)
+    law, form = product_scheme(rb, "adv_weak", 3, adv=ADV)
+    sflux = rb.RusanovFlux() if surface == "rusanov" else rb.CentralFlux()
+    dg = rb.DGSEM(law=law, grid=g, volume_form=form, surface_numericalflux=sflux, precision=precision)
+    olaw = O.Law(O.LAW_ADVECTION, 3, form=O.FORM_WEAK, volume_flux=O.FLUX_CENTRAL, adv=ADV,
+                 surface_flux=O.FLUX_RUSANOV if surface == "rusanov" else O.FLUX_CENTRAL)
+    return og, dg, olaw
+
+
+@pytest.mark.parametrize("nqk", ADV_NQS, ids=lambda c: f"nq{c[0]}")
+@pytest.mark.parametrize("surface", ["rusanov", "central"])
+@pytest.mark.parametrize("increment", [False, True])
+def test_pipelined_advection_tendency_fp64(rb, cuda_ok, surface, increment, nqk):
+    """The pipelined weak-form advection kernel (one field) against the oracle, with open
+    faces along z (default boundary state), 1e-12 relative."""
+    og, dg, olaw = _build_adv(rb, nqk[0], nqk[1], surface=surface)
+    assert dg.pipelined_ctas > 0 and og.E > dg.pipelined_ctas
+    q = initial_state(og, olaw, "adv_weak", seed=21)
+    dq0 = initial_state(og, olaw, "adv_weak", seed=22) if increment else og.state(olaw)
+    ref = og.tendency(olaw, q, dq=np.asfortranarray(dq0.copy()), increment=increment)
+    qg, dqg = rb.GridArray.from_numpy(q), rb.GridArray.from_numpy(dq0)
+    dg(dqg, qg, 0.0, increment=increment)
+    dg.sync_status()
+    assert rel_err(dqg.numpy(), ref) <= 1e-12
+
+
+@pytest.mark.parametrize("nqk", ADV_NQS, ids=lambda c: f"nq{c[0]}")
+def test_pipelined_advection_steps(rb, cuda_ok, nqk):
+    """Three LSRK steps against the oracle (FP64 1e-12; FP32 bulk 1e-6) and the FP64 run
+    against the generic kernel (1e-13)."""
+    og, dg, olaw = _build_adv(rb, nqk[0], nqk[1])
+    q = initial_state(og, olaw, "adv_weak", seed=23)
+    qo, dqo = q.copy(order="F"), og.state(olaw)
+    for i in range(3):
+        og.lsrk54_step(olaw, qo, dqo, i * 1e-3, 1e-3)
+    qa = rb.GridArray.from_numpy(q)
+    rb.LSRK54(dg, qa, 1e-3).dostep(qa, 3)
+    dg.sync_status()
+    assert rel_err(qa.numpy(), qo) <= 1e-12
+    dg.set_kernel_path("generic")
+    qb = rb.GridArray.from_numpy(q)
+    rb.LSRK54(dg, qb, 1e-3).dostep(qb, 3)
+    dg.set_kernel_path("auto")
+    assert rel_err(qa.numpy(), qb.numpy()) <= 1e-13
+    og32, dg32, _ = _build_adv(rb, nqk[0], nqk[1], precision="fp32_bulk")
+    assert dg32.pipelined_ctas > 0 and og.E > dg32.pipelined_ctas
+    qc = rb.GridArray.from_numpy(q)
+    rb.LSRK54(dg32, qc, 1e-3).dostep(qc, 3)
+    dg32.sync_status()
+    assert rel_err(qc.numpy(), qo) <= 1e-6
 
 
 def test_misaligned_state_falls_back_to_generic_kernel(rb, cuda_ok):

@@ -66,7 +66,7 @@ def _dgsem_same_kernel(rb, spec, q0):
         law, form = rb.AdvectionLaw(spec.dim, spec.advection_velocity[: spec.dim]), rb.WeakForm()
     dg = rb.DGSEM(law=law, grid=grid, volume_form=form, surface_numericalflux=rb.RusanovFlux(),
                   precision="fp64" if spec.precision == 0 else "fp32_bulk")
-    pipelined = spec.dim == 3 and spec.nq in (4, 6, 8) and spec.law == rb._lib.LAW_EULER
+    pipelined = spec.dim == 3 and spec.nq in (4, 6, 8)  # Euler KG and advection classes
     dg.set_kernel_path("auto" if pipelined else "generic")
     if pipelined:
         assert dg.pipelined_ctas > 0
@@ -88,6 +88,8 @@ PARITY = [
     (3, 8, 1, (3, 3, 3), 3, 0),
     (3, 8, 1, (2, 3, 2), 3, 1),
     (3, 4, 0, (4, 4, 4), 6, 0),
+    (3, 8, 0, (3, 4, 3), 5, 0),
+    (3, 8, 0, (4, 3, 3), 4, 1),
 ]
 
 
