@@ -205,6 +205,7 @@ cudaError_t launch_any(rb200_handle* h, const StageArgs& a, cudaStream_t st) {
     p.rkb_dt = a.rkb_dt;
     p.gamma = a.gamma;
     std::memcpy(p.S, h->pipe_S, sizeof(p.S));
+    for (int i = 0; i < 64; ++i) p.Sf[i] = (float)h->pipe_S[i];
     std::memcpy(p.w, h->w, sizeof(p.w));
     std::memcpy(p.adv, a.adv, sizeof(p.adv));
     const int grid = (int)std::min<int64_t>(h->pipe_grid, a.E);

@@ -14,9 +14,12 @@
 // element's state and LSRK register (two 1-D bulk copies) and its geometry and neighbour
 // ids (cp.async by threads 0..9), all completing on the stage's mbarrier; the copies of
 // element k + NST - 1 are issued while element k runs.  The neighbour traces of element
-// k + 1 are fetched (cp.async) during element k.  A thread owns nodes t and t + Np/2
-// (same i, j), whose z partners are loaded once.  Every mbarrier wait is bounded: after
-// kWaitLimit polls the CTA records RB200 status TIMEOUT and returns.
+// k + 1 are fetched (cp.async) during element k.
+//
+// A thread owns NPT nodes of one z-line (same i, j), whose z partners are loaded once.
+// At Nq = 8 it owns the whole line: its x and y weights W[.][i], W[.][j] stay in
+// registers, and the z weights are kernel parameters at fixed indices.  Every mbarrier
+// wait is bounded: after kWaitLimit polls the CTA records RB200 status TIMEOUT and returns.
 #pragma once
 
 #include "pipelined_kernel.cuh"
@@ -25,15 +28,17 @@ namespace rb200 {
 
 namespace pipea {
 
-#ifndef RB200_ADV_STAGES
-#define RB200_ADV_STAGES 4
-#endif
-constexpr int NST = RB200_ADV_STAGES;  // ring stages: NST - 1 elements in flight ahead
-static_assert(NST >= 3, "the stage refilled at element k must differ from those of k and k + 1");
+// nodes a thread owns, and ring stages (NST - 1 elements in flight ahead)
+template <int Q>
+constexpr int npt() { return Q == 8 ? 8 : 2; }
+template <int Q>
+constexpr int nst() { return Q == 8 ? 3 : 4; }
 
 template <typename T, int Q>
 struct Smem {
     using G = pipe::Geo<Q>;
+    static constexpr int NST = nst<Q>();
+    static_assert(NST >= 3, "the stage refilled at element k must differ from those of k and k + 1");
     __align__(16) double q[NST][G::NP];  // element state (bulk copy)
     __align__(16) T dq[NST][G::NP];      // element LSRK register (bulk copy)
     T qa[G::NPP];                        // the state in T, padded, for the partners
@@ -59,26 +64,34 @@ __device__ __forceinline__ void cp_async_wait_group() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// Entry i of the weight table as a kernel parameter in type T.
+template <typename T>
+__device__ __forceinline__ T wpar(const PipeArgs& A, int i) {
+    if constexpr (sizeof(T) == 8) return A.S[i];
+    else return A.Sf[i];
+}
+
 }  // namespace pipea
 
 // CTAs per SM the registers are sized for (one field: few registers a thread)
 template <typename T, int Q>
 constexpr int pipe_adv_min_ctas() {
-    return Q == 8 ? 4 : (Q == 6 ? 7 : 32);
+    return Q == 8 ? (sizeof(T) == 4 ? 8 : 6) : (Q == 6 ? 7 : 32);
 }
 
 template <typename T, bool BATCH, int Q>
-__global__ void __launch_bounds__(Q * Q * Q / 2, (pipe_adv_min_ctas<T, Q>()))
+__global__ void __launch_bounds__(Q * Q * Q / pipea::npt<Q>(), (pipe_adv_min_ctas<T, Q>()))
     pipelined_adv_kernel(const __grid_constant__ PipeArgs A, const __grid_constant__ PipeBatch B) {
     using namespace pipe;
-    using pipea::NST;
     using G = Geo<Q>;
-    constexpr int NP = G::NP, NFP = G::NFP, NSLOT = G::NSLOT, NT = NP / 2, KS = Q / 2;
+    constexpr int NPT = pipea::npt<Q>(), NST = pipea::nst<Q>();
+    constexpr int NP = G::NP, NFP = G::NFP, NSLOT = G::NSLOT, NT = NP / NPT, KS = Q / NPT;
     constexpr int NSL = (NSLOT + NT - 1) / NT;  // face slots a thread owns
+    constexpr bool LINE = NPT == Q;             // the thread owns its whole z-line
     extern __shared__ __align__(128) unsigned char pipe_smem_raw[];
     pipea::Smem<T, Q>& sm = *reinterpret_cast<pipea::Smem<T, Q>*>(pipe_smem_raw);
     const int t = threadIdx.x;
-    const int ii = t % Q, jj = (t / Q) % Q, k0 = t / (Q * Q);
+    const int ii = t % Q, jj = (t / Q) % Q, k0 = LINE ? 0 : t / (Q * Q);
     const bool stage = A.mode >= MODE_STAGE;
     const bool dq_is_f32 = stage && sizeof(T) == 4;
     // the register arrives by bulk copy whenever the stage reads it in type T
@@ -147,7 +160,15 @@ __global__ void __launch_bounds__(Q * Q * Q / 2, (pipe_adv_min_ctas<T, Q>()))
         }
     }
     cp_async_commit();
-    __syncthreads();  // the stage references are visible
+    __syncthreads();  // the stage references and the weight table are visible
+    T wx[LINE ? Q : 1], wy[LINE ? Q : 1];
+    if constexpr (LINE) {
+#pragma unroll
+        for (int a = 0; a < Q; ++a) {
+            wx[a] = sm.W[a][ii];
+            wy[a] = sm.W[a][jj];
+        }
+    }
     if (sm.ref[0].e >= 0) {
         if (__syncthreads_or(!bounded_wait(&sm.bar[0], 0))) {
             if (t == 0) atomicExch(A.status, kStatusTimeout);
@@ -167,12 +188,10 @@ __global__ void __launch_bounds__(Q * Q * Q / 2, (pipe_adv_min_ctas<T, Q>()))
             sm.fc[b][t] = (T)(fabs(dd) / A.w[0]);
             sm.fc[b][3 + t] = (T)dd * (T)A.adv[t];
         }
-        double qd[2];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < NPT; ++h) {
             const int n = t + NT * h;
-            qd[h] = sm.q[r][n];
-            sm.qa[PAD(n)] = (T)qd[h];
+            sm.qa[PAD(n)] = (T)sm.q[r][n];
         }
         // the next element's stage (issued NST - 2 elements ago): wait, then fetch its traces
         const bool next = sm.ref[r1].e >= 0;
@@ -195,28 +214,50 @@ __global__ void __launch_bounds__(Q * Q * Q / 2, (pipe_adv_min_ctas<T, Q>()))
         cp_async_commit();
 
         // ---- volume term: the derivative sums along x, y, z
-        T sx[2] = {T(0), T(0)}, sy[2] = {T(0), T(0)}, sz[2] = {T(0), T(0)};
-#pragma unroll
-        for (int a = 0; a < Q; ++a) {
-            const T wx = sm.W[a][ii], wy = sm.W[a][jj];
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int kk = k0 + KS * h;
-                sx[h] += wx * sm.qa[PAD(a + Q * (jj + Q * kk))];
-                sy[h] += wy * sm.qa[PAD(ii + Q * (a + Q * kk))];
-            }
-            const T qz = sm.qa[PAD(ii + Q * (jj + Q * a))];
-#pragma unroll
-            for (int h = 0; h < 2; ++h) sz[h] += sm.W[a][k0 + KS * h] * qz;
-        }
         const T cx = sm.fc[b][3], cy = sm.fc[b][4], cz = sm.fc[b][5];
-        T acc[2];
+        T acc[NPT];
+        if constexpr (LINE) {
+            T qz[Q];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            acc[h] = T(0);
-            acc[h] += cx * sx[h];
-            acc[h] += cy * sy[h];
-            acc[h] += cz * sz[h];
+            for (int a = 0; a < Q; ++a) qz[a] = sm.qa[PAD(ii + Q * (jj + Q * a))];
+#pragma unroll
+            for (int h = 0; h < Q; ++h) {
+                T sx = T(0), sy = T(0), sz = T(0);
+#pragma unroll
+                for (int a = 0; a < Q; ++a) {
+                    sx += wx[a] * sm.qa[PAD(a + Q * (jj + Q * h))];
+                    sy += wy[a] * sm.qa[PAD(ii + Q * (a + Q * h))];
+                    sz += pipea::wpar<T>(A, a * Q + h) * qz[a];
+                }
+                acc[h] = T(0);
+                acc[h] += cx * sx;
+                acc[h] += cy * sy;
+                acc[h] += cz * sz;
+            }
+        } else {
+            T sx[NPT], sy[NPT], sz[NPT];
+#pragma unroll
+            for (int h = 0; h < NPT; ++h) sx[h] = sy[h] = sz[h] = T(0);
+#pragma unroll
+            for (int a = 0; a < Q; ++a) {
+                const T wxa = sm.W[a][ii], wya = sm.W[a][jj];
+#pragma unroll
+                for (int h = 0; h < NPT; ++h) {
+                    const int kk = k0 + KS * h;
+                    sx[h] += wxa * sm.qa[PAD(a + Q * (jj + Q * kk))];
+                    sy[h] += wya * sm.qa[PAD(ii + Q * (a + Q * kk))];
+                }
+                const T qz = sm.qa[PAD(ii + Q * (jj + Q * a))];
+#pragma unroll
+                for (int h = 0; h < NPT; ++h) sz[h] += sm.W[a][k0 + KS * h] * qz;
+            }
+#pragma unroll
+            for (int h = 0; h < NPT; ++h) {
+                acc[h] = T(0);
+                acc[h] += cx * sx[h];
+                acc[h] += cy * sy[h];
+                acc[h] += cz * sz[h];
+            }
         }
 
         // ---- face-slot contributions (wsJ nf) MJI over the slot's trace (this thread's
@@ -248,7 +289,7 @@ __global__ void __launch_bounds__(Q * Q * Q / 2, (pipe_adv_min_ctas<T, Q>()))
         const double rkb_dt = BATCH ? sm.ref[r].rkb_dt : A.rkb_dt;
         const double* fl = sm.tr[b];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < NPT; ++h) {
             const int kk = k0 + KS * h;
             const int n = t + NT * h;
             const size_t g = (size_t)e * NP + n;
@@ -268,7 +309,7 @@ __global__ void __launch_bounds__(Q * Q * Q / 2, (pipe_adv_min_ctas<T, Q>()))
             if (stage) {
                 if (dq_is_f32) reinterpret_cast<float*>(dq_e)[g] = (float)v;
                 else reinterpret_cast<double*>(dq_e)[g] = (double)v;
-                qout_e[g] = qd[h] + rkb_dt * (double)v;
+                qout_e[g] = sm.q[r][n] + rkb_dt * (double)v;  // stage r is refilled at element k + 1
             } else {
                 reinterpret_cast<double*>(dq_e)[g] = (double)v;
             }

@@ -22,14 +22,14 @@ static cudaError_t launch_p(const PipeArgs& a, const PipeBatch& b, int grid, cud
     return cudaGetLastError();
 }
 
-// The advection law: one field, two nodes a thread.
+// The advection law: one field, pipea::npt<Q>() nodes a thread.
 template <typename T, bool BATCH, int Q>
 static cudaError_t launch_a(const PipeArgs& a, const PipeBatch& b, int grid, cudaStream_t s) {
     auto kern = pipelined_adv_kernel<T, BATCH, Q>;
     static std::atomic<uint64_t> configured{0};
     cudaError_t err = ensure_smem_limit(kern, (int)sizeof(pipea::Smem<T, Q>), configured);
     if (err != cudaSuccess) return err;
-    kern<<<grid, Q * Q * Q / 2, sizeof(pipea::Smem<T, Q>), s>>>(a, b);
+    kern<<<grid, Q * Q * Q / pipea::npt<Q>(), sizeof(pipea::Smem<T, Q>), s>>>(a, b);
     return cudaGetLastError();
 }
 
@@ -95,7 +95,7 @@ static int occupancy_a() {
         cudaSuccess)
         return 0;
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, Q * Q * Q / 2, sizeof(pipea::Smem<T, Q>)) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, Q * Q * Q / pipea::npt<Q>(), sizeof(pipea::Smem<T, Q>)) !=
         cudaSuccess)
         return 0;
     return n;

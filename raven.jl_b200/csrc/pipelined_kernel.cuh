@@ -48,6 +48,7 @@ struct PipeArgs {
     double S[64];  // S[a*Nq + id] = D[a,id] * w[a] / w[id] - D[id,a] (advection: D[a,id] * w[a] / w[id])
     double w[8];
     double adv[3];  // advection velocity (advection law only)
+    float Sf[64];   // (float)S, for FP32 arithmetic on table entries at fixed indices
 };
 
 // Serving loop: the elements of a launch are the chunks of a class's running solves

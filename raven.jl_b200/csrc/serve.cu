@@ -332,6 +332,7 @@ cudaError_t make_class(rb200_server* s, Class& c, const Req& r) {
                                        : c.base.D[a + q * id] * (c.base.w[a] / c.base.w[id]) - c.base.D[id + q * a];
         for (int i = 0; i < q; ++i) pa.w[i] = c.base.w[i];
         for (int d = 0; d < 3; ++d) pa.adv[d] = c.base.adv[d];
+        for (int i = 0; i < 64; ++i) pa.Sf[i] = (float)pa.S[i];
         cudaGraph_t g = nullptr;
         e = cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return e;

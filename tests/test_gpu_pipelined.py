@@ -92,7 +92,7 @@ def test_pipelined_fp32_bulk_steps(rb, cuda_ok, scheme, nqk):
 
 ADV = [1.0, 0.5, -0.25]
 # the advection kernel runs more CTAs per SM, so its grids are larger
-ADV_NQS = [(8, (10, 10, 8)), (6, (12, 12, 10)), (4, (20, 20, 16))]
+ADV_NQS = [(8, (12, 12, 10)), (6, (12, 12, 10)), (4, (20, 20, 16))]
 
 
 def _build_adv(rb, nq, K, per=(1, 1, 0), precision="fp64", surface="rusanov"):
