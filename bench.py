@@ -46,11 +46,17 @@ WORKLOADS = {
                                          warp=True),
     "adv2d_weak_n4_16_fp64": dict(dim=2, N=4, K=16, L=1.0, law="advection", vflux="weak", precision="fp64",
                                   warp=False),
+    # one field, velocity (1, 0.5, 0.25), sine + Gaussian: the pipelined advection kernel
+    "adv3d_weak_n7_32_fp64": dict(dim=3, N=7, K=32, L=1.0, law="advection", vflux="weak", precision="fp64",
+                                  warp=False),
+    "adv3d_weak_n7_32_fp32bulk": dict(dim=3, N=7, K=32, L=1.0, law="advection", vflux="weak",
+                                      precision="fp32_bulk", warp=False),
     # adapted: 4^3 trees on the periodic unit cube, refined twice within radius 0.25 of the
     # centre (2:1 balanced, hanging faces coupled by mortars), N = 5, density pulse
     "euler3d_kg_n5_adapted_fp32bulk": dict(dim=3, N=5, K=4, L=1.0, law="euler", vflux="kg", precision="fp32_bulk",
                                            warp=False, adapted=True),
 }
+ADV_VELOCITY = (1.0, 0.5, 0.25)  # advection workloads (the first dim components)
 SERVE_WORKLOAD = "serve_poisson_mix_fp32bulk"
 DEFAULT = "euler3d_kg_n7_32_fp64"
 METRIC = "DOF-updates/s per RHS"
@@ -152,7 +158,7 @@ def setup(rb, w, device):
         # for N = 7 in 3-D at CFL 0.4 (the oracle blows up after 22 steps as well)
         dt = 0.4 * grid.min_node_distance() / ic.max_wavespeed(grid, law, q0)
     else:
-        law = rb.AdvectionLaw(dim, (1.0, 0.5))
+        law = rb.AdvectionLaw(dim, ADV_VELOCITY[:dim])
         q0 = ic.sine_plus_gaussian(grid, law, sigma=0.05)
         form = rb.WeakForm()
         dt = 0.5 * grid.min_node_distance() / math.hypot(*law.u)
@@ -344,7 +350,7 @@ def cpu_sample(w, max_seconds=20.0):
         law = O.Law(O.LAW_EULER, dim, form=O.FORM_FLUXDIFF, volume_flux=O.FLUX_KG)
         q = og.initial_condition(law, 4, [5.0, 0.5 * math.sqrt(1.4), w["L"] / 2, w["L"] / 2])
     else:
-        law = O.Law(O.LAW_ADVECTION, dim, adv=[1.0, 0.5])
+        law = O.Law(O.LAW_ADVECTION, dim, adv=list(ADV_VELOCITY[:dim]))
         q = og.initial_condition(law, 3, [0.05, 0.5, 0.5, 0.5])
     dq = og.state(law)
     dt = 1e-4
@@ -389,7 +395,7 @@ def run_reference(args, w):
         law = O.Law(O.LAW_EULER, dim, form=O.FORM_FLUXDIFF, volume_flux=O.FLUX_KG)
         q = og.initial_condition(law, 4, [5.0, 0.5 * math.sqrt(1.4), w["L"] / 2, w["L"] / 2])
     else:
-        law = O.Law(O.LAW_ADVECTION, dim, adv=[1.0, 0.5])
+        law = O.Law(O.LAW_ADVECTION, dim, adv=list(ADV_VELOCITY[:dim]))
         q = og.initial_condition(law, 3, [0.05, 0.5, 0.5, 0.5])
     dq = og.state(law)
     dt = 1e-4
