@@ -109,6 +109,30 @@ rb200_status rb200_lsrk54_step(rb200_handle* h, double* q, double* dq, double ti
 rb200_status rb200_lsrk54_step_host(rb200_handle* h, double* q_host, double time, double dt, int32_t nsteps,
                                     void* stream);
 
+/* One stage (0..4) of LSRK(5,4) (odesolvers.jl:163-189) from q_in to q_out:
+ * dq = rka[stage]*dq + RHS(q_in);  q_out = q_in + rkb[stage]*dt*dq, for the active
+ * elements.  q_in and q_out must be different device buffers.  A distributed step calls
+ * it five times, refreshing the ghost elements of q_in (start!/finish! around the
+ * right-hand side, dgsem.jl:95-100) before each; see rb200_set_active_elements. */
+rb200_status rb200_lsrk54_stage(rb200_handle* h, const double* q_in, double* q_out, double* dq, int32_t stage,
+                                double time, double dt, void* stream);
+
+/* Ghost elements: only elements 0..num_active-1 are computed and summed by the
+ * reductions; elements num_active..E-1 hold other ranks' data (Raven's GridArray ghost
+ * cells, gridarrays.jl:26-40).  Their face maps point to themselves; the faces of active
+ * elements may point into them.  Default: all E elements.  Not available with mortars. */
+rb200_status rb200_set_active_elements(rb200_handle* h, int64_t num_active);
+
+/* Buffer fills of the ghost exchange (setbuffer!/getbuffer!, communication.jl:267-293),
+ * 0-based indices, device arrays, asynchronous on `stream`:
+ *   pack:    buffer[i] = src[indices[i]],   i < n;
+ *   unpack:  dest[indices[i]] = buffer[i],  i < n.
+ * An index outside [0, src_len) or [0, dest_len) is skipped. */
+rb200_status rb200_pack_values(const double* src, int64_t src_len, const int64_t* indices, int64_t n,
+                               double* buffer, void* stream);
+rb200_status rb200_unpack_values(const double* buffer, const int64_t* indices, int64_t n, double* dest,
+                                 int64_t dest_len, void* stream);
+
 /* weightednorm(dg, q, 2; componentwise=true)  (measures.jl:6-21): out[s] =
  * sqrt(sum(MJ .* q_s.^2)) for s < Ns, out[Ns] = 2-norm of those.  FP64, synchronous,
  * deterministic (fixed reduction order).  out: host, Ns+1 doubles. */

@@ -373,6 +373,16 @@ class DGSEM:
                                              _stream_ptr()), self._h)
         return dq
 
+    def set_active_elements(self, num_active):
+        """Elements 0..num_active-1 are computed; the rest are ghost elements filled by an
+        exchange (Raven's GridArray ghost cells, gridarrays.jl:26-40)."""
+        _lib.check(_lib.lib().rb200_set_active_elements(self._h, int(num_active)), self._h)
+
+    def lsrk54_stage(self, q_in, q_out, dq, stage, time, dt):
+        """One LSRK(5,4) stage from q_in to q_out (odesolvers.jl:163-189)."""
+        _lib.check(_lib.lib().rb200_lsrk54_stage(self._h, q_in.ptr(), q_out.ptr(), dq.ptr() if dq is not None else None,
+                                                 int(stage), float(time), float(dt), _stream_ptr()), self._h)
+
     def lsrk54_steps(self, q, dq, time, dt, nsteps):
         _lib.check(_lib.lib().rb200_lsrk54_step(self._h, q.ptr(), dq.ptr() if dq is not None else None,
                                                 float(time), float(dt), int(nsteps), _stream_ptr()), self._h)

@@ -31,6 +31,10 @@ EXPORTED = [
     "rb200_tendency",
     "rb200_lsrk54_step",
     "rb200_lsrk54_step_host",
+    "rb200_lsrk54_stage",
+    "rb200_set_active_elements",
+    "rb200_pack_values",
+    "rb200_unpack_values",
     "rb200_weightednorm",
     "rb200_integrals",
     "rb200_entropy_integral",
@@ -151,6 +155,10 @@ def lib():
     L.rb200_tendency.argtypes = [P, P, P, D, I32, P]
     L.rb200_lsrk54_step.argtypes = [P, P, P, D, D, I32, P]
     L.rb200_lsrk54_step_host.argtypes = [P, P, D, D, I32, P]
+    L.rb200_lsrk54_stage.argtypes = [P, P, P, P, I32, D, D, P]
+    L.rb200_set_active_elements.argtypes = [P, I64]
+    L.rb200_pack_values.argtypes = [P, I64, P, I64, P, P]
+    L.rb200_unpack_values.argtypes = [P, P, I64, P, I64, P]
     L.rb200_weightednorm.argtypes = [P, P, P, P]
     L.rb200_integrals.argtypes = [P, P, P, P]
     L.rb200_entropy_integral.argtypes = [P, P, P, P]

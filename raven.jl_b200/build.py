@@ -41,7 +41,7 @@ def _sources():
         units.append((os.path.join(CSRC, "serve_inst.cu"), os.path.join(BUILD, f"serve_d{d}.o"),
                       [f"-DRB_SERVE_DIM={d}"]))
     for name in ("dispatch", "reduce", "pipelined_inst", "serve", "utilities", "mortar", "relaxation", "diagnostics",
-                 "api"):
+                 "halo", "api"):
         units.append((os.path.join(CSRC, f"{name}.cu"), os.path.join(BUILD, f"{name}.o"), []))
     return units
 

@@ -30,6 +30,7 @@ using namespace rb200;
 struct rb200_handle {
     int dim = 0, nq = 0, np = 0, nfp = 0, nf = 0, ns = 0;
     int64_t E = 0;
+    int64_t E_active = 0;  // elements the kernels and reductions process; E_active..E-1 are ghosts
     int law = 0, form = 0, vflux = 0, sflux = 0, prec = 0, combo = 0, geom = 0;
     double gamma = 1.4, adv[3] = {0, 0, 0};
     double D[kMaxNq * kMaxNq] = {0}, w[kMaxNq] = {0};
@@ -220,7 +221,7 @@ StageArgs base_args(const rb200_handle* h) {
     a.sgeo = h->d_sgeo;
     a.nbr = h->d_nbr;
     a.ncflux = h->d_ncflux;
-    a.E = h->E;
+    a.E = h->E_active;
     a.surface_rusanov = h->sflux == RB200_FLUX_RUSANOV ? 1 : 0;
     a.surface_flux = h->sflux;
     a.gamma = h->gamma;
@@ -321,7 +322,7 @@ RelaxGeo relax_geo(const rb200_handle* h) {
     G.np = h->np;
     G.geom = h->geom;
     G.euler = h->law == RB200_LAW_EULER ? 1 : 0;
-    G.E = h->E;
+    G.E = h->E_active;
     G.gamma = h->gamma;
     std::memcpy(G.w, h->w, sizeof(G.w));
     return G;
@@ -458,6 +459,7 @@ rb200_status rb200_create(const rb200_desc* d, rb200_handle** out) {
     h->nfp = h->np / d->nq;
     h->nf = 2 * d->dim;
     h->E = d->num_elements;
+    h->E_active = d->num_elements;
     h->law = d->law;
     h->form = d->volume_form;
     h->vflux = d->volume_flux;
@@ -670,7 +672,7 @@ rb200_status rb200_tendency(rb200_handle* h, double* dq, const double* q, double
     (void)time;  // the advection and Euler laws have no time-dependent sources
     if (!h) return RB200_ERR_BAD_ARG;
     if (!dq || !q) return fail(h, RB200_ERR_BAD_ARG, "null state pointer");
-    if (h->E == 0) return RB200_OK;
+    if (h->E_active == 0) return RB200_OK;
     DeviceGuard guard(h->device);
     StageArgs a = base_args(h);
     a.q_in = q;
@@ -687,9 +689,45 @@ rb200_status rb200_lsrk54_step(rb200_handle* h, double* q, double* dq, double ti
     if (!h) return RB200_ERR_BAD_ARG;
     if (!q || (!dq && h->prec == RB200_PRECISION_FP64)) return fail(h, RB200_ERR_BAD_ARG, "null state pointer");
     if (nsteps < 0 || !std::isfinite(dt)) return fail(h, RB200_ERR_BAD_ARG, "bad nsteps or dt");
-    if (h->E == 0 || nsteps == 0) return RB200_OK;
+    if (h->E_active == 0 || nsteps == 0) return RB200_OK;
     DeviceGuard guard(h->device);
     return run_steps(h, q, dq, dt, nsteps, (cudaStream_t)stream);
+}
+
+// One stage of LSRK(5,4) (odesolvers.jl:163-189) from q_in to q_out: the building block of
+// a step whose ghost elements are refreshed between stages (the start!/finish! exchange
+// of dgsem.jl:95-100 around every right-hand side).
+rb200_status rb200_lsrk54_stage(rb200_handle* h, const double* q_in, double* q_out, double* dq, int32_t stage,
+                                double time, double dt, void* stream) {
+    (void)time;
+    if (!h) return RB200_ERR_BAD_ARG;
+    if (!q_in || !q_out || (!dq && h->prec == RB200_PRECISION_FP64))
+        return fail(h, RB200_ERR_BAD_ARG, "null state pointer");
+    if (q_in == q_out) return fail(h, RB200_ERR_BAD_ARG, "q_in and q_out must be different buffers");
+    if (stage < 0 || stage > 4 || !std::isfinite(dt)) return fail(h, RB200_ERR_BAD_ARG, "bad stage or dt");
+    if (h->E_active == 0) return RB200_OK;
+    DeviceGuard guard(h->device);
+    StageArgs a = base_args(h);
+    a.q_in = q_in;
+    a.q_out = q_out;
+    a.dq = h->prec == RB200_PRECISION_FP32_BULK ? static_cast<void*>(h->d_dq32) : static_cast<void*>(dq);
+    a.mode = RKA[stage] == 0.0 ? MODE_STAGE_FIRST : MODE_STAGE;
+    a.rka = RKA[stage];
+    a.rkb_dt = RKB[stage] * dt;
+    cudaError_t e = launch_any(h, a, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "stage kernel launch");
+    return RB200_OK;
+}
+
+rb200_status rb200_set_active_elements(rb200_handle* h, int64_t num_active) {
+    if (!h) return RB200_ERR_BAD_ARG;
+    if (num_active < 0 || num_active > h->E) return fail(h, RB200_ERR_BAD_ARG, "active elements out of range");
+    if (h->nmortars > 0 && num_active != h->E)
+        return fail(h, RB200_ERR_UNSUPPORTED, "ghost elements on an adapted grid");
+    DeviceGuard guard(h->device);
+    free_graph(h);  // a captured step holds the old element count
+    h->E_active = num_active;
+    return RB200_OK;
 }
 
 rb200_status rb200_lsrk54_step_host(rb200_handle* h, double* q_host, double time, double dt, int32_t nsteps,
@@ -719,7 +757,7 @@ static rb200_status sums(rb200_handle* h, const double* q, double* host, cudaStr
     if (!h) return RB200_ERR_BAD_ARG;
     if (!q || !host) return fail(h, RB200_ERR_BAD_ARG, "null pointer");
     DeviceGuard guard(h->device);
-    cudaError_t e = launch_weighted_sums(q, h->d_elem_geo, h->d_vgeo, h->d_w, h->dim, h->nq, h->ns, h->E, h->geom,
+    cudaError_t e = launch_weighted_sums(q, h->d_elem_geo, h->d_vgeo, h->d_w, h->dim, h->nq, h->ns, h->E_active, h->geom,
                                          h->d_partial, h->red_blocks, h->d_sums, s);
     if (e != cudaSuccess) return cuda_fail(h, e, "reduction launch");
     e = cudaMemcpyAsync(host, h->d_sums, 2 * h->ns * sizeof(double), cudaMemcpyDeviceToHost, s);
@@ -934,6 +972,7 @@ rb200_status rb200_set_mortars(rb200_handle* h, const int64_t* mortars, int64_t 
     if (num_mortars < 0 || (num_mortars > 0 && (!mortars || !IL || !IU || !PL || !PU))) return RB200_ERR_BAD_ARG;
     if (h->nmortars > 0) return fail(h, RB200_ERR_BAD_ARG, "mortars are already set");
     if (num_mortars == 0) return RB200_OK;
+    if (h->E_active != h->E) return fail(h, RB200_ERR_UNSUPPORTED, "mortars on a grid with ghost elements");
     if (h->geom != GEOM_AFFINE)
         return fail(h, RB200_ERR_UNSUPPORTED, "mortars are implemented for unwarped (affine) elements only");
     const int nf = h->nf, mcols = 2 + (h->dim == 3 ? 4 : 2);

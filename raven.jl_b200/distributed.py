@@ -1,0 +1,278 @@
+"""Element-partitioned DGSEM across ranks: one process per GPU, face traces exchanged
+between stages over torch.distributed (NCCL on GPUs, gloo on CPU).
+
+Raven's distributed design (src/balancelaws/dgsem.jl:95-100, src/communication.jl) keeps
+ghost cells behind the local cells of every GridArray (gridarrays.jl:26-40) and
+exchanges them with a CommPattern around each right-hand side:
+``start!(q, comm_manager)``, volume term, ``finish!(q, comm_manager)``, surface term.
+Here:
+
+* ``partition`` gives rank r the contiguous element range [E r / P, E (r + 1) / P) of the
+  grid's element order (the brick's tree order, so each range is a compact block).
+* ``LocalGrid`` holds the rank's elements followed by its ghost elements: the remote
+  face neighbours of its elements, in global order.  Faces between local elements and
+  ghosts are remapped into the local numbering; every face of a ghost maps to itself.
+* ``node_comm_pattern`` builds the CommPattern (communication.jl:3-40) fields with
+  0-based indices into the (Np, Ns, E + ghosts) state: only the face nodes a rank's
+  kernels read from each neighbour rank, for every field (``Nfp * Ns`` values per
+  partition-boundary face), not Raven's whole shared-node set.
+* ``HaloExchange`` packs the send buffer, posts one grouped send/receive per neighbour
+  rank and scatters the received buffer into the ghost elements.  On CUDA tensors the
+  buffer fills are the rb200_pack_values / rb200_unpack_values kernels; on CPU tensors
+  (gloo, host-logic tests) they are torch index operations.
+* ``DistributedDGSEM`` runs LSRK(5,4) stage by stage (rb200_lsrk54_stage) with the ghost
+  elements of the stage's input refreshed before each stage; the DGSEM handle computes
+  only the rank's own elements (rb200_set_active_elements).
+"""
+
+import types
+
+import numpy as np
+
+from . import _lib
+
+
+def partition(num_elements, nranks):
+    """Contiguous element ranges [(start, stop)] of the ranks (stop exclusive)."""
+    if nranks < 1:
+        raise ValueError("nranks must be positive")
+    return [(num_elements * r // nranks, num_elements * (r + 1) // nranks) for r in range(nranks)]
+
+
+def owner_of(parts, elements):
+    """Rank owning each global element index."""
+    stops = np.array([p[1] for p in parts], dtype=np.int64)
+    return np.searchsorted(stops, np.asarray(elements, dtype=np.int64), side="right")
+
+
+class LocalGrid:
+    """The rank's elements followed by its ghost elements, as a Raven-style grid object
+    the DGSEM constructor accepts (``.grid``)."""
+
+    def __init__(self, grid, parts, rank):
+        e0, e1 = parts[rank]
+        np_ = grid.np
+        vP = np.asarray(grid.vmapP, dtype=np.int64)[:, e0:e1]
+        nbr = (vP - 1) // np_  # global element of every face node's neighbour node
+        remote = (nbr < e0) | (nbr >= e1)
+        ghosts = np.unique(nbr[remote])
+        El, G = e1 - e0, len(ghosts)
+        glob = np.concatenate([np.arange(e0, e1, dtype=np.int64), ghosts])
+        local_el = np.where(remote, El + np.searchsorted(ghosts, nbr), nbr - e0)
+        vP_loc = np.empty((vP.shape[0], El + G), dtype=np.int64)
+        vP_loc[:, :El] = local_el * np_ + (vP - 1) % np_ + 1
+        vM = np.asarray(grid.vmapM, dtype=np.int64)[:, glob]
+        vM_loc = (vM - 1) % np_ + np_ * np.arange(El + G, dtype=np.int64)[None, :] + 1
+        vP_loc[:, El:] = vM_loc[:, El:]  # ghost faces map to themselves
+        bc = np.zeros((grid.nfaces, El + G), dtype=np.int64)
+        if getattr(grid, "boundarycodes", None) is not None:
+            bc[:, :El] = np.asarray(grid.boundarycodes, dtype=np.int64)[:, e0:e1]
+        self.rank, self.parts = rank, parts
+        self.start, self.stop = e0, e1
+        self.num_local, self.num_ghosts = El, G
+        self.ghosts = ghosts  # global indices of the ghost elements, ascending
+        self.global_elements = glob
+        vm = np.asfortranarray(np.asarray(grid.volume_metrics)[:, :, glob])
+        g = types.SimpleNamespace(
+            cell=grid.cell, dim=grid.dim, nq=grid.nq, np=np_, nfp=grid.nfp, nfaces=grid.nfaces, E=El + G,
+            points=np.asfortranarray(np.asarray(grid.points)[:, :, glob]),
+            volume_metrics=vm,
+            surface_metrics=np.asfortranarray(np.asarray(grid.surface_metrics)[:, :, glob]),
+            vmapM=np.asfortranarray(vM_loc), vmapP=np.asfortranarray(vP_loc), boundarycodes=np.asfortranarray(bc),
+        )
+        g.volume_weights = lambda: vm[:, grid.dim * grid.dim + 1, :]
+        self.grid = g
+
+    def local_state(self, q_global):
+        """The rank's (Np, Ns, E_local + ghosts) block of a global state (ghosts filled)."""
+        return np.asfortranarray(np.asarray(q_global)[:, :, self.global_elements])
+
+
+class CommPattern:
+    """Raven's CommPattern fields (communication.jl:3-27) with 0-based flat indices into
+    the rank's (Np, Ns, E_local + ghosts) state and (start, stop) slices per rank."""
+
+    def __init__(self, recvindices, recvranks, recvrankindices, sendindices, sendranks, sendrankindices):
+        self.recvindices = np.asarray(recvindices, dtype=np.int64)
+        self.recvranks = list(recvranks)
+        self.recvrankindices = list(recvrankindices)
+        self.sendindices = np.asarray(sendindices, dtype=np.int64)
+        self.sendranks = list(sendranks)
+        self.sendrankindices = list(sendrankindices)
+
+
+def _needed_nodes(grid, parts, reader, owner):
+    """Global (element, node) pairs of rank `owner` that rank `reader`'s faces read,
+    sorted by (element, node)."""
+    np_ = grid.np
+    r0, r1 = parts[reader]
+    o0, o1 = parts[owner]
+    vP = np.asarray(grid.vmapP, dtype=np.int64)[:, r0:r1].ravel() - 1
+    el = vP // np_
+    sel = np.unique(vP[(el >= o0) & (el < o1)])  # global node indices, sorted = (element, node) order
+    return sel // np_, sel % np_
+
+
+def _flat(elements_local, nodes, np_, ns):
+    """Flat indices n + Np (s + Ns e) of the given (element, node) pairs for every field,
+    ascending, which is the (element, field, node) order.  Sender and receiver number a
+    rank's elements in the same global order, so both sides list the values alike."""
+    e = np.asarray(elements_local, dtype=np.int64)[:, None]
+    n = np.asarray(nodes, dtype=np.int64)[:, None]
+    s = np.arange(ns, dtype=np.int64)[None, :]
+    return np.sort((n + np_ * (s + ns * e)).ravel())
+
+
+def node_comm_pattern(grid, parts, rank, ns):
+    """The rank's CommPattern for a law with `ns` fields."""
+    np_ = grid.np
+    nranks = len(parts)
+    e0, e1 = parts[rank]
+    vP = np.asarray(grid.vmapP, dtype=np.int64)[:, e0:e1]
+    nbr = (vP - 1) // np_
+    ghosts = np.unique(nbr[(nbr < e0) | (nbr >= e1)])
+    El = e1 - e0
+    recv, recvranks, recvslices = [], [], []
+    send, sendranks, sendslices = [], [], []
+    for other in range(nranks):
+        if other == rank:
+            continue
+        ge, gn = _needed_nodes(grid, parts, rank, other)  # what this rank reads from `other`
+        if len(ge):
+            idx = _flat(El + np.searchsorted(ghosts, ge), gn, np_, ns)
+            recvslices.append((sum(len(x) for x in recv), sum(len(x) for x in recv) + len(idx)))
+            recv.append(idx)
+            recvranks.append(other)
+        se, sn = _needed_nodes(grid, parts, other, rank)  # what `other` reads from this rank
+        if len(se):
+            idx = _flat(se - e0, sn, np_, ns)
+            sendslices.append((sum(len(x) for x in send), sum(len(x) for x in send) + len(idx)))
+            send.append(idx)
+            sendranks.append(other)
+    cat = lambda xs: np.concatenate(xs) if xs else np.zeros(0, dtype=np.int64)  # noqa: E731
+    pat = CommPattern(cat(recv), recvranks, recvslices, cat(send), sendranks, sendslices)
+    total = np_ * ns * (El + len(ghosts))
+    if pat.sendindices.size and (pat.sendindices.min() < 0 or pat.sendindices.max() >= np_ * ns * El):
+        raise AssertionError("send indices outside the rank's own elements")
+    if pat.recvindices.size and (pat.recvindices.min() < np_ * ns * El or pat.recvindices.max() >= total):
+        raise AssertionError("receive indices outside the rank's ghost elements")
+    return pat
+
+
+class HaloExchange:
+    """start!/finish! of a buffered comm manager (communication.jl:296-334) over
+    torch.distributed point-to-point operations."""
+
+    def __init__(self, pattern, device=None, group=None):
+        import torch
+
+        self.pattern = pattern
+        self.group = group
+        self.device = torch.device("cpu") if device is None else torch.device(device)
+        self.send_idx = torch.as_tensor(pattern.sendindices, dtype=torch.int64, device=self.device)
+        self.recv_idx = torch.as_tensor(pattern.recvindices, dtype=torch.int64, device=self.device)
+        self.sendbuf = torch.zeros(len(pattern.sendindices), dtype=torch.float64, device=self.device)
+        self.recvbuf = torch.zeros(len(pattern.recvindices), dtype=torch.float64, device=self.device)
+        self._reqs = []
+
+    def pack(self, q):
+        """Send buffer <- the values of the flat state q the other ranks read."""
+        import torch
+
+        if q.is_cuda:
+            from . import _stream_ptr
+
+            _lib.check(_lib.lib().rb200_pack_values(q.data_ptr(), q.numel(), self.send_idx.data_ptr(),
+                                                    self.send_idx.numel(), self.sendbuf.data_ptr(), _stream_ptr()))
+        else:
+            torch.index_select(q, 0, self.send_idx, out=self.sendbuf)
+
+    def unpack(self, q):
+        """Ghost values of the flat state q <- receive buffer."""
+        if q.is_cuda:
+            from . import _stream_ptr
+
+            _lib.check(_lib.lib().rb200_unpack_values(self.recvbuf.data_ptr(), self.recv_idx.data_ptr(),
+                                                      self.recv_idx.numel(), q.data_ptr(), q.numel(), _stream_ptr()))
+        else:
+            q.index_copy_(0, self.recv_idx, self.recvbuf)
+
+    def start(self, q):
+        import torch.distributed as dist
+
+        self.pack(q)
+        p = self.pattern
+        ops = [dist.P2POp(dist.irecv, self.recvbuf[a:b], r, self.group) for r, (a, b) in zip(p.recvranks, p.recvrankindices)]
+        ops += [dist.P2POp(dist.isend, self.sendbuf[a:b], r, self.group) for r, (a, b) in zip(p.sendranks, p.sendrankindices)]
+        self._reqs = dist.batch_isend_irecv(ops) if ops else []
+
+    def finish(self, q):
+        for r in self._reqs:
+            r.wait()
+        self._reqs = []
+        if self.recv_idx.numel():
+            self.unpack(q)
+
+    def share(self, q):
+        self.start(q)
+        self.finish(q)
+
+
+class DistributedDGSEM:
+    """DGSEM over the ranks of a process group: this rank's elements plus ghosts on its
+    GPU, LSRK(5,4) stage by stage with a ghost exchange before every stage."""
+
+    def __init__(self, *, law, grid, surface_numericalflux, volume_form=None, precision="fp64", group=None,
+                 device=None):
+        import torch.distributed as dist
+
+        from . import DGSEM
+
+        self.rank = dist.get_rank(group)
+        self.nranks = dist.get_world_size(group)
+        self.parts = partition(grid.E, self.nranks)
+        self.local = LocalGrid(grid, self.parts, self.rank)
+        self.law = law
+        self.dg = DGSEM(law=law, grid=self.local.grid, surface_numericalflux=surface_numericalflux,
+                        volume_form=volume_form, precision=precision, device=device)
+        self.dg.set_active_elements(self.local.num_local)
+        self.pattern = node_comm_pattern(grid, self.parts, self.rank, law.ns)
+        # NCCL addresses peers by global rank
+        ranks = dist.get_process_group_ranks(group) if group is not None else None
+        if ranks is not None:
+            self.pattern.recvranks = [ranks[r] for r in self.pattern.recvranks]
+            self.pattern.sendranks = [ranks[r] for r in self.pattern.sendranks]
+        self.halo = HaloExchange(self.pattern, device=f"cuda:{self.dg.device}", group=group)
+        self._qtmp = None
+
+    def state(self, q_global):
+        """This rank's GridArray (elements and ghosts) of a global host state."""
+        from . import GridArray
+
+        return GridArray.from_numpy(self.local.local_state(q_global))
+
+    def lsrk54_steps(self, q, dq, time, dt, nsteps):
+        """nsteps of LSRK(5,4) on this rank's elements (dostep!, odesolvers.jl:51-66)."""
+        if self._qtmp is None or self._qtmp.data.shape != q.data.shape:
+            self._qtmp = q.similar()
+        cur, oth = q, self._qtmp
+        for step in range(nsteps):
+            for s in range(5):
+                self.halo.share(cur.data.view(-1))
+                self.dg.lsrk54_stage(cur, oth, dq, s, time + step * dt, dt)
+                cur, oth = oth, cur
+        if cur is not q:
+            q.data.copy_(cur.data)
+
+    def weightednorm(self, q):
+        """weightednorm over all ranks (measures.jl:6-21): the per-field sums of squares of
+        every rank are added with one all-reduce."""
+        import torch
+        import torch.distributed as dist
+
+        from . import weightednorm
+
+        per = weightednorm(self.dg, q, componentwise=True)
+        sq = torch.tensor([v * v for v in per], dtype=torch.float64, device=f"cuda:{self.dg.device}")
+        dist.all_reduce(sq, group=self.halo.group)
+        return float(sq.sum().sqrt().item())

@@ -1,0 +1,169 @@
+"""The element-partitioned path on one GPU.
+
+The ranks of a partition are emulated in one process: each rank has its own DGSEM
+handle on its local grid (elements plus ghosts), and between stages the ranks' send
+buffers, packed by rb200_pack_values, are copied into the receivers' buffers and
+scattered by rb200_unpack_values.  No kernel waits on another rank.  Bar: the
+partitioned LSRK steps equal the single-handle steps bit for bit on every rank's
+elements (the per-element arithmetic is the same; only the element walk differs).
+A one-rank process group (NCCL) runs DistributedDGSEM itself.
+"""
+
+import os
+import socket
+
+import numpy as np
+import pytest
+
+import oracle as O
+from gpu_util import initial_state, oracle_law, product_scheme, wrap_oracle_grid
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    # scheme, nq, K, periodic, precision: pipelined Euler, pipelined advection, generic kernel
+    ("eul_kg", 8, (6, 5, 4), (1, 1, 0), "fp64"),
+    ("eul_kg", 6, (6, 5, 4), (1, 1, 1), "fp32_bulk"),
+    ("adv_weak", 8, (6, 5, 4), (1, 0, 1), "fp64"),
+    ("eul_kg", 5, (5, 4, 4), (1, 1, 1), "fp64"),
+]
+
+
+def _setup(rb, scheme, nq, K, per, precision):
+    L = 1.0 if scheme.startswith("adv") else 10.0  # the Euler initial state lives on [0, 10]^3
+    og = O.Grid(3, nq, K, [0.0] * 3, [L] * 3, per)
+    g = wrap_oracle_grid(og)
+    adv = [1.0, 0.5, -0.25] if scheme.startswith("adv") else None
+    law, form = product_scheme(rb, scheme, 3, adv=adv)
+    olaw = oracle_law(scheme, 3, adv=adv)
+    q0 = initial_state(og, olaw, scheme, seed=31, amp=0.01)
+    return og, g, law, form, q0
+
+
+@pytest.mark.parametrize("nranks", [2, 3])
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c[0]}-nq{c[1]}-{c[4]}")
+def test_partitioned_steps_equal_single_handle(rb, cuda_ok, case, nranks):
+    import torch
+
+    from raven_b200 import distributed as D
+
+    scheme, nq, K, per, precision = case
+    og, g, law, form, q0 = _setup(rb, scheme, nq, K, per, precision)
+    dt, nsteps = 1e-3, 2
+    ref_dg = rb.DGSEM(law=law, grid=g, volume_form=form, surface_numericalflux=rb.RusanovFlux(), precision=precision)
+    ref = rb.GridArray.from_numpy(q0)
+    ref_dg.lsrk54_steps(ref, ref.similar(), 0.0, dt, nsteps)
+    ref_dg.sync_status()
+    q_ref = ref.numpy()
+
+    parts = D.partition(g.E, nranks)
+    locs = [D.LocalGrid(g, parts, r) for r in range(nranks)]
+    dgs, halos, qs, tmps, dqs = [], [], [], [], []
+    for r, L in enumerate(locs):
+        dg = rb.DGSEM(law=law, grid=L.grid, volume_form=form, surface_numericalflux=rb.RusanovFlux(),
+                      precision=precision)
+        dg.set_active_elements(L.num_local)
+        assert (dg.pipelined_ctas > 0) == (ref_dg.pipelined_ctas > 0)
+        s = L.local_state(q0)
+        s[:, :, L.num_local:] = 0.0
+        q = rb.GridArray.from_numpy(s)
+        dgs.append(dg)
+        halos.append(D.HaloExchange(D.node_comm_pattern(g, parts, r, law.ns), device="cuda"))
+        qs.append(q)
+        tmps.append(q.similar())
+        dqs.append(q.similar())
+    cur, oth = qs, tmps
+    for step in range(nsteps):
+        for st in range(5):
+            for r in range(nranks):
+                halos[r].pack(cur[r].data.view(-1))
+            for r in range(nranks):
+                p = halos[r].pattern
+                for peer, (a, b) in zip(p.recvranks, p.recvrankindices):
+                    pp = halos[peer].pattern
+                    sa, sb = pp.sendrankindices[pp.sendranks.index(r)]
+                    halos[r].recvbuf[a:b].copy_(halos[peer].sendbuf[sa:sb])
+                halos[r].unpack(cur[r].data.view(-1))
+            for r in range(nranks):
+                dgs[r].lsrk54_stage(cur[r], oth[r], dqs[r], st, step * dt, dt)
+            cur, oth = oth, cur
+    torch.cuda.synchronize()
+    for r, L in enumerate(locs):
+        dgs[r].sync_status()
+        got = cur[r].numpy()[:, :, : L.num_local]
+        assert np.array_equal(got, q_ref[:, :, L.start:L.stop]), (r, np.abs(got - q_ref[:, :, L.start:L.stop]).max())
+
+
+def test_pack_unpack_kernels(rb, cuda_ok):
+    """rb200_pack_values / rb200_unpack_values against torch indexing, and the skipped
+    out-of-range indices."""
+    import torch
+
+    from raven_b200 import _lib, _stream_ptr
+
+    src = torch.randn(1000, dtype=torch.float64, device="cuda")
+    idx = torch.tensor([5, 999, 0, 17, 2000, -3, 400], dtype=torch.int64, device="cuda")
+    buf = torch.full((7,), -1.0, dtype=torch.float64, device="cuda")
+    _lib.check(_lib.lib().rb200_pack_values(src.data_ptr(), src.numel(), idx.data_ptr(), 7, buf.data_ptr(),
+                                            _stream_ptr()))
+    want = torch.where((idx >= 0) & (idx < 1000), src[idx.clamp(0, 999)], torch.full_like(buf, -1.0))
+    assert torch.equal(buf, want)
+    dest = torch.zeros(1000, dtype=torch.float64, device="cuda")
+    _lib.check(_lib.lib().rb200_unpack_values(buf.data_ptr(), idx.data_ptr(), 7, dest.data_ptr(), dest.numel(),
+                                              _stream_ptr()))
+    ok = (idx >= 0) & (idx < 1000)
+    assert torch.equal(dest[idx[ok]], buf[ok])
+    assert int((dest != 0).sum()) == int(ok.sum())
+
+
+def test_stage_api_checks(rb, cuda_ok):
+    og, g, law, form, q0 = _setup(rb, "eul_kg", 4, (3, 3, 3), (1, 1, 1), "fp64")
+    dg = rb.DGSEM(law=law, grid=g, volume_form=form, surface_numericalflux=rb.RusanovFlux())
+    q = rb.GridArray.from_numpy(q0)
+    with pytest.raises(rb.RB200Error):
+        dg.lsrk54_stage(q, q, q.similar(), 0, 0.0, 1e-3)  # in place
+    with pytest.raises(rb.RB200Error):
+        dg.lsrk54_stage(q, q.similar(), q.similar(), 5, 0.0, 1e-3)
+    with pytest.raises(rb.RB200Error):
+        dg.set_active_elements(g.E + 1)
+    # five stages by hand equal one step
+    a, b, dq = rb.GridArray.from_numpy(q0), rb.GridArray.from_numpy(q0), q.similar()
+    cur, oth = a, a.similar()
+    for st in range(5):
+        dg.lsrk54_stage(cur, oth, dq, st, 0.0, 1e-3)
+        cur, oth = oth, cur
+    dg.lsrk54_steps(b, b.similar(), 0.0, 1e-3, 1)
+    assert np.array_equal(cur.numpy(), b.numpy())
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_distributed_dgsem_one_rank(rb, cuda_ok):
+    """DistributedDGSEM on a one-rank NCCL group equals the plain handle (no ghosts)."""
+    import datetime
+
+    import torch.distributed as dist
+
+    from raven_b200 import distributed as D
+
+    og, g, law, form, q0 = _setup(rb, "eul_kg", 8, (4, 4, 3), (1, 1, 1), "fp64")
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(_free_port())
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        ddg = D.DistributedDGSEM(law=law, grid=g, volume_form=form, surface_numericalflux=rb.RusanovFlux())
+        assert ddg.local.num_ghosts == 0 and ddg.pattern.recvindices.size == 0
+        q = ddg.state(q0)
+        ddg.lsrk54_steps(q, q.similar(), 0.0, 1e-3, 3)
+        dg = rb.DGSEM(law=law, grid=g, volume_form=form, surface_numericalflux=rb.RusanovFlux())
+        r = rb.GridArray.from_numpy(q0)
+        dg.lsrk54_steps(r, r.similar(), 0.0, 1e-3, 3)
+        assert np.array_equal(q.numpy(), r.numpy())
+        n = ddg.weightednorm(q)
+        assert abs(n - rb.weightednorm(dg, r)) <= 1e-14 * n
+    finally:
+        dist.destroy_process_group()
