@@ -127,8 +127,14 @@ def sine_warp(L, dim):
 
 
 def setup(rb, w, device):
-    import numpy as np
+    grid, law, form, q0, dt = problem(rb, w)
+    dg = rb.DGSEM(law=law, grid=grid, volume_form=form, surface_numericalflux=rb.RusanovFlux(),
+                  precision=w["precision"], device=device)
+    return grid, law, dg, q0, dt
 
+
+def problem(rb, w):
+    """The workload's grid, law, volume form, initial state and time step."""
     from raven_b200 import initial_conditions as ic
 
     dim, N, K, L = w["dim"], w["N"], w["K"], w["L"]
@@ -162,9 +168,7 @@ def setup(rb, w, device):
         q0 = ic.sine_plus_gaussian(grid, law, sigma=0.05)
         form = rb.WeakForm()
         dt = 0.5 * grid.min_node_distance() / math.hypot(*law.u)
-    dg = rb.DGSEM(law=law, grid=grid, volume_form=form, surface_numericalflux=rb.RusanovFlux(),
-                  precision=w["precision"], device=device)
-    return grid, law, dg, q0, dt
+    return grid, law, form, q0, dt
 
 
 class ClockSampler:
@@ -666,6 +670,101 @@ def run_serving_reference(args):
     return 0
 
 
+def run_sharded(args, w):
+    """The workload's grid partitioned over the ranks (raven_b200.distributed): each rank
+    steps its own elements stage by stage and exchanges face traces with its neighbour
+    ranks over NCCL before every stage.  value = global DOF updates / max-over-ranks time
+    (strong scaling: the grid is fixed as the ranks grow)."""
+    import datetime
+    import socket
+
+    import torch
+    import torch.distributed as dist
+
+    if w.get("adapted"):
+        raise SystemExit("--sharded: the adapted workload has mortars, which the partitioned path does not take")
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world == 1 and "MASTER_PORT" not in os.environ:
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            os.environ["MASTER_PORT"] = str(sk.getsockname()[1])
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120),
+                            device_id=torch.device("cuda", local))
+    try:
+        rb = load_product()
+        from raven_b200 import distributed as D
+
+        grid, law, form, q0, dt = problem(rb, w)
+        ddg = D.DistributedDGSEM(law=law, grid=grid, volume_form=form, surface_numericalflux=rb.RusanovFlux(),
+                                 precision=w["precision"], device=local)
+        q = ddg.state(q0)
+        dq = q.similar()
+        stream = torch.cuda.current_stream()
+
+        def barrier():
+            torch.cuda.synchronize()
+            dist.barrier()
+            torch.cuda.synchronize()
+
+        ddg.lsrk54_steps(q, dq, 0.0, dt, args.warmup)
+        barrier()
+        sampler = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local)
+        sampler.start()
+        time.sleep(0.3)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        e0.record(stream)
+        ddg.lsrk54_steps(q, dq, args.warmup * dt, dt, args.steps)
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+        sampler.stop()
+        t = torch.tensor([e0.elapsed_time(e1)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        nodes, ns = grid.np * grid.E, law.ns
+        value = nodes * ns * 5 * args.steps / (ms / 1e3)
+        norm = ddg.weightednorm(q)
+        pat = ddg.pattern
+        exch = torch.tensor([len(pat.recvindices) * 8.0, ddg.local.num_ghosts, ddg.local.num_local],
+                            device="cuda", dtype=torch.float64)
+        dist.all_reduce(exch)
+        if rank == 0:
+            packs = 2 if len(pat.recvindices) or len(pat.sendindices) else 0
+            line = {
+                "metric": METRIC,
+                "value": value,
+                "unit": UNIT,
+                "n_gpus": world,
+                "steps": args.steps,
+                "warmup": args.warmup,
+                "ms_per_step": ms / args.steps,
+                "higher_is_better": True,
+                "scaling": "strong",
+                "vs_baseline": None,
+                "dtype": "f32+f64" if w["precision"] == "fp32_bulk" else "f64",
+                "data": "synthetic",
+                "config": dict(config_json(args.workload, w, grid),
+                               parallelism=f"element partition over {world} ranks, face traces exchanged "
+                                           "over NCCL before every stage"),
+                "exchange": {"bytes_received_per_stage_all_ranks": exch[0].item(),
+                             "ghost_elements_all_ranks": int(exch[1].item()), "elements": grid.E},
+                "weightednorm": norm,
+                # rank 0's launches: 5 stage kernels a step, plus a pack and an unpack
+                # kernel a stage when the rank has neighbour ranks
+                "gpu_launches": 5 * args.steps * (1 + packs),
+                "clocks": sampler.summary(),
+            }
+            print(json.dumps(line), flush=True)
+    finally:
+        dist.destroy_process_group()
+    return 0
+
+
 def main(argv=None):
     p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     p.add_argument("--gpus", type=int, default=1)
@@ -680,6 +779,9 @@ def main(argv=None):
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--elements-per-side", type=int, default=None,
                    help="override the workload's elements per side (smaller cases for profiling)")
+    p.add_argument("--sharded", action="store_true",
+                   help="partition the workload's elements over the ranks (face-trace exchange between "
+                        "stages, strong scaling) instead of running one replica per rank")
     args = p.parse_args(argv)
     if args.workload == SERVE_WORKLOAD:
         return run_serving(args)
@@ -688,6 +790,8 @@ def main(argv=None):
         w["K"] = int(args.elements_per_side)
     if args.impl == "reference":
         return run_reference(args, w)
+    if args.sharded:
+        return run_sharded(args, w)
 
     import numpy as np
     import torch

@@ -167,3 +167,20 @@ def test_distributed_dgsem_one_rank(rb, cuda_ok):
         assert abs(n - rb.weightednorm(dg, r)) <= 1e-14 * n
     finally:
         dist.destroy_process_group()
+
+
+def test_bench_sharded_one_rank(rb, cuda_ok):
+    """bench.py --sharded on one rank prints its line (no ghosts, no exchange)."""
+    import json
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items() if k not in ("MASTER_PORT", "RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--sharded", "--steps", "3", "--warmup", "3",
+                        "--elements-per-side", "6"], capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads([x for x in r.stdout.splitlines() if x.startswith("{")][-1])
+    assert line["n_gpus"] == 1 and line["scaling"] == "strong" and line["value"] > 0
+    assert line["exchange"]["bytes_received_per_stage_all_ranks"] == 0
+    assert line["exchange"]["ghost_elements_all_ranks"] == 0
