@@ -117,6 +117,14 @@ rb200_status rb200_lsrk54_step_host(rb200_handle* h, double* q_host, double time
 rb200_status rb200_lsrk54_stage(rb200_handle* h, const double* q_in, double* q_out, double* dq, int32_t stage,
                                 double time, double dt, void* stream);
 
+/* The same stage on the active elements e_begin..e_end-1 only (0 <= e_begin <= e_end <=
+ * the active count).  A rank numbers its interior elements (no ghost neighbour) first:
+ * it runs them while its ghost exchange is in flight, then the rest once the ghosts
+ * have arrived (Raven's start!, volume term, finish!, dgsem.jl:95-100). */
+rb200_status rb200_lsrk54_stage_range(rb200_handle* h, const double* q_in, double* q_out, double* dq,
+                                      int32_t stage, int64_t e_begin, int64_t e_end, double time, double dt,
+                                      void* stream);
+
 /* Ghost elements: only elements 0..num_active-1 are computed and summed by the
  * reductions; elements num_active..E-1 hold other ranks' data (Raven's GridArray ghost
  * cells, gridarrays.jl:26-40).  Their face maps point to themselves; the faces of active

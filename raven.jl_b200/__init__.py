@@ -383,6 +383,13 @@ class DGSEM:
         _lib.check(_lib.lib().rb200_lsrk54_stage(self._h, q_in.ptr(), q_out.ptr(), dq.ptr() if dq is not None else None,
                                                  int(stage), float(time), float(dt), _stream_ptr()), self._h)
 
+    def lsrk54_stage_range(self, q_in, q_out, dq, stage, e_begin, e_end, time, dt):
+        """One LSRK(5,4) stage on the active elements e_begin..e_end-1."""
+        _lib.check(_lib.lib().rb200_lsrk54_stage_range(self._h, q_in.ptr(), q_out.ptr(),
+                                                       dq.ptr() if dq is not None else None, int(stage),
+                                                       int(e_begin), int(e_end), float(time), float(dt),
+                                                       _stream_ptr()), self._h)
+
     def lsrk54_steps(self, q, dq, time, dt, nsteps):
         _lib.check(_lib.lib().rb200_lsrk54_step(self._h, q.ptr(), dq.ptr() if dq is not None else None,
                                                 float(time), float(dt), int(nsteps), _stream_ptr()), self._h)

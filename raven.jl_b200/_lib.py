@@ -32,6 +32,7 @@ EXPORTED = [
     "rb200_lsrk54_step",
     "rb200_lsrk54_step_host",
     "rb200_lsrk54_stage",
+    "rb200_lsrk54_stage_range",
     "rb200_set_active_elements",
     "rb200_pack_values",
     "rb200_unpack_values",
@@ -156,6 +157,7 @@ def lib():
     L.rb200_lsrk54_step.argtypes = [P, P, P, D, D, I32, P]
     L.rb200_lsrk54_step_host.argtypes = [P, P, D, D, I32, P]
     L.rb200_lsrk54_stage.argtypes = [P, P, P, P, I32, D, D, P]
+    L.rb200_lsrk54_stage_range.argtypes = [P, P, P, P, I32, I64, I64, D, D, P]
     L.rb200_set_active_elements.argtypes = [P, I64]
     L.rb200_pack_values.argtypes = [P, I64, P, I64, P, P]
     L.rb200_unpack_values.argtypes = [P, P, I64, P, I64, P]

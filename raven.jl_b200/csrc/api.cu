@@ -178,13 +178,14 @@ cudaError_t launch_any(rb200_handle* h, const StageArgs& a, cudaStream_t st) {
         c.nbr = h->d_nbr;
         c.status = h->d_status;
         c.E = a.E;
+        c.e_begin = a.e_begin;
         c.mode = a.mode;
         c.surface_rusanov = a.surface_rusanov;
         c.rka = a.rka;
         c.rkb_dt = a.rkb_dt;
         c.gamma = a.gamma;
         std::memcpy(c.D, h->D, sizeof(c.D));
-        return launch_pipelined_curved(c, (int)std::min<int64_t>(h->pipe_curved_grid, a.E), st);
+        return launch_pipelined_curved(c, (int)std::min<int64_t>(h->pipe_curved_grid, a.E - a.e_begin), st);
     }
     const bool eligible = h->kernel_path == 0 && h->pipe_grid > 0 && aligned16(a.q_in) && aligned16(a.dq) &&
                           (!stage_mode || aligned16(a.q_out)) &&
@@ -200,6 +201,7 @@ cudaError_t launch_any(rb200_handle* h, const StageArgs& a, cudaStream_t st) {
     p.ncflux = h->d_ncflux;
     p.status = h->d_status;
     p.E = a.E;
+    p.e_begin = a.e_begin;
     p.mode = a.mode;
     p.surface_rusanov = a.surface_rusanov;
     p.rka = a.rka;
@@ -209,7 +211,7 @@ cudaError_t launch_any(rb200_handle* h, const StageArgs& a, cudaStream_t st) {
     for (int i = 0; i < 64; ++i) p.Sf[i] = (float)h->pipe_S[i];
     std::memcpy(p.w, h->w, sizeof(p.w));
     std::memcpy(p.adv, a.adv, sizeof(p.adv));
-    const int grid = (int)std::min<int64_t>(h->pipe_grid, a.E);
+    const int grid = (int)std::min<int64_t>(h->pipe_grid, a.E - a.e_begin);
     return launch_pipelined(h->nq, h->combo, h->prec, p, grid, st);
 }
 
@@ -694,29 +696,47 @@ rb200_status rb200_lsrk54_step(rb200_handle* h, double* q, double* dq, double ti
     return run_steps(h, q, dq, dt, nsteps, (cudaStream_t)stream);
 }
 
-// One stage of LSRK(5,4) (odesolvers.jl:163-189) from q_in to q_out: the building block of
-// a step whose ghost elements are refreshed between stages (the start!/finish! exchange
-// of dgsem.jl:95-100 around every right-hand side).
-rb200_status rb200_lsrk54_stage(rb200_handle* h, const double* q_in, double* q_out, double* dq, int32_t stage,
-                                double time, double dt, void* stream) {
-    (void)time;
-    if (!h) return RB200_ERR_BAD_ARG;
+// One stage of LSRK(5,4) (odesolvers.jl:163-189) from q_in to q_out on elements
+// e_begin..e_end-1: the building block of a step whose ghost elements are refreshed
+// between stages (the start!/finish! exchange of dgsem.jl:95-100 around every
+// right-hand side), with the interior elements computed while the exchange runs.
+static rb200_status stage_range(rb200_handle* h, const double* q_in, double* q_out, double* dq, int32_t stage,
+                                int64_t e_begin, int64_t e_end, double dt, cudaStream_t s) {
     if (!q_in || !q_out || (!dq && h->prec == RB200_PRECISION_FP64))
         return fail(h, RB200_ERR_BAD_ARG, "null state pointer");
     if (q_in == q_out) return fail(h, RB200_ERR_BAD_ARG, "q_in and q_out must be different buffers");
     if (stage < 0 || stage > 4 || !std::isfinite(dt)) return fail(h, RB200_ERR_BAD_ARG, "bad stage or dt");
-    if (h->E_active == 0) return RB200_OK;
+    if (e_begin < 0 || e_begin > e_end || e_end > h->E_active)
+        return fail(h, RB200_ERR_BAD_ARG, "element range outside the active elements");
+    if (e_begin == e_end) return RB200_OK;
     DeviceGuard guard(h->device);
     StageArgs a = base_args(h);
+    a.e_begin = e_begin;
+    a.E = e_end;
     a.q_in = q_in;
     a.q_out = q_out;
     a.dq = h->prec == RB200_PRECISION_FP32_BULK ? static_cast<void*>(h->d_dq32) : static_cast<void*>(dq);
     a.mode = RKA[stage] == 0.0 ? MODE_STAGE_FIRST : MODE_STAGE;
     a.rka = RKA[stage];
     a.rkb_dt = RKB[stage] * dt;
-    cudaError_t e = launch_any(h, a, (cudaStream_t)stream);
+    cudaError_t e = launch_any(h, a, s);
     if (e != cudaSuccess) return cuda_fail(h, e, "stage kernel launch");
     return RB200_OK;
+}
+
+rb200_status rb200_lsrk54_stage(rb200_handle* h, const double* q_in, double* q_out, double* dq, int32_t stage,
+                                double time, double dt, void* stream) {
+    (void)time;
+    if (!h) return RB200_ERR_BAD_ARG;
+    return stage_range(h, q_in, q_out, dq, stage, 0, h->E_active, dt, (cudaStream_t)stream);
+}
+
+rb200_status rb200_lsrk54_stage_range(rb200_handle* h, const double* q_in, double* q_out, double* dq,
+                                      int32_t stage, int64_t e_begin, int64_t e_end, double time, double dt,
+                                      void* stream) {
+    (void)time;
+    if (!h) return RB200_ERR_BAD_ARG;
+    return stage_range(h, q_in, q_out, dq, stage, e_begin, e_end, dt, (cudaStream_t)stream);
 }
 
 rb200_status rb200_set_active_elements(rb200_handle* h, int64_t num_active) {

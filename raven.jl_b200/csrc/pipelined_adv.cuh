@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(Q * Q * Q / pipea::npt<Q>(), (pipe_adv_min_cta
     }
     cp_async_commit();
 
-    int64_t es = blockIdx.x;
+    int64_t es = A.e_begin + blockIdx.x;
     for (int k = 0;; ++k, es += gridDim.x) {
         const int r = k % NST, r1 = (k + 1) % NST, b = k & 1;
         const int64_t e = BATCH ? sm.ref[r].e : (es < A.E ? es : -1);

@@ -36,7 +36,8 @@ struct PipeCurvedArgs {
     const double* sgeo;      // (4, 384, E): n, wsJ per face node
     const int32_t* nbr;      // (6, E)
     int32_t* status;
-    int64_t E;
+    int64_t E;               // elements e_begin..E-1 are computed
+    int64_t e_begin;
     int32_t mode;            // MODE_STAGE or MODE_STAGE_FIRST
     int32_t surface_rusanov;
     double rka, rkb_dt, gamma;
@@ -91,7 +92,7 @@ __global__ void __launch_bounds__(256, 2) pipelined_curved_kernel(const __grid_c
         fence_mbar_init();
     }
     for (int c = t; c < 64; c += NT) sm.D[c & 7][c >> 3] = (float)A.D[c];
-    int64_t e = blockIdx.x;
+    int64_t e = A.e_begin + blockIdx.x;
     if (t < 6 && e < A.E) cp_async4(&sm.nb[0][t], A.nbr + 6 * e + t);
     cp_async_commit();
     cp_async_wait_all();

@@ -41,7 +41,8 @@ struct PipeArgs {
     const int32_t* nbr;      // (6, E); -2 marks a mortar face of an adapted grid
     const double* ncflux;    // mortar face fluxes ((6, E) faces x (Ns, Nfp)), or null
     int32_t* status;         // device status word (0 = ok)
-    int64_t E;
+    int64_t E;        // elements e_begin..E-1 are computed (one state)
+    int64_t e_begin;
     int32_t mode;
     int32_t surface_rusanov;
     double rka, rkb_dt, gamma;
@@ -231,7 +232,7 @@ struct Cursor {
 
     __device__ bool start(const PipeArgs& A, const PipeBatch& B) {
         if constexpr (!BATCH) {
-            e = blockIdx.x;
+            e = A.e_begin + blockIdx.x;
             return e < A.E;
         } else {
             nch = *B.nchunks;
@@ -332,7 +333,7 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q>()))
         bulk_g2s(&sm.q[0][0], sm.ref[0].q + (size_t)sm.ref[0].e * NS * NP, qbytes, &sm.bar);
     }
     uint32_t phase = 0;
-    int64_t es = blockIdx.x;  // one state: the current element, kept in registers
+    int64_t es = A.e_begin + blockIdx.x;  // one state: the current element, kept in registers
     for (int buf = 0;; buf ^= 1, es += gridDim.x) {
         const int64_t e = BATCH ? sm.ref[buf].e : (es < A.E ? es : -1);
         if (e < 0) break;

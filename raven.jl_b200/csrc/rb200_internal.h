@@ -61,7 +61,8 @@ struct StageArgs {
     const int32_t* nbr;      // (2*dim, E): neighbour element across each face, -1 = boundary,
                              // -2 = a mortar face (its flux is in ncflux)
     const double* ncflux;    // mortar face fluxes ((2*dim, E) faces x (Ns, Nfp)), or null
-    int64_t E;
+    int64_t E;                // elements e_begin..E-1 are computed
+    int64_t e_begin;
     int32_t mode;
     int32_t surface_rusanov;  // 1 Rusanov, 0 central (with surface_flux Rusanov or central)
     int32_t surface_flux;     // kFlux*: the entropy family (EC, KG, Roe, matrix) runs its own kernels

@@ -674,7 +674,7 @@ __global__ void __launch_bounds__(Shape<DIM, NQ>::THREADS, (PersistentCfg<DIM, N
     using S = Shape<DIM, NQ>;
     using PC = PersistentCfg<DIM, NQ, COMBO, GEOM, T>;
     if constexpr (!PC::PF) {
-        const int64_t e = (int64_t)blockIdx.x * S::EPB + threadIdx.x / S::NP;
+        const int64_t e = A.e_begin + (int64_t)blockIdx.x * S::EPB + threadIdx.x / S::NP;
         stage_element<DIM, NQ, COMBO, GEOM, T, 0, SF>(A, elem_ptrs(A), e, e < A.E, smem_raw);
         return;
     }
@@ -683,10 +683,10 @@ __global__ void __launch_bounds__(Shape<DIM, NQ>::THREADS, (PersistentCfg<DIM, N
     T* dqs = reinterpret_cast<T*>(smem_raw + PC::off_dq);           // [2][NS][TH]
     const int tid = threadIdx.x, el = tid / NP, n = tid - el * NP;
     const bool pf_dq = A.mode == MODE_STAGE;
-    const int64_t ngroups = (A.E + S::EPB - 1) / S::EPB;
+    const int64_t ngroups = (A.E - A.e_begin + S::EPB - 1) / S::EPB;
     const ElemPtrs P = elem_ptrs(A);
     auto prefetch = [&](int64_t g, int b) {
-        const int64_t e = g * S::EPB + el;
+        const int64_t e = A.e_begin + g * S::EPB + el;
         if (g < ngroups && e < A.E) {
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
@@ -705,7 +705,7 @@ __global__ void __launch_bounds__(Shape<DIM, NQ>::THREADS, (PersistentCfg<DIM, N
     for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x, b ^= 1) {
         cpa_wait_all();                  // this group's values (issued one iteration ago)
         prefetch(g + gridDim.x, b ^ 1);  // the next group's, into the other buffer
-        const int64_t e = g * S::EPB + el;
+        const int64_t e = A.e_begin + g * S::EPB + el;
         Prefetched pf;
         pf.q = qs + b * NS * TH + tid;
         pf.dq = pf_dq ? static_cast<const void*>(dqs + b * NS * TH + tid) : nullptr;
@@ -725,7 +725,7 @@ cudaError_t launch_one(const StageArgs& a, cudaStream_t st) {
     static std::atomic<uint64_t> configured{0};
     cudaError_t err = ensure_smem_limit(kern, (int)PC::smem, configured);
     if (err != cudaSuccess) return err;
-    const int64_t groups = (a.E + S::EPB - 1) / S::EPB;
+    const int64_t groups = (a.E - a.e_begin + S::EPB - 1) / S::EPB;
     if (groups <= 0) return cudaSuccess;
     if constexpr (!PC::PF) {
         kern<<<(unsigned)groups, S::THREADS, PC::smem, st>>>(a);

@@ -20,9 +20,11 @@ Here:
   rank and scatters the received buffer into the ghost elements.  On CUDA tensors the
   buffer fills are the rb200_pack_values / rb200_unpack_values kernels; on CPU tensors
   (gloo, host-logic tests) they are torch index operations.
-* ``DistributedDGSEM`` runs LSRK(5,4) stage by stage (rb200_lsrk54_stage) with the ghost
-  elements of the stage's input refreshed before each stage; the DGSEM handle computes
-  only the rank's own elements (rb200_set_active_elements).
+* ``DistributedDGSEM`` runs LSRK(5,4) stage by stage: it posts the exchange of the
+  stage's input, runs the interior elements (rb200_lsrk54_stage_range) while the face
+  traces travel, waits, scatters them into the ghosts and runs the partition-boundary
+  elements.  The DGSEM handle computes only the rank's own elements
+  (rb200_set_active_elements).
 """
 
 import types
@@ -45,20 +47,40 @@ def owner_of(parts, elements):
     return np.searchsorted(stops, np.asarray(elements, dtype=np.int64), side="right")
 
 
+def _local_order(grid, parts, rank):
+    """The rank's own elements in local order (interior ones, those without a face
+    neighbour on another rank, first; each group in global order), the inverse map
+    (global - start -> local index), the number of interior elements and the ghost
+    elements (ascending global indices)."""
+    e0, e1 = parts[rank]
+    np_ = grid.np
+    vP = np.asarray(grid.vmapP, dtype=np.int64)[:, e0:e1]
+    nbr = (vP - 1) // np_
+    remote = (nbr < e0) | (nbr >= e1)
+    ghosts = np.unique(nbr[remote])
+    own = np.arange(e0, e1, dtype=np.int64)
+    boundary = remote.any(axis=0)
+    order = np.concatenate([own[~boundary], own[boundary]])
+    inv = np.empty(e1 - e0, dtype=np.int64)
+    inv[order - e0] = np.arange(e1 - e0, dtype=np.int64)
+    return order, inv, int((~boundary).sum()), ghosts
+
+
 class LocalGrid:
     """The rank's elements followed by its ghost elements, as a Raven-style grid object
-    the DGSEM constructor accepts (``.grid``)."""
+    the DGSEM constructor accepts (``.grid``).  The own elements come interior first
+    (``num_interior`` of them), then those with a face on another rank."""
 
     def __init__(self, grid, parts, rank):
         e0, e1 = parts[rank]
         np_ = grid.np
-        vP = np.asarray(grid.vmapP, dtype=np.int64)[:, e0:e1]
+        order, inv, n_int, ghosts = _local_order(grid, parts, rank)
+        vP = np.asarray(grid.vmapP, dtype=np.int64)[:, order]
         nbr = (vP - 1) // np_  # global element of every face node's neighbour node
         remote = (nbr < e0) | (nbr >= e1)
-        ghosts = np.unique(nbr[remote])
         El, G = e1 - e0, len(ghosts)
-        glob = np.concatenate([np.arange(e0, e1, dtype=np.int64), ghosts])
-        local_el = np.where(remote, El + np.searchsorted(ghosts, nbr), nbr - e0)
+        glob = np.concatenate([order, ghosts])
+        local_el = np.where(remote, El + np.searchsorted(ghosts, nbr), inv[np.clip(nbr - e0, 0, El - 1)])
         vP_loc = np.empty((vP.shape[0], El + G), dtype=np.int64)
         vP_loc[:, :El] = local_el * np_ + (vP - 1) % np_ + 1
         vM = np.asarray(grid.vmapM, dtype=np.int64)[:, glob]
@@ -66,12 +88,12 @@ class LocalGrid:
         vP_loc[:, El:] = vM_loc[:, El:]  # ghost faces map to themselves
         bc = np.zeros((grid.nfaces, El + G), dtype=np.int64)
         if getattr(grid, "boundarycodes", None) is not None:
-            bc[:, :El] = np.asarray(grid.boundarycodes, dtype=np.int64)[:, e0:e1]
+            bc[:, :El] = np.asarray(grid.boundarycodes, dtype=np.int64)[:, order]
         self.rank, self.parts = rank, parts
         self.start, self.stop = e0, e1
-        self.num_local, self.num_ghosts = El, G
+        self.num_local, self.num_ghosts, self.num_interior = El, G, n_int
         self.ghosts = ghosts  # global indices of the ghost elements, ascending
-        self.global_elements = glob
+        self.global_elements = glob  # global index of every local element (own, then ghosts)
         vm = np.asfortranarray(np.asarray(grid.volume_metrics)[:, :, glob])
         g = types.SimpleNamespace(
             cell=grid.cell, dim=grid.dim, nq=grid.nq, np=np_, nfp=grid.nfp, nfaces=grid.nfaces, E=El + G,
@@ -113,24 +135,23 @@ def _needed_nodes(grid, parts, reader, owner):
     return sel // np_, sel % np_
 
 
-def _flat(elements_local, nodes, np_, ns):
-    """Flat indices n + Np (s + Ns e) of the given (element, node) pairs for every field,
-    ascending, which is the (element, field, node) order.  Sender and receiver number a
-    rank's elements in the same global order, so both sides list the values alike."""
-    e = np.asarray(elements_local, dtype=np.int64)[:, None]
-    n = np.asarray(nodes, dtype=np.int64)[:, None]
-    s = np.arange(ns, dtype=np.int64)[None, :]
-    return np.sort((n + np_ * (s + ns * e)).ravel())
+def _flat(elements_global, elements_local, nodes, np_, ns):
+    """Flat indices n + Np (s + Ns e_local) of the given (element, node) pairs for every
+    field, in (global element, field, node) order: the order both the sender and the
+    receiver list the values in, whatever their local numbering."""
+    g = np.repeat(np.asarray(elements_global, dtype=np.int64), ns)
+    e = np.repeat(np.asarray(elements_local, dtype=np.int64), ns)
+    n = np.repeat(np.asarray(nodes, dtype=np.int64), ns)
+    s = np.tile(np.arange(ns, dtype=np.int64), len(nodes))
+    return (n + np_ * (s + ns * e))[np.lexsort((n, s, g))]
 
 
 def node_comm_pattern(grid, parts, rank, ns):
-    """The rank's CommPattern for a law with `ns` fields."""
+    """The rank's CommPattern for a law with `ns` fields (local numbering of LocalGrid)."""
     np_ = grid.np
     nranks = len(parts)
     e0, e1 = parts[rank]
-    vP = np.asarray(grid.vmapP, dtype=np.int64)[:, e0:e1]
-    nbr = (vP - 1) // np_
-    ghosts = np.unique(nbr[(nbr < e0) | (nbr >= e1)])
+    _, inv, _, ghosts = _local_order(grid, parts, rank)
     El = e1 - e0
     recv, recvranks, recvslices = [], [], []
     send, sendranks, sendslices = [], [], []
@@ -139,13 +160,13 @@ def node_comm_pattern(grid, parts, rank, ns):
             continue
         ge, gn = _needed_nodes(grid, parts, rank, other)  # what this rank reads from `other`
         if len(ge):
-            idx = _flat(El + np.searchsorted(ghosts, ge), gn, np_, ns)
+            idx = _flat(ge, El + np.searchsorted(ghosts, ge), gn, np_, ns)
             recvslices.append((sum(len(x) for x in recv), sum(len(x) for x in recv) + len(idx)))
             recv.append(idx)
             recvranks.append(other)
         se, sn = _needed_nodes(grid, parts, other, rank)  # what `other` reads from this rank
         if len(se):
-            idx = _flat(se - e0, sn, np_, ns)
+            idx = _flat(se, inv[se - e0], sn, np_, ns)
             sendslices.append((sum(len(x) for x in send), sum(len(x) for x in send) + len(idx)))
             send.append(idx)
             sendranks.append(other)
@@ -256,10 +277,16 @@ class DistributedDGSEM:
         if self._qtmp is None or self._qtmp.data.shape != q.data.shape:
             self._qtmp = q.similar()
         cur, oth = q, self._qtmp
+        n_int, n_loc = self.local.num_interior, self.local.num_local
         for step in range(nsteps):
+            t = time + step * dt
             for s in range(5):
-                self.halo.share(cur.data.view(-1))
-                self.dg.lsrk54_stage(cur, oth, dq, s, time + step * dt, dt)
+                # start!: pack and post the exchange; the interior elements read no ghost
+                # and run while it is in flight; finish!, then the partition-boundary ones
+                self.halo.start(cur.data.view(-1))
+                self.dg.lsrk54_stage_range(cur, oth, dq, s, 0, n_int, t, dt)
+                self.halo.finish(cur.data.view(-1))
+                self.dg.lsrk54_stage_range(cur, oth, dq, s, n_int, n_loc, t, dt)
                 cur, oth = oth, cur
         if cur is not q:
             q.data.copy_(cur.data)

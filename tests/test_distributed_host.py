@@ -84,11 +84,15 @@ def test_local_grids_and_in_process_exchange(rb, nranks):
     for r, L in enumerate(locs):
         lvP = np.asarray(L.grid.vmapP) - 1
         for le in range(L.num_local):
-            ge = L.start + le
+            ge = L.global_elements[le]
             lnode, gnode = lvP[:, le], vP[:, ge]
             got = states[r][lnode % g.np, :, lnode // g.np]
             want = q[gnode % g.np, :, gnode // g.np]
             assert np.array_equal(got, want)
+        # own elements in order: interior (no ghost neighbour) first, then the others
+        assert sorted(L.global_elements[: L.num_local]) == list(range(L.start, L.stop))
+        has_ghost = (lvP[:, : L.num_local] // g.np >= L.num_local).any(axis=0)
+        assert not has_ghost[: L.num_interior].any() and has_ghost[L.num_interior:].all()
         # ghosts are exactly the remote face neighbours, and each ghost face maps to itself
         nb = np.unique(vP[:, L.start:L.stop] // g.np)
         assert np.array_equal(L.ghosts, nb[(nb < L.start) | (nb >= L.stop)])
@@ -147,7 +151,7 @@ def _rank_main(rank, world, port, out):
         ref = og.tendency(law, q)
         lo = _oracle_of(L.grid)
         got = lo.tendency(law, local_q)
-        ok = bool(np.array_equal(got[:, :, : L.num_local], ref[:, :, L.start:L.stop]))
+        ok = bool(np.array_equal(got[:, :, : L.num_local], ref[:, :, L.global_elements[: L.num_local]]))
         flag = torch.tensor([1 if ok else 0])
         dist.all_reduce(flag)
         out.put((rank, ok, int(flag.item())))

@@ -75,8 +75,10 @@ def test_partitioned_steps_equal_single_handle(rb, cuda_ok, case, nranks):
     cur, oth = qs, tmps
     for step in range(nsteps):
         for st in range(5):
+            # the order of DistributedDGSEM: pack, interior elements, exchange, the rest
             for r in range(nranks):
                 halos[r].pack(cur[r].data.view(-1))
+                dgs[r].lsrk54_stage_range(cur[r], oth[r], dqs[r], st, 0, locs[r].num_interior, step * dt, dt)
             for r in range(nranks):
                 p = halos[r].pattern
                 for peer, (a, b) in zip(p.recvranks, p.recvrankindices):
@@ -85,13 +87,15 @@ def test_partitioned_steps_equal_single_handle(rb, cuda_ok, case, nranks):
                     halos[r].recvbuf[a:b].copy_(halos[peer].sendbuf[sa:sb])
                 halos[r].unpack(cur[r].data.view(-1))
             for r in range(nranks):
-                dgs[r].lsrk54_stage(cur[r], oth[r], dqs[r], st, step * dt, dt)
+                L = locs[r]
+                dgs[r].lsrk54_stage_range(cur[r], oth[r], dqs[r], st, L.num_interior, L.num_local, step * dt, dt)
             cur, oth = oth, cur
     torch.cuda.synchronize()
     for r, L in enumerate(locs):
         dgs[r].sync_status()
         got = cur[r].numpy()[:, :, : L.num_local]
-        assert np.array_equal(got, q_ref[:, :, L.start:L.stop]), (r, np.abs(got - q_ref[:, :, L.start:L.stop]).max())
+        want = q_ref[:, :, L.global_elements[: L.num_local]]
+        assert np.array_equal(got, want), (r, np.abs(got - want).max())
 
 
 def test_pack_unpack_kernels(rb, cuda_ok):
@@ -126,14 +130,24 @@ def test_stage_api_checks(rb, cuda_ok):
         dg.lsrk54_stage(q, q.similar(), q.similar(), 5, 0.0, 1e-3)
     with pytest.raises(rb.RB200Error):
         dg.set_active_elements(g.E + 1)
-    # five stages by hand equal one step
-    a, b, dq = rb.GridArray.from_numpy(q0), rb.GridArray.from_numpy(q0), q.similar()
-    cur, oth = a, a.similar()
-    for st in range(5):
-        dg.lsrk54_stage(cur, oth, dq, st, 0.0, 1e-3)
-        cur, oth = oth, cur
+    with pytest.raises(rb.RB200Error):
+        dg.lsrk54_stage_range(q, q.similar(), q.similar(), 0, 3, 2, 0.0, 1e-3)
+    with pytest.raises(rb.RB200Error):
+        dg.lsrk54_stage_range(q, q.similar(), q.similar(), 0, 0, g.E + 1, 0.0, 1e-3)
+    # five stages by hand, whole or in two element ranges, equal one step
+    b = rb.GridArray.from_numpy(q0)
     dg.lsrk54_steps(b, b.similar(), 0.0, 1e-3, 1)
-    assert np.array_equal(cur.numpy(), b.numpy())
+    for split in (None, 0, 11, g.E):
+        a, dq = rb.GridArray.from_numpy(q0), q.similar()
+        cur, oth = a, a.similar()
+        for st in range(5):
+            if split is None:
+                dg.lsrk54_stage(cur, oth, dq, st, 0.0, 1e-3)
+            else:
+                dg.lsrk54_stage_range(cur, oth, dq, st, 0, split, 0.0, 1e-3)
+                dg.lsrk54_stage_range(cur, oth, dq, st, split, g.E, 0.0, 1e-3)
+            cur, oth = oth, cur
+        assert np.array_equal(cur.numpy(), b.numpy()), split
 
 
 def _free_port():
