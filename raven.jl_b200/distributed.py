@@ -265,6 +265,9 @@ class DistributedDGSEM:
             self.pattern.sendranks = [ranks[r] for r in self.pattern.sendranks]
         self.halo = HaloExchange(self.pattern, device=f"cuda:{self.dg.device}", group=group)
         self._qtmp = None
+        # a grouped point-to-point call must not be a group's first collective unless
+        # every rank takes part in it; a rank without neighbour ranks posts none
+        dist.barrier(group=group)
 
     def state(self, q_global):
         """This rank's GridArray (elements and ghosts) of a global host state."""
