@@ -150,6 +150,32 @@ def test_stage_api_checks(rb, cuda_ok):
         assert np.array_equal(cur.numpy(), b.numpy()), split
 
 
+@pytest.mark.parametrize("precision", ["fp32_bulk", "fp64"])
+def test_stage_ranges_curved(rb, cuda_ok, precision):
+    """Stages split into element ranges on a warped grid (the curved pipelined kernel in
+    FP32 bulk, the generic curved kernel in FP64) equal whole stages bit for bit."""
+    og = O.Grid(3, 8, (5, 4, 4), [0.0] * 3, [10.0] * 3, (1, 1, 1), O.WARP_SINE, 0.1)
+    g = wrap_oracle_grid(og)
+    law, form = product_scheme(rb, "eul_kg", 3)
+    q0 = initial_state(og, oracle_law("eul_kg", 3), "eul_kg", seed=33, amp=0.01)
+    dg = rb.DGSEM(law=law, grid=g, volume_form=form, surface_numericalflux=rb.RusanovFlux(), precision=precision)
+    assert dg.geometry == "curved" and ((dg.pipelined_ctas > 0) == (precision == "fp32_bulk"))
+    res = []
+    for split in (None, 37):
+        a, dq = rb.GridArray.from_numpy(q0), rb.GridArray.from_numpy(q0).similar()
+        cur, oth = a, a.similar()
+        for st in range(5):
+            if split is None:
+                dg.lsrk54_stage(cur, oth, dq, st, 0.0, 1e-3)
+            else:
+                dg.lsrk54_stage_range(cur, oth, dq, st, 0, split, 0.0, 1e-3)
+                dg.lsrk54_stage_range(cur, oth, dq, st, split, g.E, 0.0, 1e-3)
+            cur, oth = oth, cur
+        dg.sync_status()
+        res.append(cur.numpy())
+    assert np.array_equal(res[0], res[1])
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
@@ -167,7 +193,10 @@ def test_distributed_dgsem_one_rank(rb, cuda_ok):
     og, g, law, form, q0 = _setup(rb, "eul_kg", 8, (4, 4, 3), (1, 1, 1), "fp64")
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(_free_port())
-    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    import torch
+
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60),
+                            device_id=torch.device("cuda", torch.cuda.current_device()))
     try:
         ddg = D.DistributedDGSEM(law=law, grid=g, volume_form=form, surface_numericalflux=rb.RusanovFlux())
         assert ddg.local.num_ghosts == 0 and ddg.pattern.recvindices.size == 0

@@ -24,7 +24,7 @@ def F(rb, cuda_ok):
 
 
 GRIDS = [(2, 4, (3, 2), (True, True), 2), (2, 6, (2, 2), (False, True), 2), (3, 4, (2, 2, 2), (True, True, True), 2),
-         (3, 6, (2, 1, 2), (True, True, False), 2)]
+         (3, 6, (2, 1, 2), (True, True, False), 2), (3, 8, (2, 2, 1), (True, True, True), 2)]
 
 
 def _product(rb, grid, lw, precision="fp64"):
