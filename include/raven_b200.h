@@ -203,9 +203,12 @@ rb200_status rb200_face_vmapP(rb200_handle* h, int64_t* vmapP_out, void* stream)
 rb200_status rb200_set_mortars(rb200_handle* h, const int64_t* mortars, int64_t num_mortars, const double* IL,
                                const double* IU, const double* PL, const double* PU);
 
-/* Kernel selection: 0 = automatic (the persistent TMA-pipelined kernel for 3-D, nq = 8,
- * unwarped-brick flux differencing when the state pointers are 16-byte aligned, the
- * generic stage kernel otherwise), 1 = generic stage kernel only. */
+/* Kernel selection: 0 = automatic, 1 = generic stage kernel only.  Automatic runs a
+ * persistent bulk-copy-pipelined kernel where one exists and the state pointers are
+ * 16-byte aligned: 3-D unwarped bricks with nq = 4, 6, 8 (Euler Kennedy-Gruber or
+ * entropy-conservative flux differencing with Rusanov or central surface flux; weak-form
+ * advection), and 3-D nq = 8 curved grids in FP32_BULK (Euler Kennedy-Gruber).  Every
+ * other configuration runs the generic stage kernel. */
 rb200_status rb200_set_kernel_path(rb200_handle* h, int32_t path);
 
 /* Synchronizes `stream` and returns RB200_ERR_TIMEOUT if a kernel of this handle gave
