@@ -184,11 +184,14 @@ class HaloExchange:
     """start!/finish! of a buffered comm manager (communication.jl:296-334) over
     torch.distributed point-to-point operations."""
 
-    def __init__(self, pattern, device=None, group=None):
+    def __init__(self, pattern, device=None, group=None, tag=0):
         import torch
 
+        if not 0 <= tag <= 32767:  # the tag range of commmanager (communication.jl:167-169)
+            raise ValueError(f"The tag={tag} is not in the valid range 0:32767")
         self.pattern = pattern
         self.group = group
+        self.tag = tag
         self.device = torch.device("cpu") if device is None else torch.device(device)
         self.send_idx = torch.as_tensor(pattern.sendindices, dtype=torch.int64, device=self.device)
         self.recv_idx = torch.as_tensor(pattern.recvindices, dtype=torch.int64, device=self.device)
@@ -223,8 +226,10 @@ class HaloExchange:
 
         self.pack(q)
         p = self.pattern
-        ops = [dist.P2POp(dist.irecv, self.recvbuf[a:b], r, self.group) for r, (a, b) in zip(p.recvranks, p.recvrankindices)]
-        ops += [dist.P2POp(dist.isend, self.sendbuf[a:b], r, self.group) for r, (a, b) in zip(p.sendranks, p.sendrankindices)]
+        ops = [dist.P2POp(dist.irecv, self.recvbuf[a:b], r, self.group, self.tag)
+               for r, (a, b) in zip(p.recvranks, p.recvrankindices)]
+        ops += [dist.P2POp(dist.isend, self.sendbuf[a:b], r, self.group, self.tag)
+                for r, (a, b) in zip(p.sendranks, p.sendrankindices)]
         self._reqs = dist.batch_isend_irecv(ops) if ops else []
 
     def finish(self, q):

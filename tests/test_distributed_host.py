@@ -176,3 +176,59 @@ def test_gloo_two_ranks_tendency_bit_exact(rb):
     assert all(p.exitcode == 0 for p in procs)
     assert sorted(r for r, _, _ in res) == [0, 1]
     assert all(ok and total == 2 for _, ok, total in res), res
+
+
+def _comm_rank_main(rank, world, port, out):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        import commpattern_cases as C
+        import conftest
+
+        conftest.load_product()
+        D = _dist()
+        c = C.CASES[rank]
+        pat = C.pattern(D, rank)
+        data1 = torch.arange(1, c["datalength"] + 1, dtype=torch.float64) + 100 * rank
+        data2 = 2 * data1
+        cm1, cm2 = D.HaloExchange(pat, tag=1), D.HaloExchange(pat, tag=2)
+        cm2.start(data2)  # two exchanges in flight at once, told apart by their tags
+        cm1.share(data1)
+        cm2.finish(data2)
+        want = torch.tensor(c["datacomm"], dtype=torch.float64)
+        out.put((rank, bool(torch.equal(data1, want)), bool(torch.equal(data2, 2 * want))))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_three_ranks_reference_patterns(rb):
+    """The reference's three-rank start!/share!/finish! test
+    (test/mpitest_n3_communication.jl) on gloo ranks: hand-built patterns, known data."""
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_comm_rank_main, args=(r, 3, port, out)) for r in range(3)]
+    for p in procs:
+        p.start()
+    res = [out.get(timeout=240) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+    assert all(p.exitcode == 0 for p in procs)
+    assert sorted(r[0] for r in res) == [0, 1, 2]
+    assert all(a and b for _, a, b in res), res
+
+
+def test_halo_exchange_rejects_bad_tag(rb):
+    D = _dist()
+    import commpattern_cases as C
+
+    with pytest.raises(ValueError):
+        D.HaloExchange(C.pattern(D, 0), tag=40000)

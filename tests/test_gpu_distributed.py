@@ -120,6 +120,31 @@ def test_pack_unpack_kernels(rb, cuda_ok):
     assert int((dest != 0).sum()) == int(ok.sum())
 
 
+def test_reference_patterns_on_device(rb, cuda_ok):
+    """The reference's three-rank patterns (test/mpitest_n3_communication.jl) through the
+    device pack/unpack kernels, the ranks emulated in one process."""
+    import torch
+
+    import commpattern_cases as C
+    from raven_b200 import distributed as D
+
+    halos, data = [], []
+    for r in range(3):
+        halos.append(D.HaloExchange(C.pattern(D, r), device="cuda"))
+        data.append(torch.arange(1, C.CASES[r]["datalength"] + 1, dtype=torch.float64, device="cuda") + 100 * r)
+    for r in range(3):
+        halos[r].pack(data[r])
+    for r in range(3):
+        p = halos[r].pattern
+        for peer, (a, b) in zip(p.recvranks, p.recvrankindices):
+            pp = halos[peer].pattern
+            sa, sb = pp.sendrankindices[pp.sendranks.index(r)]
+            halos[r].recvbuf[a:b].copy_(halos[peer].sendbuf[sa:sb])
+        halos[r].unpack(data[r])
+    for r in range(3):
+        assert data[r].cpu().tolist() == [float(v) for v in C.CASES[r]["datacomm"]]
+
+
 def test_stage_api_checks(rb, cuda_ok):
     og, g, law, form, q0 = _setup(rb, "eul_kg", 4, (3, 3, 3), (1, 1, 1), "fp64")
     dg = rb.DGSEM(law=law, grid=g, volume_form=form, surface_numericalflux=rb.RusanovFlux())
