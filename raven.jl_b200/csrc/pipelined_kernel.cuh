@@ -286,10 +286,20 @@ __device__ __forceinline__ void fetch_part(const ElemRef& r, int t, double (&geo
 #ifndef RB200_PIPE_MIN4
 #define RB200_PIPE_MIN4 14, 20
 #endif
+#ifndef RB200_PIPE_MIN8_FP64
+#define RB200_PIPE_MIN8_FP64 2
+#endif
+#ifndef RB200_PIPE_MIN8_FP32
+#define RB200_PIPE_MIN8_FP32 3
+#endif
+// unroll factor of the pair loop over partners (8: fully unrolled)
+#ifndef RB200_PIPE_UNROLL_A
+#define RB200_PIPE_UNROLL_A 8
+#endif
 template <typename T, int Q = 8>
 constexpr int pipe_min_ctas() {
-    constexpr int m6[2] = {RB200_PIPE_MIN6}, m4[2] = {RB200_PIPE_MIN4};
-    return Q == 8 ? (sizeof(T) == 4 ? 3 : 2) : Q == 6 ? m6[sizeof(T) == 4] : m4[sizeof(T) == 4];
+    constexpr int m8[2] = {RB200_PIPE_MIN8_FP64, RB200_PIPE_MIN8_FP32}, m6[2] = {RB200_PIPE_MIN6}, m4[2] = {RB200_PIPE_MIN4};
+    return Q == 8 ? m8[sizeof(T) == 4] : Q == 6 ? m6[sizeof(T) == 4] : m4[sizeof(T) == 4];
 }
 
 // NPT nodes per thread: thread t owns nodes t + (Np/NPT)*h, h < NPT, which share i, j
@@ -475,7 +485,8 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q>()))
             }
         };
         auto load_aux = [&](T (&pv)[NAUX], const int n) { sm.aux.get(PAD(n), pv); };
-#pragma unroll
+        constexpr int kUnrA = RB200_PIPE_UNROLL_A < NQ ? RB200_PIPE_UNROLL_A : NQ;
+#pragma unroll kUnrA
         for (int a = 0; a < NQ; ++a) {
             const T sx = sm.S[0][a][ii], sy = sm.S[1][a][jj];
 #pragma unroll
