@@ -16,8 +16,13 @@ advection or Euler, N in {3, 5, 7}, 8-64 (2-D) or 4-32 (3-D) elements per side,
 50-500 LSRK(5,4) steps, FP32 bulk) is replayed against the serving loop; the line
 reports p50/p99 latency and solves/s beside the DOF-update rate.
 
-Multi-GPU (torchrun): every rank runs an independent replica of the workload (the
-single-grid path has no cross-rank exchange on one rank); time is the max over ranks.
+Multi-GPU (torchrun): the workload's elements are partitioned over the ranks, which
+exchange face traces before every stage (strong scaling; `--replicas` runs one
+independent replica per rank instead); time is the max over ranks.
+
+The default line also carries the FP32-bulk form of the same workload timed in the same
+process (`fp32_bulk`), its accuracy against the FP64 form and the exact solution after
+`--accuracy-steps` steps, and a short serving stream (`serving`).
 """
 
 import argparse
@@ -282,9 +287,15 @@ def kernel_name(w, dg):
     return "stage_kernel (fused volume + surface + LSRK stage)"
 
 
-def fp64_comparison(rb, w, grid, law, dg, q0, dt, steps, device):
+def rel_max_norm(rb, dg, a, b):
+    """max |a| / max |b| through the library's max-norm (weightednorm(dg, q, Inf))."""
+    return rb.weightednorm(dg, a, math.inf) / rb.weightednorm(dg, b, math.inf)
+
+
+def fp64_comparison(rb, w, grid, law, dg, q0, dt, steps, device, exact=None):
     """The FP32-bulk run against an FP64 run on the same grid from the same state, every
-    100 steps (untimed): relative L2 (MJ-weighted) and max-norm differences."""
+    100 steps (untimed): relative L2 (MJ-weighted) and max-norm differences.  With
+    `exact(t)` (the exact state at time t) both runs' errors against it at the end."""
     form = rb.FluxDifferencingForm(rb.KennedyGruberFlux() if w["vflux"] == "kg" else rb.EntropyConservativeFlux())
     dg64 = rb.DGSEM(law=law, grid=grid, volume_form=form, surface_numericalflux=rb.RusanovFlux(), precision="fp64",
                     device=device)
@@ -299,14 +310,87 @@ def fp64_comparison(rb, w, grid, law, dg, q0, dt, steps, device):
         diff = q64.copy()
         diff.data.sub_(q32.data)
         rows.append({"step": done, "l2_diff_relative": rb.weightednorm(dg64, diff) / rb.weightednorm(dg64, q64),
-                     "max_diff_relative": float(diff.data.abs().max().item() / q64.data.abs().max().item())})
+                     "max_diff_relative": rel_max_norm(rb, dg64, diff, q64)})
         del diff
     I0 = rb.integrals(dg64, rb.GridArray.from_numpy(q0))
     I32, I64 = rb.integrals(dg64, q32), rb.integrals(dg64, q64)
     out = {"every_100_steps": rows,
            "conservation_drift_fp32bulk": [abs(a - b) / max(abs(b), abs(I0[0])) for a, b in zip(I32, I0)],
            "conservation_drift_fp64": [abs(a - b) / max(abs(b), abs(I0[0])) for a, b in zip(I64, I0)]}
+    if exact is not None:
+        qe = rb.GridArray.from_numpy(exact(done * dt))
+        errs = {}
+        for name, q in (("fp32bulk", q32), ("fp64", q64)):
+            d = qe.copy()
+            d.data.sub_(q.data)
+            errs[name] = (rb.weightednorm(dg64, d), rel_max_norm(rb, dg64, d, qe))
+            del d
+        out.update({"steps": done,
+                    "l2_error_vs_exact_fp32bulk": errs["fp32bulk"][0], "l2_error_vs_exact_fp64": errs["fp64"][0],
+                    "l2_error_ratio_fp32bulk_over_fp64": errs["fp32bulk"][0] / errs["fp64"][0],
+                    "max_error_vs_exact_relative_fp32bulk": errs["fp32bulk"][1],
+                    "max_error_vs_exact_relative_fp64": errs["fp64"][1]})
+        del qe
     del q32, q64, dq32, dq64, dg64
+    return out
+
+
+def timed_steps(dg, q, dq, t0, dt, steps, stream, barrier, dist):
+    """Device time (ms) of `steps` LSRK(5,4) steps on `stream`, CUDA events bracketed by a
+    barrier and a synchronize on both sides, max over ranks."""
+    import torch
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    dg.lsrk54_steps(q, dq, t0, dt, steps)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms
+
+
+def fp32_bulk_leg(rb, w, grid, law, q0, dt, args, ms64, local, stream, barrier, dist, world):
+    """The FP32-bulk form of the same workload in the same process: the same grid,
+    initial state, steps and timing as the FP64 line, then (untimed) its accuracy
+    against the FP64 form and the exact solution after `--accuracy-steps` steps."""
+    from raven_b200 import initial_conditions as ic
+
+    w32 = dict(w, precision="fp32_bulk")
+    dg32 = rb.DGSEM(law=law, grid=grid, volume_form=rb.FluxDifferencingForm(rb.KennedyGruberFlux()),
+                    surface_numericalflux=rb.RusanovFlux(), precision="fp32_bulk", device=local)
+    q = rb.GridArray.from_numpy(q0)
+    dq = q.similar()
+    dg32.lsrk54_steps(q, dq, 0.0, dt, args.warmup)
+    ms = timed_steps(dg32, q, dq, args.warmup * dt, dt, args.steps, stream, barrier, dist)
+    del q, dq
+    nodes, ns = grid.np * grid.E, law.ns
+    peak, peak_kind = measured_peaks()
+    bytes_launch = stage_bytes_per_launch(w32, nodes, ns)
+    achieved = bytes_launch / (ms / 1e3 / (5 * args.steps)) / 1e9
+    out = {
+        "workload": args.workload.replace("fp64", "fp32bulk"),
+        "precision": "fp32_bulk: FP32 volume/surface arithmetic, FP64 geometry, state and reductions, FP32 register",
+        "ms_per_step": ms / args.steps,
+        "value": world * nodes * ns * 5 * args.steps / (ms / 1e3),
+        "unit": UNIT,
+        "speedup_vs_fp64": ms64 / ms,
+        "gpu_launches": 5 * args.steps,
+        "kernel": kernel_name(w32, dg32),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "algorithmic_bytes_per_launch": bytes_launch,
+                     "traffic": profiled_traffic(args.workload.replace("fp64", "fp32bulk"))},
+    }
+    if args.accuracy_steps > 0:
+        u0 = 0.5 * math.sqrt(law.gamma)
+        exact = lambda t: ic.isentropic_vortex(grid, law, beta=5.0, u0=u0, center=(w["L"] / 2, w["L"] / 2), t=t)
+        out["accuracy"] = fp64_comparison(rb, w32, grid, law, dg32, q0, dt, args.accuracy_steps, local, exact=exact)
+    del dg32
     return out
 
 
@@ -335,82 +419,83 @@ def adapted_oracle(w):
     return og, law, np.asfortranarray(q), f"the adapted grid itself ({grid.E} elements, {grid.mortars.shape[1]} mortars)"
 
 
-def cpu_sample(w, max_seconds=20.0):
-    """The oracle (C++ FP64 restatement) on the host cores: LSRK(5,4) steps of the same
-    element type, law and flux on a small brick, repeated for up to ~max_seconds."""
+def oracle_workload(w):
+    """The workload's own grid, law and initial state on the oracle (C++ FP64
+    restatement of Raven's CPU path): the same elements, order and data the GPU steps."""
     import oracle as O
 
-    dim, N = w["dim"], w["N"]
-    K = 8 if dim == 3 else 16
+    O.build()
+    dim, N, K, L = w["dim"], w["N"], w["K"], w["L"]
+    if w.get("adapted"):
+        return adapted_oracle(w)
     warp = O.WARP_SINE if w["warp"] else O.WARP_NONE
-    if w.get("adapted"):
-        og, law, q, where = adapted_oracle(w)
-    else:
-        og = O.Grid(dim, N + 1, [K] * dim, [0.0] * dim, [w["L"]] * dim, [True] * dim, warp, 0.1)
-        where = f"a {K}^{dim}-element periodic brick"
-    if w.get("adapted"):
-        pass
-    elif w["law"] == "euler":
+    og = O.Grid(dim, N + 1, [K] * dim, [0.0] * dim, [L] * dim, [True] * dim, warp, 0.1)
+    where = f"the workload's own {K}^{dim}-element periodic {'warped ' if w['warp'] else ''}brick"
+    if w["law"] == "euler":
         law = O.Law(O.LAW_EULER, dim, form=O.FORM_FLUXDIFF, volume_flux=O.FLUX_KG)
-        q = og.initial_condition(law, 4, [5.0, 0.5 * math.sqrt(1.4), w["L"] / 2, w["L"] / 2])
+        q = og.initial_condition(law, 4, [5.0, 0.5 * math.sqrt(1.4), L / 2, L / 2])
     else:
         law = O.Law(O.LAW_ADVECTION, dim, adv=list(ADV_VELOCITY[:dim]))
         q = og.initial_condition(law, 3, [0.05, 0.5, 0.5, 0.5])
+    return og, law, q, where
+
+
+def time_oracle_steps(og, law, q, warmup, steps, budget_s):
+    """Untimed warm-up steps, then up to `steps` timed LSRK(5,4) steps of the oracle on
+    its grid, stopping early once `budget_s` seconds of timed work have been spent (at
+    least one step).  Returns (timed steps, seconds)."""
     dq = og.state(law)
     dt = 1e-4
-    steps, t0 = 0, time.perf_counter()
-    while True:
-        og.lsrk54_step(law, q, dq, steps * dt, dt)
-        steps += 1
-        if time.perf_counter() - t0 >= max_seconds or steps >= 1000:
+    for i in range(warmup):
+        og.lsrk54_step(law, q, dq, i * dt, dt)
+    n, t0 = 0, time.perf_counter()
+    while n < steps:
+        og.lsrk54_step(law, q, dq, (warmup + n) * dt, dt)
+        n += 1
+        if time.perf_counter() - t0 >= budget_s:
             break
-    el = time.perf_counter() - t0
+    return n, time.perf_counter() - t0
+
+
+def cpu_sample(w, max_seconds=20.0):
+    """The oracle (C++ FP64 restatement) on the host cores: LSRK(5,4) steps on the
+    workload's own grid and initial state (one untimed warm-up step, then timed steps
+    until ~max_seconds have passed)."""
+    import oracle as O
+
+    og, law, q, where = oracle_workload(w)
+    steps, el = time_oracle_steps(og, law, q, 1, 1000, max_seconds)
     nodes = og.np * og.E
     return {
         "value": nodes * law.ns * 5 * steps / el,
         "unit": UNIT,
         "cores": O.num_threads(),
         "kind": "port",
-        "sample": f"{steps} LSRK(5,4) steps of the same scheme (dim {dim}, N {N}, {w['vflux']}, "
-                  f"{'warped' if w['warp'] else 'brick'}) on {where}, FP64, "
-                  f"OpenMP over elements, {el:.1f} s",
+        "sample": f"{steps} LSRK(5,4) steps (after 1 untimed) of the same scheme (dim {w['dim']}, N {w['N']}, "
+                  f"{w['vflux']}) on {where} ({og.E} elements), FP64, OpenMP over elements, {el:.1f} s",
     }
 
 
+# timed seconds the reference arm spends at most (its warm-up is one step)
+REFERENCE_BUDGET_S = 150.0
+
+
 def run_reference(args, w):
+    """Reference arm: Raven's CPU path restated (the oracle port; Raven is a Julia package
+    and no Julia exists on these machines) on the workload's own grid and initial state,
+    all host threads.  Timed LSRK(5,4) steps stop early once REFERENCE_BUDGET_S seconds
+    have been spent; `timed_steps` says how many ran."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     import oracle as O
 
-    O.build()
-    dim, N = w["dim"], w["N"]
-    # per-step sample size: keep (warmup + steps) * step time within ~2 minutes
-    K = {3: 4, 2: 8}[dim]
-    warp = O.WARP_SINE if w["warp"] else O.WARP_NONE
-    if w.get("adapted"):
-        og, law, q, where = adapted_oracle(w)
-    else:
-        og = O.Grid(dim, N + 1, [K] * dim, [0.0] * dim, [w["L"]] * dim, [True] * dim, warp, 0.1)
-        where = f"a {K}^{dim}-element periodic brick"
-    if w.get("adapted"):
-        pass
-    elif w["law"] == "euler":
-        law = O.Law(O.LAW_EULER, dim, form=O.FORM_FLUXDIFF, volume_flux=O.FLUX_KG)
-        q = og.initial_condition(law, 4, [5.0, 0.5 * math.sqrt(1.4), w["L"] / 2, w["L"] / 2])
-    else:
-        law = O.Law(O.LAW_ADVECTION, dim, adv=list(ADV_VELOCITY[:dim]))
-        q = og.initial_condition(law, 3, [0.05, 0.5, 0.5, 0.5])
-    dq = og.state(law)
-    dt = 1e-4
-    for i in range(args.warmup):
-        og.lsrk54_step(law, q, dq, i * dt, dt)
-    t0 = time.perf_counter()
-    for i in range(args.steps):
-        og.lsrk54_step(law, q, dq, i * dt, dt)
-    el = time.perf_counter() - t0
+    og, law, q, where = oracle_workload(w)
+    n, el = time_oracle_steps(og, law, q, min(args.warmup, 1), args.steps, REFERENCE_BUDGET_S)
     nodes = og.np * og.E
-    value = nodes * law.ns * 5 * args.steps / el
+    value = nodes * law.ns * 5 * n / el
+    cfg = config_json(args.workload, w)
+    cfg["elements"], cfg["nodes"] = og.E, nodes
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -418,21 +503,23 @@ def run_reference(args, w):
         "unit": UNIT,
         "n_gpus": args.gpus,
         "steps": args.steps,
+        "timed_steps": n,
         "warmup": args.warmup,
-        "ms_per_step": el / args.steps * 1e3,
+        "ms_per_step": el / n * 1e3,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": config_json(args.workload, w),
+        "config": cfg,
         "cpu_baseline": {
             "value": value,
             "unit": UNIT,
             "cores": O.num_threads(),
             "kind": "port",
-            "sample": f"each step: one LSRK(5,4) step of the same scheme on {where} "
-                      f"(N {N}), FP64 C++ restatement of Raven's CPU path, OpenMP over elements",
+            "sample": f"{n} of {args.steps} LSRK(5,4) steps (after {min(args.warmup, 1)} untimed; the timed steps "
+                      f"stop after {REFERENCE_BUDGET_S:.0f} s) of the same scheme on {where} ({og.E} elements, "
+                      f"N {w['N']}), FP64 C++ restatement of Raven's CPU path, OpenMP over elements",
         },
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -484,6 +571,57 @@ def serve_cpu_sample(arrivals, max_seconds=20.0):
     }
 
 
+def serving_warm_specs(rb, S):
+    """One short solve per class of the stream: creates the class, captures its graphs
+    and lets the autotuner pick its tile."""
+    warm = []
+    for dim in (2, 3):
+        for nq in (4, 6, 8):
+            for law in (0, 1):
+                f = S.vortex_spec if law == 1 else S.wave_spec
+                warm.append(f(dim, nq, (4,) * dim if dim == 3 else (8, 8), 10,
+                              precision=rb._lib.PRECISION_FP32_BULK))
+    return warm
+
+
+def serving_leg(rb, local, requests, rates, seed):
+    """A short seeded stream of the serving workload (config 4's generator) replayed at
+    each arrival rate in `rates` against one warm server: p50/p99 latency (submit to
+    final state on the host), solves/s and DOF updates/s per rate."""
+    import numpy as np
+
+    from raven_b200 import serving as S
+
+    srv = S.Server(arena_bytes=48 << 30, device=local)
+    try:
+        for t in [srv.submit(sp, keep_result=False) for sp in serving_warm_specs(rb, S)]:
+            srv.wait(t)
+        out = []
+        for rate in rates:
+            arrivals = S.poisson_mix(seed, requests, rate=rate)
+            t0 = time.perf_counter()
+            res = S.run_load(srv, arrivals, keep_results=True)
+            wall = time.perf_counter() - t0
+            lat = res["latencies"]
+            dof = float(sum(a.spec.dof_updates() for a in arrivals))
+            out.append({
+                "arrival_rate_per_s": rate,
+                "requests": requests,
+                "seed": seed,
+                "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                "mean_ms": float(lat.mean() * 1e3),
+                "max_ms": float(lat.max() * 1e3),
+                "solves_per_s": requests / wall,
+                "dof_updates_per_s": dof / wall,
+                "offered_dof_updates_per_s": dof / max(arrivals[-1].t, 1e-9),
+                "seconds": wall,
+            })
+        return out
+    finally:
+        srv.close()
+
+
 def run_serving(args):
     """The serving loop under the seeded Poisson stream (one server per GPU; replicas)."""
     import numpy as np
@@ -509,15 +647,7 @@ def run_serving(args):
 
     arrivals = S.poisson_mix(args.seed, args.requests, rate=args.rate)
     srv = S.Server(arena_bytes=48 << 30, device=local)
-    # warm-up: one short solve per class of the stream (creates the class, captures its
-    # graphs and lets the autotuner pick its tile), then W more rounds of the same
-    warm = []
-    for dim in (2, 3):
-        for nq in (4, 6, 8):
-            for law in (0, 1):
-                f = S.vortex_spec if law == 1 else S.wave_spec
-                warm.append(f(dim, nq, (4,) * dim if dim == 3 else (8, 8), 10,
-                              precision=rb._lib.PRECISION_FP32_BULK))
+    warm = serving_warm_specs(rb, S)
     for _ in range(max(1, args.warmup)):
         for t in [srv.submit(sp, keep_result=False) for sp in warm]:
             srv.wait(t)
@@ -781,7 +911,15 @@ def main(argv=None):
                    help="override the workload's elements per side (smaller cases for profiling)")
     p.add_argument("--sharded", action="store_true",
                    help="partition the workload's elements over the ranks (face-trace exchange between "
-                        "stages, strong scaling) instead of running one replica per rank")
+                        "stages, strong scaling); the default when more than one rank runs")
+    p.add_argument("--replicas", action="store_true",
+                   help="with more than one rank: one independent replica of the workload per rank instead "
+                        "of the element partition")
+    p.add_argument("--accuracy-steps", type=int, default=1000,
+                   help="steps of the untimed FP32-bulk vs FP64 accuracy comparison (0: skip)")
+    p.add_argument("--no-fp32-leg", action="store_true", help="skip the FP32-bulk sub-measurement")
+    p.add_argument("--serving-requests", type=int, default=40,
+                   help="requests of the short serving stream of the default line (0: skip)")
     args = p.parse_args(argv)
     if args.workload == SERVE_WORKLOAD:
         return run_serving(args)
@@ -790,7 +928,8 @@ def main(argv=None):
         w["K"] = int(args.elements_per_side)
     if args.impl == "reference":
         return run_reference(args, w)
-    if args.sharded:
+    multi = int(os.environ.get("WORLD_SIZE", "1")) > 1 or args.gpus > 1
+    if args.sharded or (multi and not args.replicas and not w.get("adapted")):
         return run_sharded(args, w)
 
     import numpy as np
@@ -826,21 +965,21 @@ def main(argv=None):
     sampler = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local)
     sampler.start()
     time.sleep(0.3)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier()
-    e0.record(stream)
-    dg.lsrk54_steps(q, dq, args.warmup * dt, dt, args.steps)
-    e1.record(stream)
-    e1.synchronize()
-    barrier()
+    ms = timed_steps(dg, q, dq, args.warmup * dt, dt, args.steps, stream, barrier, dist)
     sampler.stop()
-    ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
     value = world * nodes * ns * 5 * args.steps / (ms / 1e3)
     launches = 5 * args.steps
+
+    # the FP32-bulk form of the same workload, timed the same way in the same process
+    fp32_leg = None
+    if (w["law"] == "euler" and w["precision"] == "fp64" and not w["warp"] and not w.get("adapted")
+            and not args.no_fp32_leg):
+        sampler32 = ClockSampler(torch.cuda.current_device() if "CUDA_VISIBLE_DEVICES" not in os.environ else local)
+        sampler32.start()
+        time.sleep(0.3)
+        fp32_leg = fp32_bulk_leg(rb, w, grid, law, q0, dt, args, ms, local, stream, barrier, dist, world)
+        sampler32.stop()
+        fp32_leg["clocks"] = sampler32.summary()
 
     # accuracy of the run: L2 distance to the exactly advected vortex, and conservation
     l2_err = None
@@ -860,7 +999,7 @@ def main(argv=None):
         diff.data.sub_(q.data)
         fp64_cmp = {
             "l2_diff_vs_fp64_relative": rb.weightednorm(dg64, diff) / rb.weightednorm(dg64, q64),
-            "max_diff_vs_fp64_relative": float(diff.data.abs().max().item() / q64.data.abs().max().item()),
+            "max_diff_vs_fp64_relative": rel_max_norm(rb, dg64, diff, q64),
             # |integral(t) - integral(0)| over max(|integral(0)|, mass): the momenta start at 0
             "conservation_drift_fp32bulk": [abs(a - b) / max(abs(b), abs(I0[0])) for a, b in zip(I32, I0)],
             "conservation_drift_fp64": [abs(a - b) / max(abs(b), abs(I0[0])) for a, b in zip(I64, I0)],
@@ -878,13 +1017,13 @@ def main(argv=None):
         T = (args.warmup + args.steps) * dt
         qe = rb.GridArray.from_numpy(ic.isentropic_vortex(grid, law, beta=5.0, u0=0.5 * math.sqrt(law.gamma),
                                                           center=(w["L"] / 2, w["L"] / 2), t=T))
-        qmax = float(qe.data.abs().max().item())
+        qmax = rb.weightednorm(dg, qe, math.inf)
         qe.data.sub_(q.data)
         l2_err = rb.weightednorm(dg, qe)
         I0, I1 = rb.integrals(dg, rb.GridArray.from_numpy(q0)), rb.integrals(dg, q)
         accuracy = {
             "l2_error_vs_exact": l2_err,
-            "max_error_vs_exact_relative": float(qe.data.abs().max().item()) / qmax,
+            "max_error_vs_exact_relative": rb.weightednorm(dg, qe, math.inf) / qmax,
             # |integral(t) - integral(0)| over max(|integral(0)|, mass): the vortex's z momentum is 0
             "conservation_drift": [abs(a - b) / max(abs(b), abs(I0[0])) for a, b in zip(I1, I0)],
             "steps": args.warmup + args.steps,
@@ -914,6 +1053,8 @@ def main(argv=None):
             "h2d_bytes_per_step": nodes * ns * 8,
             "d2h_bytes_per_step": nodes * ns * 8,
             "ms_per_step": e2e_s / args.e2e_steps * 1e3,
+            "note": "rb200_lsrk54_step_host, one synchronous call per step: the whole state is copied in "
+                    "from pinned host memory and back every step, so PCIe copies dominate",
         }
 
     peak, peak_kind = measured_peaks()
@@ -939,6 +1080,15 @@ def main(argv=None):
         tf = flops_node * nodes / (ms / 1e3 / launches) / 1e12
         fp64_pipe = {"achieved": tf, "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s", "frac": tf / FP64_NOMINAL_TFLOPS,
                      "peak_source": "nominal (datasheet)", "flops_per_node_stage": flops_node}
+    # a short serving stream (config 4's generator) on the same GPU, after the timed work
+    serving = None
+    if args.serving_requests > 0 and args.workload == DEFAULT and w["K"] == WORKLOADS[DEFAULT]["K"]:
+        del q, dq
+        serving = {"note": "config 4's seeded stream (FP32 bulk), shortened; latency = submit to final "
+                           "state on the host; at 200/s the stream offers more work than the GPU drains, "
+                           "so latency there includes queueing; the lower rate is below the drain rate",
+                   "streams": serving_leg(rb, local, args.serving_requests, (200.0, 10.0), args.seed)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample(w)
@@ -966,6 +1116,8 @@ def main(argv=None):
             "l2_error_vs_exact": l2_err,
             "accuracy": accuracy,
             "vs_fp64": fp64_cmp,
+            "fp32_bulk": fp32_leg,
+            "serving": serving,
             "dt": dt,
         }
         print(json.dumps(line))

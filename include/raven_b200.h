@@ -146,6 +146,14 @@ rb200_status rb200_unpack_values(const double* buffer, const int64_t* indices, i
  * deterministic (fixed reduction order).  out: host, Ns+1 doubles. */
 rb200_status rb200_weightednorm(rb200_handle* h, const double* q, double* out, void* stream);
 
+/* weightednorm(dg, q, p; componentwise=true) for any p > 0 (measures.jl:6-14) and for
+ * p = Inf (measures.jl:16-21; pass INFINITY): out[s] = (sum(MJ .* abs.(q_s).^p))^(1/p),
+ * or maximum(abs.(q_s)) for p = Inf (unweighted, as in the reference); out[Ns] =
+ * norm(out[0..Ns-1], p).  p = 2 gives rb200_weightednorm's result.  FP64, synchronous,
+ * deterministic (fixed reduction order; NaN propagates through the maximum).  p <= 0 or
+ * NaN: BAD_ARG.  out: host, Ns+1 doubles. */
+rb200_status rb200_weightednorm_p(rb200_handle* h, const double* q, double p, double* out, void* stream);
+
 /* Conservation integrals out[s] = sum(MJ .* q_s)  (FP64, synchronous).  out: host, Ns. */
 rb200_status rb200_integrals(rb200_handle* h, const double* q, double* out, void* stream);
 

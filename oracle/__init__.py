@@ -90,6 +90,8 @@ def lib():
         L.og_solve_rlsrk.argtypes = [P, P, P, ctypes.c_double, ctypes.c_double, P]
         L.og_weightednorm.restype = ctypes.c_double
         L.og_weightednorm.argtypes = [P, P, ctypes.c_int, P]
+        L.og_weightednorm_p.restype = ctypes.c_double
+        L.og_weightednorm_p.argtypes = [P, P, ctypes.c_int, ctypes.c_double, P]
         L.og_integrals.argtypes = [P, P, ctypes.c_int, P]
         L.og_decode8.argtypes = [P, ctypes.c_int64, P]
         L.og_decode16.argtypes = [P, ctypes.c_int64, P]
@@ -254,6 +256,12 @@ class Grid:
     def weightednorm(self, q, ns):
         comp = np.zeros(ns)
         v = lib().og_weightednorm(self.h, _ptr(np.asfortranarray(q)), ns, _ptr(comp))
+        return v, comp
+
+    def weightednorm_p(self, q, ns, p):
+        """weightednorm for any p >= 1 or p = inf: (total, per-field)."""
+        comp = np.zeros(ns)
+        v = lib().og_weightednorm_p(self.h, _ptr(np.asfortranarray(q)), ns, float(p), _ptr(comp))
         return v, comp
 
     def integrals(self, q, ns):

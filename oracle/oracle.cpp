@@ -1256,6 +1256,38 @@ extern "C" double og_weightednorm(const og_grid* g, const double* q, int ns, dou
     return std::sqrt((double)tot);
 }
 
+// weightednorm(dg, q, p; componentwise) for any p >= 1 (measures.jl:6-14) and p = Inf
+// (measures.jl:16-21).  comp[s] = (sum MJ |q_s|^p)^(1/p), or max |q_s| for p = Inf
+// (no weights, as in the reference); the return value is norm(comp, p).
+extern "C" double og_weightednorm_p(const og_grid* g, const double* q, int ns, double p, double* comp) {
+    const int np = g->np;
+    const bool inf = std::isinf(p);
+    double tot = 0.0, mx = 0.0;
+    for (int s = 0; s < ns; ++s) {
+        long double acc = 0;
+        double m = 0.0;
+        for (int64_t e = 0; e < g->E; ++e)
+            for (int n = 0; n < np; ++n) {
+                const double v = std::fabs(q[(size_t)np * ns * e + (size_t)np * s + n]);
+                if (inf) {
+                    if (std::isnan(v) || v > m) m = v;
+                    continue;
+                }
+                const double mj = g->vmet[n + (size_t)np * (g->nvmet - 1 + (size_t)g->nvmet * e)];
+                const double vp = p == 1.0 ? v : (p == 2.0 ? v * v : std::pow(v, p));
+                acc += (long double)(mj * vp);
+            }
+        const double c = inf ? m : (p == 2.0 ? std::sqrt((double)acc) : std::pow((double)acc, 1.0 / p));
+        if (comp) comp[s] = c;
+        if (std::isnan(c) || c > mx) mx = c;
+        tot += p == 1.0 ? c : (p == 2.0 ? c * c : std::pow(c, p));
+    }
+    // norm(n, p) of LinearAlgebra: maximum for Inf, the sum for 1, (sum n^p)^(1/p) else
+    if (inf) return mx;
+    if (p == 1.0) return tot;
+    return p == 2.0 ? std::sqrt(tot) : std::pow(tot, 1.0 / p);
+}
+
 extern "C" void og_integrals(const og_grid* g, const double* q, int ns, double* out) {
     const int np = g->np;
     for (int s = 0; s < ns; ++s) {

@@ -98,6 +98,9 @@ int64_t og_solve(const og_grid* g, const og_law* law, double* q, double dt, doub
 
 /* weightednorm(dg, q, p=2): componentwise sqrt(sum(MJ |q_s|^2)), then the 2-norm. */
 double og_weightednorm(const og_grid* g, const double* q, int ns, double* componentwise);
+/* weightednorm(dg, q, p; componentwise) for p >= 1 or p = INFINITY (measures.jl:6-21):
+ * componentwise[s] = (sum MJ |q_s|^p)^(1/p), max |q_s| for p = Inf; returns norm(., p). */
+double og_weightednorm_p(const og_grid* g, const double* q, int ns, double p, double* componentwise);
 
 /* sum(MJ .* q_s) per field (conservation integrals). */
 void og_integrals(const og_grid* g, const double* q, int ns, double* out);

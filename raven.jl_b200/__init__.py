@@ -411,6 +411,11 @@ class DGSEM:
 # ------------------------------------------------------------------------------- LSRK(5,4)
 
 
+# LSRK(5,4) stage times c_i (odesolvers.jl:181-187), rationals rounded once to Float64
+LSRK54_RKC = (0.0, 1432997174477 / 9575080441755, 2526269341429 / 6820363962896,
+              2006345519317 / 3224310063776, 2802321613138 / 2924317926251)
+
+
 class LSRK54:
     """LSRK54(rhs!, q, dt; t0 = 0) (src/balancelaws/odesolvers.jl:63-66, 32-49)."""
 
@@ -419,11 +424,29 @@ class LSRK54:
         self.dt = float(dt)
         self.time = float(t0)
         self.dq = q.similar()  # fill!(dq, 0)
+        self._stage_out = None
 
-    def dostep(self, q, nsteps=1):
-        """dostep!(q, lsrk) (odesolvers.jl:51-61), `nsteps` times with the same dt."""
-        self.dg.lsrk54_steps(q, self.dq, self.time, self.dt, nsteps)
+    def dostep(self, q, nsteps=1, after_stage=None):
+        """dostep!(q, lsrk, after_stage) (odesolvers.jl:51-61), `nsteps` times with the
+        same dt.  Without `after_stage` the steps run as fused, graph-replayed stage
+        kernels.  With it, every stage is its own kernel (rb200_lsrk54_stage) whose
+        result is written back into `q` before `after_stage(stagetime, q)` is called
+        with stagetime = time + c_i dt, so the callback may read or change q in place,
+        as in the reference."""
+        if after_stage is None:
+            self.dg.lsrk54_steps(q, self.dq, self.time, self.dt, nsteps)
+            for _ in range(nsteps):
+                self.time += self.dt
+            return
+        if self._stage_out is None or self._stage_out.data.shape != q.data.shape:
+            self._stage_out = q.similar()
+        out = self._stage_out
         for _ in range(nsteps):
+            for stage in range(5):
+                stagetime = self.time + LSRK54_RKC[stage] * self.dt
+                self.dg.lsrk54_stage(q, out, self.dq, stage, stagetime, self.dt)
+                q.data.copy_(out.data)
+                after_stage(stagetime, q)
             self.time += self.dt
 
 
@@ -440,8 +463,12 @@ class RLSRK54:
         self.gamma = 1.0
         self.dq = q.similar()  # fill!(dq, 0)
 
-    def dostep(self, q, nsteps=1):
-        """dostep!(q, rlsrk) (odesolvers.jl:118-151), `nsteps` times with the same dt."""
+    def dostep(self, q, nsteps=1, after_stage=None):
+        """dostep!(q, rlsrk) (odesolvers.jl:118-151), `nsteps` times with the same dt.
+        The stages and the relaxation run fused on the device, so a stage callback cannot
+        be honoured: `after_stage` raises instead of being ignored."""
+        if after_stage is not None:
+            raise NotImplementedError("RLSRK54 runs its stages fused on the device; after_stage is not supported")
         g = ctypes.c_double(self.gamma)
         _lib.check(_lib.lib().rb200_rlsrk54_step(self.dg._h, q.ptr(), self.dq.ptr(), ctypes.byref(g), self.time,
                                                  self.dt, int(nsteps), _stream_ptr()), self.dg._h)
@@ -450,16 +477,18 @@ class RLSRK54:
             self.time += self.dt
 
 
-def solve(q, timeend, solver, after_step=None, adjust_final=True):
-    """solve!(q, timeend, solver; after_step, adjust_final) (odesolvers.jl:9-30).
+def solve(q, timeend, solver, after_step=None, after_stage=None, adjust_final=True):
+    """solve!(q, timeend, solver; after_step, after_stage, adjust_final) (odesolvers.jl:9-30).
 
     The reference loop is `time = solver.time; if time + dt >= timeend (dt = timeend -
-    time; final); dostep!; after_step(step, time, q)`.  Here the number of non-final
-    steps is found by replaying the same floating-point time accumulation on the host,
-    and (without an after_step callback) those steps go to the device in one call."""
+    time; final); dostep!(q, solver, after_stage); after_step(step, time, q)`.  Here the
+    number of non-final steps is found by replaying the same floating-point time
+    accumulation on the host, and (without callbacks) those steps go to the device in
+    one call.  With `after_stage`, every stage is a separate kernel followed by the
+    callback (LSRK54.dostep)."""
     step = 0
     while True:
-        if after_step is None:
+        if after_step is None and after_stage is None:
             n, t = 0, solver.time
             while not (t + solver.dt >= timeend):
                 t += solver.dt
@@ -471,7 +500,10 @@ def solve(q, timeend, solver, after_step=None, adjust_final=True):
         final = time + solver.dt >= timeend
         if final and adjust_final:
             solver.dt = timeend - time
-        solver.dostep(q, 1)
+        if after_stage is None:
+            solver.dostep(q, 1)
+        else:
+            solver.dostep(q, 1, after_stage=after_stage)
         step += 1
         if after_step is not None:
             after_step(step, time, q)
@@ -507,11 +539,15 @@ def restore(dg, data, q, solver):
 
 
 def weightednorm(dg, q, p=2, componentwise=False):
-    """weightednorm(dg, q, p=2; componentwise) (src/balancelaws/measures.jl:6-21)."""
-    if p != 2:
-        raise NotImplementedError("only p = 2 is implemented on the device")
+    """weightednorm(dg, q, p=2; componentwise) (src/balancelaws/measures.jl:6-21).
+
+    p = 2 (default), any p > 0, or p = math.inf (Julia's `Inf`): the per-field
+    (sum MJ |q_s|^p)^(1/p), or max |q_s| for p = Inf, then their p-norm."""
     out = (ctypes.c_double * (q.ns + 1))()
-    _lib.check(_lib.lib().rb200_weightednorm(dg._h, q.ptr(), out, _stream_ptr()), dg._h)
+    if p == 2:
+        _lib.check(_lib.lib().rb200_weightednorm(dg._h, q.ptr(), out, _stream_ptr()), dg._h)
+    else:
+        _lib.check(_lib.lib().rb200_weightednorm_p(dg._h, q.ptr(), float(p), out, _stream_ptr()), dg._h)
     vals = list(out)
     return vals[: q.ns] if componentwise else vals[q.ns]
 

@@ -37,6 +37,7 @@ EXPORTED = [
     "rb200_pack_values",
     "rb200_unpack_values",
     "rb200_weightednorm",
+    "rb200_weightednorm_p",
     "rb200_integrals",
     "rb200_entropy_integral",
     "rb200_entropy_product",
@@ -162,6 +163,7 @@ def lib():
     L.rb200_pack_values.argtypes = [P, I64, P, I64, P, P]
     L.rb200_unpack_values.argtypes = [P, P, I64, P, I64, P]
     L.rb200_weightednorm.argtypes = [P, P, P, P]
+    L.rb200_weightednorm_p.argtypes = [P, P, D, P, P]
     L.rb200_integrals.argtypes = [P, P, P, P]
     L.rb200_entropy_integral.argtypes = [P, P, P, P]
     L.rb200_entropy_product.argtypes = [P, P, P, P, P]

@@ -799,6 +799,34 @@ rb200_status rb200_weightednorm(rb200_handle* h, const double* q, double* out, v
     return RB200_OK;
 }
 
+rb200_status rb200_weightednorm_p(rb200_handle* h, const double* q, double p, double* out, void* stream) {
+    if (!h) return RB200_ERR_BAD_ARG;
+    if (!q || !out) return fail(h, RB200_ERR_BAD_ARG, "null pointer");
+    if (std::isnan(p) || p <= 0.0) return fail(h, RB200_ERR_BAD_ARG, "weightednorm: p must be > 0 or Inf");
+    if (p == 2.0) return rb200_weightednorm(h, q, out, stream);
+    DeviceGuard guard(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = launch_weighted_pnorm(q, h->d_elem_geo, h->d_vgeo, h->d_w, h->dim, h->nq, h->ns, h->E_active,
+                                          h->geom, p, h->d_partial, h->red_blocks, h->d_sums, s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "reduction launch");
+    double buf[5];
+    e = cudaMemcpyAsync(buf, h->d_sums, h->ns * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(h, e, "reduction readback");
+    // per field: the sum to the power 1/p (measures.jl:11), or the maximum (:18); then
+    // norm(n, p) over the fields: maximum, sum, or (sum n^p)^(1/p)
+    const bool inf = std::isinf(p);
+    double tot = 0.0, mx = 0.0;
+    for (int f = 0; f < h->ns; ++f) {
+        const double c = inf ? buf[f] : (p == 1.0 ? buf[f] : std::pow(buf[f], 1.0 / p));
+        out[f] = c;
+        if (std::isnan(c) || c > mx) mx = c;
+        tot += p == 1.0 ? c : std::pow(c, p);
+    }
+    out[h->ns] = inf ? mx : (p == 1.0 ? tot : std::pow(tot, 1.0 / p));
+    return RB200_OK;
+}
+
 rb200_status rb200_integrals(rb200_handle* h, const double* q, double* out, void* stream) {
     double buf[2 * 5];
     rb200_status st = sums(h, q, buf, (cudaStream_t)stream);

@@ -129,6 +129,10 @@ int pipelined_curved_blocks_per_sm();
 cudaError_t launch_weighted_sums(const double* q, const double* elem_geo, const double* vgeo, const double* w,
                                  int dim, int nq, int ns, int64_t E, int geom, double* partial, int nblocks,
                                  double* out_dev, cudaStream_t s);
+// weightednorm for p != 2: out_dev[s] = sum MJ |q_s|^p, or max |q_s| for p = Inf.
+cudaError_t launch_weighted_pnorm(const double* q, const double* elem_geo, const double* vgeo, const double* w,
+                                  int dim, int nq, int ns, int64_t E, int geom, double p, double* partial,
+                                  int nblocks, double* out_dev, cudaStream_t s);
 cudaError_t launch_face_vmapP(const int32_t* nbr, int dim, int nq, int64_t E, int64_t* out, cudaStream_t s);
 
 // Entropy measures and the RLSRK(5,4) step (relaxation.cu).  Sums land in out[0..1]

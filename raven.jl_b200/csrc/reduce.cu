@@ -57,6 +57,66 @@ __global__ void __launch_bounds__(kRedThreads) weighted_sums_kernel(const double
     }
 }
 
+// max that keeps a NaN, as Julia's maximum does
+__device__ __forceinline__ double nan_max(double a, double b) { return (isnan(b) || b > a) ? b : a; }
+
+// weightednorm for p != 2 (measures.jl:9-21), same element partition and tree as
+// weighted_sums_kernel.  kind 0: partial[b*ns + s] = sum MJ |q_s|^p; kind 1 (p = Inf):
+// partial[b*ns + s] = max |q_s| (unweighted, as in the reference).
+__global__ void __launch_bounds__(kRedThreads) weighted_pnorm_kernel(const double* __restrict__ q,
+                                                                     const double* __restrict__ elem_geo,
+                                                                     const double* __restrict__ vgeo,
+                                                                     const double* __restrict__ wgt, int dim, int nq,
+                                                                     int ns, int64_t E, int geom, double p, int kind,
+                                                                     double* __restrict__ partial) {
+    __shared__ double red[kRedThreads];
+    const int np = dim == 2 ? nq * nq : nq * nq * nq;
+    const int nvg = dim * dim + 2;
+    for (int s = 0; s < ns; ++s) {
+        double acc = 0.0;
+        for (int64_t e = blockIdx.x; e < E; e += gridDim.x) {
+            for (int n = threadIdx.x; n < np; n += blockDim.x) {
+                const double v = fabs(q[((size_t)e * ns + s) * np + n]);
+                if (kind == 1) {
+                    acc = nan_max(acc, v);
+                    continue;
+                }
+                double mj;
+                if (geom == GEOM_AFFINE) {
+                    const int i = n % nq, j = (n / nq) % nq, k = n / (nq * nq);
+                    mj = wgt[i] * wgt[j];
+                    if (dim == 3) mj = mj * wgt[k];
+                    mj = mj * elem_geo[4 * e + 3];
+                } else {
+                    mj = vgeo[((size_t)e * nvg + dim * dim + 1) * np + n];
+                }
+                acc += mj * (p == 1.0 ? v : pow(v, p));
+            }
+        }
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w)
+                red[threadIdx.x] = kind == 1 ? nan_max(red[threadIdx.x], red[threadIdx.x + w])
+                                             : red[threadIdx.x] + red[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) partial[(size_t)blockIdx.x * ns + s] = red[0];
+        __syncthreads();
+    }
+}
+
+__global__ void finish_pnorm_kernel(const double* __restrict__ partial, int nblocks, int ns, int kind, double* out) {
+    const int v = threadIdx.x;
+    if (v >= ns) return;
+    double acc = 0.0;
+    for (int b = 0; b < nblocks; ++b) {
+        const double x = partial[(size_t)b * ns + v];
+        acc = kind == 1 ? nan_max(acc, x) : acc + x;
+    }
+    out[v] = acc;
+}
+
 __global__ void finish_sums_kernel(const double* __restrict__ partial, int nblocks, int nvals, double* out) {
     const int v = threadIdx.x;
     if (v >= nvals) return;
@@ -140,6 +200,18 @@ cudaError_t launch_weighted_sums(const double* q, const double* elem_geo, const 
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return err;
     finish_sums_kernel<<<1, 32, 0, s>>>(partial, nblocks, 2 * ns, out_dev);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_weighted_pnorm(const double* q, const double* elem_geo, const double* vgeo, const double* w, int dim,
+                                  int nq, int ns, int64_t E, int geom, double p, double* partial, int nblocks,
+                                  double* out_dev, cudaStream_t s) {
+    const int kind = isinf(p) ? 1 : 0;
+    weighted_pnorm_kernel<<<nblocks, kRedThreads, 0, s>>>(q, elem_geo, vgeo, w, dim, nq, ns, E, geom, p, kind,
+                                                          partial);
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    finish_pnorm_kernel<<<1, 32, 0, s>>>(partial, nblocks, ns, kind, out_dev);
     return cudaGetLastError();
 }
 

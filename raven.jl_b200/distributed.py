@@ -299,15 +299,27 @@ class DistributedDGSEM:
         if cur is not q:
             q.data.copy_(cur.data)
 
-    def weightednorm(self, q):
-        """weightednorm over all ranks (measures.jl:6-21): the per-field sums of squares of
-        every rank are added with one all-reduce."""
+    def weightednorm(self, q, p=2, componentwise=False):
+        """weightednorm over all ranks (measures.jl:6-21): each field's sum of MJ |q|^p is
+        added over the ranks with one all-reduce (MPI.SUM), or its maximum |q| taken with
+        one all-reduce (MPI.MAX) for p = Inf; then the p-norm over the fields."""
+        import math
+
         import torch
         import torch.distributed as dist
 
         from . import weightednorm
 
-        per = weightednorm(self.dg, q, componentwise=True)
-        sq = torch.tensor([v * v for v in per], dtype=torch.float64, device=f"cuda:{self.dg.device}")
-        dist.all_reduce(sq, group=self.halo.group)
-        return float(sq.sum().sqrt().item())
+        per = weightednorm(self.dg, q, p, componentwise=True)
+        dev = f"cuda:{self.dg.device}"
+        if math.isinf(p):
+            t = torch.tensor(per, dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX, group=self.halo.group)
+            comp = [float(v) for v in t.tolist()]
+            return comp if componentwise else max(comp)
+        t = torch.tensor([v ** p for v in per], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, group=self.halo.group)
+        comp = [float(v) ** (1.0 / p) for v in t.tolist()]
+        if componentwise:
+            return comp
+        return sum(c ** p for c in comp) ** (1.0 / p)

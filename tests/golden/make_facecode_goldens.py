@@ -40,7 +40,9 @@ def extract(root):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {os.path.basename(__file__)} <path of a Raven.jl checkout>")
+    root = sys.argv[1]
     data = extract(root)
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "facecode_goldens.json")
     with open(dst, "w") as f:

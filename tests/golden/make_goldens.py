@@ -108,7 +108,9 @@ def extract_vmapP(root):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {os.path.basename(__file__)} <path of a Raven.jl checkout>")
+    root = sys.argv[1]
     data = {
         "generator": "tests/golden/make_goldens.py",
         "errors": extract_errors(root),

@@ -114,6 +114,33 @@ def test_norms_and_integrals(rb, cuda_ok, case):
     assert np.allclose(rb.integrals(dg, qg), ints, rtol=1e-12, atol=1e-12 * np.abs(ints).max())
 
 
+@pytest.mark.parametrize("case", CASES[::3], ids=[_id(c) for c in CASES[::3]])
+@pytest.mark.parametrize("p", [1, 3, 2.5, math.inf])
+def test_weightednorm_p(rb, cuda_ok, case, p):
+    """weightednorm(dg, q, p; componentwise) for p != 2 (measures.jl:6-21): the weighted
+    p-sums per field and the unweighted max-norm for p = Inf, 1e-13 against the oracle;
+    the max-norm is an exact maximum, so it matches bit for bit."""
+    og, g, dg, olaw, law = _build(rb, *case)
+    q = initial_state(og, olaw, case[4], seed=6)
+    qg = rb.GridArray.from_numpy(q)
+    tot, comp = og.weightednorm_p(q, law.ns, p)
+    got = rb.weightednorm(dg, qg, p, componentwise=True)
+    if math.isinf(p):
+        assert got == list(comp) and rb.weightednorm(dg, qg, p) == tot
+        assert tot == float(np.abs(q).max())
+    else:
+        assert np.allclose(got, comp, rtol=1e-13, atol=0)
+        assert rb.weightednorm(dg, qg, p) == pytest.approx(tot, rel=1e-13)
+
+
+def test_weightednorm_p_rejects(rb, cuda_ok):
+    og, g, dg, olaw, law = _build(rb, *CASES[0])
+    qg = rb.GridArray.from_numpy(initial_state(og, olaw, CASES[0][4]))
+    for bad in (0, -1, float("nan"), -math.inf):
+        with pytest.raises(rb.RB200Error):
+            rb.weightednorm(dg, qg, bad)
+
+
 @pytest.mark.parametrize("case", CASES[2::2], ids=[_id(c) for c in CASES[2::2]])
 def test_tendency_fp32_bulk(rb, cuda_ok, case):
     dim, nq, K, per, scheme, warp = case

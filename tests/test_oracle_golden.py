@@ -106,3 +106,26 @@ def test_brick_morton_order():
             y |= ((e >> (3 * b + 1)) & 1) << b
             z |= ((e >> (3 * b + 2)) & 1) << b
         assert tuple(t[:, e]) == (x, y, z)
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 2.5, math.inf])
+def test_oracle_weightednorm_p(p):
+    """The oracle's weightednorm(dg, q, p) against numpy, formula by formula
+    (measures.jl:6-21: weighted p-sums per field, unweighted maximum for p = Inf, then
+    LinearAlgebra.norm over the fields)."""
+    g = O.Grid(2, 4, [3, 2], [0.0, 0.0], [1.0, 2.0], [True, True])
+    L = O.Law(O.LAW_EULER, 2)
+    rng = np.random.default_rng(7)
+    q = np.asfortranarray(rng.standard_normal((g.np, L.ns, g.E)))
+    mj = g.volume_metrics()[:, -1, :]
+    tot, comp = g.weightednorm_p(q, L.ns, p)
+    if math.isinf(p):
+        want = [float(np.abs(q[:, s]).max()) for s in range(L.ns)]
+        assert list(comp) == want and tot == max(want)
+    else:
+        want = [float((mj * np.abs(q[:, s]) ** p).sum() ** (1 / p)) for s in range(L.ns)]
+        assert np.allclose(comp, want, rtol=1e-14, atol=0)
+        assert tot == pytest.approx(np.linalg.norm(want, p), rel=1e-14)
+    if p == 2:
+        t2, c2 = g.weightednorm(q, L.ns)
+        assert tot == pytest.approx(t2, rel=1e-15) and np.allclose(comp, c2, rtol=1e-15, atol=0)
