@@ -122,6 +122,11 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
         : "memory");
 }
 
+// Bulk prefetch of `bytes` (multiple of 16, 16-byte aligned) from global memory into L2.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
 }
@@ -292,6 +297,11 @@ __device__ __forceinline__ void fetch_part(const ElemRef& r, int t, double (&geo
 #ifndef RB200_PIPE_MIN8_FP32
 #define RB200_PIPE_MIN8_FP32 3
 #endif
+// L2 prefetch distance (elements of this CTA) for the state and the LSRK register: 0 off;
+// 1 the next element's register; 2 also the state and register of the element after it
+#ifndef RB200_PIPE_PF
+#define RB200_PIPE_PF 0
+#endif
 // unroll factor of the pair loop over partners (8: fully unrolled)
 #ifndef RB200_PIPE_UNROLL_A
 #define RB200_PIPE_UNROLL_A 8
@@ -411,6 +421,16 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q>()))
                 }
             }
             if (rn.e >= 0) fetch_part(rn, t, sm.geo[buf ^ 1], sm.nb[buf ^ 1]);
+        }
+        if constexpr (!BATCH && RB200_PIPE_PF > 0) {
+            // the registers (and state) of the coming elements into L2, so that the late
+            // loads of their stages hit L2 instead of HBM
+            const int64_t ef = es + (int64_t)RB200_PIPE_PF * gridDim.x;
+            if (t == 32 && ef < A.E && (A.mode == MODE_STAGE || A.mode == MODE_TENDENCY_INC)) {
+                const uint32_t dqb = NS * NP * (dq_is_f32 ? 4 : 8);
+                bulk_prefetch_l2(reinterpret_cast<const char*>(A.dq) + (size_t)ef * dqb, dqb);
+                if (RB200_PIPE_PF >= 2) bulk_prefetch_l2(A.q_in + (size_t)ef * NS * NP, qbytes);
+            }
         }
         // the element's state buffers (one state: the kernel parameters)
         const double* const qin_e = BATCH ? sm.ref[buf].q : A.q_in;
