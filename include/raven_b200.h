@@ -255,8 +255,12 @@ rb200_status rb200_get_info(const rb200_handle* h, int64_t* info, int32_t n);
  * loading the library holds until exit; hence ns <= 5 (larger ns returns
  * RB200_ERR_UNSUPPORTED), np <= 512.  The first call on a device looks up the array's
  * device address (cudaGetSymbolAddress, with that device current); make that first call
- * before any stream capture.  All calls share the array: calls that overlap on the GPU
- * (for instance on two streams) race and must be ordered by the caller. */
+ * before any stream capture.  The address is kept per device and CUDA context: after a
+ * device reset (or any new context on the device) the next call looks it up again, so
+ * that call too should come before any stream capture.  q, MJ and sums_out must be device
+ * (or managed) memory usable on the current device; otherwise RB200_ERR_BAD_ARG.  All
+ * calls share the array: calls that overlap on the GPU (for instance on two streams)
+ * race and must be ordered by the caller. */
 rb200_status rb200_weighted_sums_noalloc(const double* q, const double* MJ, int32_t np, int32_t ns,
                                          int64_t num_elements, double* sums_out, void* stream);
 

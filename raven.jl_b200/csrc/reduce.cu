@@ -4,6 +4,8 @@
 // The reductions are deterministic: a fixed number of CTAs each own a fixed,
 // strided set of elements, partial sums are combined in a fixed tree, and a single
 // CTA adds the per-CTA partials in index order.
+#include <cuda.h>  // CUcontext (cuCtxGetCurrent is reached through cudaGetDriverEntryPoint)
+
 #include <mutex>
 
 #include "../../include/raven_b200.h"
@@ -190,6 +192,43 @@ __device__ __align__(256) double g_noalloc_partials[kNoAllocBlocks * 2 * kNoAllo
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mutex;
 double* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
+// the context the address was looked up in: a device reset (or a destroyed and recreated
+// primary context) reloads the module at another address, so a new context means a new
+// lookup
+CUcontext g_noalloc_ctx[kNoAllocMaxDevices] = {nullptr};
+
+using CtxGetCurrent = CUresult (*)(CUcontext*);
+CtxGetCurrent ctx_get_current() {
+    static const CtxGetCurrent fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return static_cast<CtxGetCurrent>(nullptr);
+        }
+        return reinterpret_cast<CtxGetCurrent>(p);
+    }();
+    return fn;
+}
+
+CUcontext current_context() {
+    CUcontext c = nullptr;
+    if (CtxGetCurrent f = ctx_get_current()) {
+        if (f(&c) != CUDA_SUCCESS) c = nullptr;
+    }
+    return c;
+}
+
+// true if p is device (or managed) memory that the current device `dev` can use
+bool on_device(const void* p, int dev) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return (a.type == cudaMemoryTypeDevice && a.device == dev) || a.type == cudaMemoryTypeManaged;
+}
 
 }  // namespace
 
@@ -238,17 +277,23 @@ extern "C" rb200_status rb200_weighted_sums_noalloc(const double* q, const doubl
     if (ns < 1 || ns > kNoAllocMaxFields) return RB200_ERR_UNSUPPORTED;  // beyond the scratch array
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return RB200_ERR_CUDA;
+    // the arrays must be device memory of the current device (a host or foreign-device
+    // pointer would otherwise fail later as an asynchronous launch error)
+    if (!on_device(q, dev) || !on_device(MJ, dev) || !on_device(sums_out, dev)) return RB200_ERR_BAD_ARG;
     double* scratch;
     {
-        // once per device, with that device current: the device address of the array
+        // once per device and context, with that device current: the device address of
+        // the array (looked up again when the current context changed, e.g. after a reset)
         std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-        if (!g_noalloc_ptr[dev]) {
+        const CUcontext ctx = current_context();
+        if (!g_noalloc_ptr[dev] || g_noalloc_ctx[dev] != ctx) {
             void* p = nullptr;
             if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p) {
                 cudaGetLastError();
                 return RB200_ERR_CUDA;
             }
             g_noalloc_ptr[dev] = static_cast<double*>(p);
+            g_noalloc_ctx[dev] = current_context();  // current now, if it was not before the lookup
         }
         scratch = g_noalloc_ptr[dev];
     }

@@ -192,6 +192,7 @@ struct Solve {
     int slot = -1;
     int64_t steps_done = 0;
     SolveDesc desc{};
+    const double* final_state = nullptr;  // set when the last step's tick has completed
 };
 
 struct Class {
@@ -236,13 +237,18 @@ struct rb200_server {
     char* arena_base = nullptr;
     std::unique_ptr<Arena> arena;
     cudaStream_t upload = nullptr;
+    cudaEvent_t uploaded = nullptr;  // recorded after each admission's uploads
+    cudaStream_t download = nullptr;  // copies of finished states to the host
     std::mutex mu;
-    std::condition_variable cv_work, cv_done;
+    std::condition_variable cv_work, cv_done, cv_drain;
     std::deque<std::shared_ptr<Req>> queue;
     std::unordered_map<uint64_t, std::shared_ptr<Req>> reqs;
     std::map<std::string, std::unique_ptr<Class>> classes;
     std::vector<std::unique_ptr<Solve>> running;
-    std::thread loop;
+    // finished solves whose state is being copied to the host: they have left their
+    // class (no tick reads or writes them) and keep their arena space until the copy ends
+    std::deque<std::unique_ptr<Solve>> draining;
+    std::thread loop, completer;
     bool stop = false;
     uint64_t next_ticket = 1;
     std::string err;
@@ -475,7 +481,10 @@ cudaError_t admit(rb200_server* s) {
                 e = cudaGetLastError();
             }
         }
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s->upload);
+        // the class's next tick waits for the uploads on the device; the host does not
+        // (pageable sources are staged by the time cudaMemcpyAsync returns)
+        if (e == cudaSuccess) e = cudaEventRecord(s->uploaded, s->upload);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(c.stream, s->uploaded, 0);
         if (e != cudaSuccess) return e;
         r->geo = std::vector<double>();
         r->nbr = std::vector<int32_t>();
@@ -549,38 +558,77 @@ cudaError_t finish_tick(rb200_server* s, Class& c) {
     }
     c.tick += 1;
     s->ticks += 1;
+    bool status_read = false;
     for (int i = 0; i < kMaxSolvesPerClass; ++i) {
         Solve* sv = c.slots[i];
         if (!sv || sv->desc.start_tick > done_tick) continue;  // admitted while the tick ran
         sv->steps_done += 1;
         Req& r = *sv->req;
         if (sv->steps_done < r.nsteps) continue;
-        const size_t nstate = (size_t)r.np * r.ns * r.E;
-        cudaError_t e = cudaSuccess;
-        if (c.pipelined) {  // a bounded wait of the pipelined kernel gave up: the result is void
+        if (c.pipelined && !status_read) {  // a bounded wait of the pipelined kernel gave up: the result is void
             int32_t status = 0;
-            e = cudaMemcpy(&status, c.d_status, sizeof(status), cudaMemcpyDeviceToHost);
-            if (e == cudaSuccess && status != 0) return cudaErrorTimeout;
+            cudaError_t e = cudaMemcpyAsync(&status, c.d_status, sizeof(status), cudaMemcpyDeviceToHost, c.stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);  // the tick has completed: idle stream
+            if (e != cudaSuccess) return e;
+            if (status != 0) return cudaErrorTimeout;
+            status_read = true;
         }
-        if (e == cudaSuccess && r.q_out)
-            e = cudaMemcpy(r.q_out, sv->desc.q[sv->steps_done & 1], nstate * 8, cudaMemcpyDeviceToHost);
-        if (e != cudaSuccess) return e;
-        r.state = 2;
-        r.t_done = now_s();
-        s->completed += 1;
-        s->last_done = r.t_done;
-        s->dof_updates += (double)nstate * 5.0 * r.nsteps;  // one update per RHS evaluation
-        s->arena->release(sv->off, r.bytes);
+        // the solve leaves its class now (the next tick's chunk table no longer names it)
+        // and its final state goes to the completion thread, which copies it to the host
+        // while the class's next ticks run
+        sv->final_state = sv->desc.q[sv->steps_done & 1];
         c.slots[i] = nullptr;
         c.h_solves[i] = SolveDesc{};
         c.nchunks -= chunks_needed(c, r.E);
         c.active -= 1;
         c.dirty = true;
         auto pos = std::find_if(s->running.begin(), s->running.end(), [&](auto& p) { return p.get() == sv; });
-        if (pos != s->running.end()) s->running.erase(pos);
+        if (pos != s->running.end()) {
+            s->draining.push_back(std::move(*pos));
+            s->running.erase(pos);
+        }
     }
-    s->cv_done.notify_all();
+    s->cv_drain.notify_all();
     return cudaSuccess;
+}
+
+// Completion thread: copies each finished solve's state to its host buffer on the
+// download stream, outside the server lock, then marks the request done and releases its
+// arena space.  Pending copies are finished before the thread exits.
+void completion_loop(rb200_server* s) {
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    while (true) {
+        if (s->draining.empty()) {
+            if (s->stop) break;
+            s->cv_drain.wait(lk);
+            continue;
+        }
+        std::unique_ptr<Solve> sv = std::move(s->draining.front());
+        s->draining.pop_front();
+        Req& r = *sv->req;
+        const size_t nstate = (size_t)r.np * r.ns * r.E;
+        lk.unlock();
+        cudaError_t e = cudaSuccess;
+        if (r.q_out && r.state < 2) {
+            e = cudaMemcpyAsync(r.q_out, sv->final_state, nstate * 8, cudaMemcpyDeviceToHost, s->download);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s->download);
+        }
+        const double t = now_s();
+        lk.lock();
+        if (e != cudaSuccess) {
+            fail_server(s, RB200_ERR_CUDA, std::string("result copy: ") + cudaGetErrorString(e));
+        } else if (r.state < 2) {
+            r.state = 2;
+            r.t_done = t;
+            s->completed += 1;
+            s->last_done = t;
+            s->dof_updates += (double)nstate * 5.0 * r.nsteps;  // one update per RHS evaluation
+        }
+        s->arena->release(sv->off, r.bytes);
+        s->cv_done.notify_all();
+        s->cv_work.notify_all();  // arena space for queued requests
+    }
 }
 
 // Each class advances independently: as soon as a class's tick has completed, its
@@ -639,6 +687,7 @@ void server_loop(rb200_server* s) {
     // drain: no graph of this server may still run when its memory is freed
     for (auto& kv : s->classes)
         if (kv.second->stream) cudaStreamSynchronize(kv.second->stream);
+    if (s->upload) cudaStreamSynchronize(s->upload);
 }
 
 }  // namespace
@@ -656,6 +705,8 @@ rb200_status rb200_server_create(int32_t device, uint64_t arena_bytes, rb200_ser
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaMalloc(&s->arena_base, arena_bytes);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->upload, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->download, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->uploaded, cudaEventDisableTiming);
     cudaSetDevice(prev);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -665,6 +716,7 @@ rb200_status rb200_server_create(int32_t device, uint64_t arena_bytes, rb200_ser
     }
     s->arena = std::make_unique<Arena>(arena_bytes);
     s->loop = std::thread(server_loop, s);
+    s->completer = std::thread(completion_loop, s);
     *out = s;
     return RB200_OK;
 }
@@ -833,8 +885,15 @@ rb200_status rb200_server_destroy(rb200_server* s) {
         s->cv_done.notify_all();
     }
     if (s->loop.joinable()) s->loop.join();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->cv_drain.notify_all();
+    }
+    if (s->completer.joinable()) s->completer.join();  // finishes the copies in flight
     cudaSetDevice(s->device);
     for (auto& kv : s->classes) destroy_class(*kv.second);
+    if (s->uploaded) cudaEventDestroy(s->uploaded);
+    if (s->download) cudaStreamDestroy(s->download);
     if (s->upload) cudaStreamDestroy(s->upload);
     if (s->arena_base) cudaFree(s->arena_base);
     delete s;

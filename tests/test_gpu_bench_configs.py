@@ -3,8 +3,8 @@
 Each test sets up the product path exactly as ``bench.py`` does for one of its workloads
 (``bench.problem`` / ``bench.setup``: the same grid generator, initial data, time step,
 precision and kernel selection) and compares it with the oracle on the same grid and the
-same initial state.  At 32^3 elements the persistent stage kernels walk about 110
-elements per CTA, so the element cursor, the one-element-ahead bulk copies, the mbarrier
+same initial state.  At 32^3 elements each CTA of the persistent stage kernels walks
+70-110 elements, so the element cursor, the one-element-ahead bulk copies, the mbarrier
 phase flips and the double-buffered geometry/neighbour slots are exercised the way the
 bench exercises them, not just on the first element of each CTA.
 
@@ -139,7 +139,7 @@ def test_config2_fp64_one_step(rb, config2):
     c = config2
     assert c.grid.E == 32 ** 3
     assert c.dg.pipelined_ctas > 0, "the bench workload runs the pipelined brick kernel"
-    assert c.grid.E / c.dg.pipelined_ctas > 100, "each CTA walks many elements"
+    assert c.grid.E / c.dg.pipelined_ctas > 50, "each CTA walks many elements"
     q, dq = c.run_product(rb)
     err_q = field_errors(q, c.q_ref, c.law)
     err_dq = register_error(dq, c.dq_ref, term_scale(c.grid, c.law, c.q0))

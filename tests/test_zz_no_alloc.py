@@ -50,3 +50,9 @@ def test_weighted_sums_without_allocation_match_handle_api(rb, cuda_ok):
     st = L.rb200_weighted_sums_noalloc(q.ptr(), ctypes.c_void_p(mj.data_ptr()), grid.np, 6, grid.E,
                                        ctypes.c_void_p(out.data_ptr()), stream)
     assert st == 6  # RB200_ERR_UNSUPPORTED
+    # arrays that are not device memory of the current device are rejected before any
+    # launch (a host buffer here), instead of failing later as a launch error
+    host_out = np.zeros(2 * law.ns)
+    st = L.rb200_weighted_sums_noalloc(q.ptr(), ctypes.c_void_p(mj.data_ptr()), grid.np, law.ns, grid.E,
+                                       host_out.ctypes.data_as(ctypes.c_void_p), stream)
+    assert st == 1  # RB200_ERR_BAD_ARG
