@@ -279,6 +279,8 @@ def kernel_name(w, dg):
         return "batched_stage_kernel (all running solves of a class per launch)"
     if dg.pipelined_ctas > 0:
         if dg.geometry == "curved":
+            if w["precision"] == "fp64":
+                return "pipelined_curved64_kernel (3-D Nq=8 curved, FP64, fused volume + surface + LSRK stage)"
             return "pipelined_curved_kernel (3-D Nq=8 curved, FP32 bulk, fused volume + surface + LSRK stage)"
         extra = " with mortar fluxes" if w.get("adapted") else ""
         if w.get("law") == "advection":

@@ -58,7 +58,7 @@ struct rb200_handle {
     double graph_dt = 0.0;
     int use_graphs = 1;
     int pipe_grid = 0;            // CTAs of the pipelined kernel (0: not eligible)
-    int pipe_curved_grid = 0;     // CTAs of the curved-grid pipelined kernel (0: not eligible)
+    int pipe_curved_grid = 0;     // CTAs of the curved-grid pipelined kernel, FP32 bulk or FP64 (0: not eligible)
     double pipe_S[64] = {0};      // D[a,id] w[a] / w[id] - D[id,a] (advection: D[a,id] w[a] / w[id])
     // mortars of an adapted grid (rb200_set_mortars)
     int64_t nmortars = 0;
@@ -172,7 +172,8 @@ cudaError_t launch_any(rb200_handle* h, const StageArgs& a, cudaStream_t st) {
         std::memset(&c, 0, sizeof(c));
         c.q_in = a.q_in;
         c.q_out = a.q_out;
-        c.dq = static_cast<float*>(a.dq);
+        if (h->prec == RB200_PRECISION_FP64) c.dq64 = static_cast<double*>(a.dq);
+        else c.dq = static_cast<float*>(a.dq);
         c.vgeo = h->d_vgeo;
         c.sgeo = h->d_sgeo;
         c.nbr = h->d_nbr;
@@ -185,7 +186,9 @@ cudaError_t launch_any(rb200_handle* h, const StageArgs& a, cudaStream_t st) {
         c.rkb_dt = a.rkb_dt;
         c.gamma = a.gamma;
         std::memcpy(c.D, h->D, sizeof(c.D));
-        return launch_pipelined_curved(c, (int)std::min<int64_t>(h->pipe_curved_grid, a.E - a.e_begin), st);
+        const int grid = (int)std::min<int64_t>(h->pipe_curved_grid, a.E - a.e_begin);
+        return h->prec == RB200_PRECISION_FP64 ? launch_pipelined_curved64(c, grid, st)
+                                               : launch_pipelined_curved(c, grid, st);
     }
     const bool eligible = h->kernel_path == 0 && h->pipe_grid > 0 && aligned16(a.q_in) && aligned16(a.dq) &&
                           (!stage_mode || aligned16(a.q_out)) &&
@@ -641,12 +644,14 @@ rb200_status rb200_create(const rb200_desc* d, rb200_handle** out) {
         h->pipe_grid = per_sm > 0 ? per_sm * nsm : 0;
         cudaGetLastError();
     }
-    if (dim == 3 && nq == 8 && !affine && h->combo == EUL_KG && h->prec == RB200_PRECISION_FP32_BULK && !entropy_flux &&
-        h->d_vgeo && h->d_sgeo && aligned16(h->d_vgeo) && aligned16(h->d_sgeo)) {
+    if (dim == 3 && nq == 8 && !affine && h->combo == EUL_KG && !entropy_flux && h->d_vgeo && h->d_sgeo &&
+        aligned16(h->d_vgeo) && aligned16(h->d_sgeo)) {
+        // curved 3-D Nq = 8 Kennedy-Gruber: the curved pipelined kernel of the handle's precision
         int dev = 0, nsm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        const int per_sm = pipelined_curved_blocks_per_sm();
+        const int per_sm = h->prec == RB200_PRECISION_FP64 ? pipelined_curved64_blocks_per_sm()
+                                                           : pipelined_curved_blocks_per_sm();
         h->pipe_curved_grid = per_sm > 0 ? per_sm * nsm : 0;
         cudaGetLastError();
     }

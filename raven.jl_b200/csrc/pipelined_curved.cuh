@@ -31,7 +31,8 @@ namespace rb200 {
 struct PipeCurvedArgs {
     const double* q_in;
     double* q_out;
-    float* dq;               // FP32 LSRK register
+    float* dq;               // FP32 LSRK register (FP32-bulk kernel)
+    double* dq64;            // FP64 LSRK register (FP64 kernel)
     const double* vgeo;      // (512, 11, E): wJ dRdX[dir][d] (dir-major), MJI, MJ
     const double* sgeo;      // (4, 384, E): n, wsJ per face node
     const int32_t* nbr;      // (6, E)

@@ -3,6 +3,7 @@
 // the chunks of a serving class (BATCH).
 #include "pipelined_adv.cuh"
 #include "pipelined_curved.cuh"
+#include "pipelined_curved64.cuh"
 #include "pipelined_kernel.cuh"
 
 namespace rb200 {
@@ -142,6 +143,27 @@ cudaError_t launch_pipelined_curved(const PipeCurvedArgs& a, int grid, cudaStrea
     if (err != cudaSuccess) return err;
     kern<<<grid, pipec::NT, sizeof(pipec::Smem), s>>>(a);
     return cudaGetLastError();
+}
+
+// The curved-grid kernel in FP64 (Kennedy-Gruber): two CTAs per SM.
+cudaError_t launch_pipelined_curved64(const PipeCurvedArgs& a, int grid, cudaStream_t s) {
+    auto kern = pipelined_curved64_kernel<EUL_KG>;
+    static std::atomic<uint64_t> configured{0};
+    cudaError_t err = ensure_smem_limit(kern, (int)sizeof(pipec64::Smem), configured);
+    if (err != cudaSuccess) return err;
+    kern<<<grid, pipec64::NT, sizeof(pipec64::Smem), s>>>(a);
+    return cudaGetLastError();
+}
+
+int pipelined_curved64_blocks_per_sm() {
+    auto kern = pipelined_curved64_kernel<EUL_KG>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(pipec64::Smem)) !=
+        cudaSuccess)
+        return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, pipec64::NT, sizeof(pipec64::Smem)) != cudaSuccess)
+        return 0;
+    return n;
 }
 
 int pipelined_curved_blocks_per_sm() {

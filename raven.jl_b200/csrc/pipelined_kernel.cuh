@@ -122,11 +122,6 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
         : "memory");
 }
 
-// Bulk prefetch of `bytes` (multiple of 16, 16-byte aligned) from global memory into L2.
-__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
-}
-
 __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
 }
@@ -182,30 +177,23 @@ struct AuxBuf<float, NPP_> {
     }
 };
 
-// 1: the state double-buffered in shared memory (the stage reads the element's old state
-// there) and the LSRK register bulk-copied in at the element's start, in FP64 too
-#ifndef RB200_PIPE_QDB
-#define RB200_PIPE_QDB 0
-#endif
-
 template <typename T, int Q = 8>
 struct Smem {
     using G = Geo<Q>;
-    static constexpr int QB = RB200_PIPE_QDB ? 2 : 1;                  // state buffers
-    static constexpr bool STAGE_DQ = sizeof(T) == 4 || RB200_PIPE_QDB;  // register in shared memory
-    double q[QB][NS][G::NP];                    // state of the element (TMA destination)
+    double q[NS][G::NP];                        // state of the element (TMA destination)
     AuxBuf<T, G::NPP> aux;                      // per-node partner values
     double slot[NS][G::NSLOT];                  // neighbour trace, then (wsJ * nf) * MJI, per face slot
     T S[3][Q][Q];                               // S_dir[a][id] * drdx_dir of the current element
-    // LSRK register of the element, staged during the volume term (FP32; FP64 with
-    // RB200_PIPE_QDB, otherwise FP64 reads it at the end)
-    __align__(16) T dqs[STAGE_DQ ? NS : 1][STAGE_DQ ? G::NP : 1];
+    // FP32 LSRK register of the element, staged during the volume term.  FP64 reads its
+    // register at the end instead: staging the state or the register in shared memory (by
+    // cp.async or bulk copies, with bulk stores of the results) measured slower, because the
+    // stage is bound by shared-memory bandwidth (the partner loads of the volume term)
+    __align__(16) T dqs[sizeof(T) == 4 ? NS : 1][sizeof(T) == 4 ? G::NP : 1];
     T rs[3][Q];                                 // sum_a S[dir][a][id]
     double geo[2][4];                           // elem_geo of the current / next element
     int32_t nb[2][8];                           // neighbours of the current / next element
     ElemRef ref[2];                             // the current / next element
-    uint64_t bar[QB];                           // arrival of each state buffer
-    uint64_t bard;                              // arrival of the register (bulk copy)
+    uint64_t bar;
 };
 
 __device__ __forceinline__ bool bounded_wait(uint64_t* bar, uint32_t parity) {
@@ -306,40 +294,20 @@ __device__ __forceinline__ void fetch_part(const ElemRef& r, int t, double (&geo
 #ifndef RB200_PIPE_MIN8_FP32
 #define RB200_PIPE_MIN8_FP32 3
 #endif
-// L2 prefetch distance (elements of this CTA) for the state and the LSRK register: 0 off;
-// 1 the next element's register; 2 also the state and register of the element after it
-#ifndef RB200_PIPE_PF
-#define RB200_PIPE_PF 0
-#endif
-// code-shape switches (experiments): face fluxes field by field (1) or with per-side
-// arrays (0); the own e/2, p/2 reloaded after the pair loop (1); the final update read
-// field by field next to its use (1) or all loads first (0)
-#ifndef RB200_PIPE_FACE_LEAN
-#define RB200_PIPE_FACE_LEAN (sizeof(T) == 4)
-#endif
-#ifndef RB200_PIPE_OWN_RELOAD
-#define RB200_PIPE_OWN_RELOAD (sizeof(T) == 4)
-#endif
-#ifndef RB200_PIPE_UPD_STREAM
-#define RB200_PIPE_UPD_STREAM 0
-#endif
 // unroll factor of the pair loop over partners (8: fully unrolled)
 #ifndef RB200_PIPE_UNROLL_A
 #define RB200_PIPE_UNROLL_A 8
 #endif
-template <typename T, int Q = 8, int COMBO = EUL_KG>
+template <typename T, int Q = 8>
 constexpr int pipe_min_ctas() {
     constexpr int m8[2] = {RB200_PIPE_MIN8_FP64, RB200_PIPE_MIN8_FP32}, m6[2] = {RB200_PIPE_MIN6}, m4[2] = {RB200_PIPE_MIN4};
-    // the entropy-conservative pair (logarithmic means) needs more registers: two CTAs
-    // of 256 threads per SM in FP64 at Nq = 8
-    if (Q == 8 && COMBO == EUL_EC && sizeof(T) == 8) return 2;
     return Q == 8 ? m8[sizeof(T) == 4] : Q == 6 ? m6[sizeof(T) == 4] : m4[sizeof(T) == 4];
 }
 
 // NPT nodes per thread: thread t owns nodes t + (Np/NPT)*h, h < NPT, which share i, j
 // (k = k0 + (Nq/NPT)*h), so their z-partners are loaded once.
 template <int COMBO, typename T, int NPT, bool BATCH, int Q = 8>
-__global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q, COMBO>()))
+__global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q>()))
     pipelined_stage_kernel(const __grid_constant__ PipeArgs A, const __grid_constant__ PipeBatch B) {
     using namespace pipe;
     using G = Geo<Q>;
@@ -352,16 +320,13 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q, COMBO>()
     const int ii = t % Q, jj = (t / Q) % Q, k0 = t / (Q * Q);
     const bool stage = A.mode >= MODE_STAGE;
     const bool dq_is_f32 = stage && sizeof(T) == 4;
-    constexpr bool kStageDq = Smem<T, Q>::STAGE_DQ;
-    constexpr int QB = Smem<T, Q>::QB;
-    constexpr bool kBulkDq = RB200_PIPE_QDB != 0;  // the register arrives by one bulk copy
+    constexpr bool kStageDq = sizeof(T) == 4;
     const uint32_t qbytes = NS * NP * sizeof(double);
     const T gm1 = (T)(A.gamma - 1.0), gam = (T)A.gamma;
 
     Cursor<BATCH> cur;  // meaningful in threads 0..9
     if (t == 0) {
-        for (int b = 0; b < QB; ++b) mbar_init(&sm.bar[b], 1);
-        mbar_init(&sm.bard, 1);
+        mbar_init(&sm.bar, 1);
         fence_mbar_init();
     }
     if (t < 10) {
@@ -376,10 +341,10 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q, COMBO>()
     __syncthreads();
 
     if (t == 0 && sm.ref[0].e >= 0) {
-        mbar_expect_tx(&sm.bar[0], qbytes);
-        bulk_g2s(&sm.q[0][0][0], sm.ref[0].q + (size_t)sm.ref[0].e * NS * NP, qbytes, &sm.bar[0]);
+        mbar_expect_tx(&sm.bar, qbytes);
+        bulk_g2s(&sm.q[0][0], sm.ref[0].q + (size_t)sm.ref[0].e * NS * NP, qbytes, &sm.bar);
     }
-    uint32_t phase = 0, phase_d = 0;  // phase: one bit per state buffer
+    uint32_t phase = 0;
     int64_t es = A.e_begin + blockIdx.x;  // one state: the current element, kept in registers
     for (int buf = 0;; buf ^= 1, es += gridDim.x) {
         const int64_t e = BATCH ? sm.ref[buf].e : (es < A.E ? es : -1);
@@ -401,22 +366,21 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q, COMBO>()
             }
         }
         // ---- this element's state
-        const int qb = QB == 2 ? buf : 0;
-        if (__syncthreads_or(!bounded_wait(&sm.bar[qb], (phase >> qb) & 1))) {
+        if (__syncthreads_or(!bounded_wait(&sm.bar, phase))) {
             if (t == 0) atomicExch(A.status, kStatusTimeout);
             return;
         }
-        phase ^= 1u << qb;
+        phase ^= 1;
         // ---- per-node partner values
         T own[NPT][NAUX];
 #pragma unroll
         for (int h = 0; h < NPT; ++h) {
             const int n = t + NT * h;
-            const T rho = (T)sm.q[qb][0][n];
+            const T rho = (T)sm.q[0][n];
             const T rinv = T(1) / rho;
-            const T m0 = (T)sm.q[qb][1][n], m1 = (T)sm.q[qb][2][n], m2 = (T)sm.q[qb][3][n];
+            const T m0 = (T)sm.q[1][n], m1 = (T)sm.q[2][n], m2 = (T)sm.q[3][n];
             const T u0 = m0 * rinv, u1 = m1 * rinv, u2 = m2 * rinv;
-            const T rhoe = (T)sm.q[qb][4][n];
+            const T rhoe = (T)sm.q[4][n];
             const T p = gm1 * (rhoe - (m0 * m0 + m1 * m1 + m2 * m2) * (T(0.5) * rinv));
             if constexpr (COMBO == EUL_KG) {
                 own[h][0] = rho * T(0.5);
@@ -442,30 +406,13 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q, COMBO>()
             if (cur.advance(A, B)) cur.resolve(A, B, rn);
             if (t == 0) {
                 sm.ref[buf ^ 1] = rn;
-                fence_proxy_async();  // the buffers below were last read by the generic proxy
                 if (rn.e >= 0) {
-                    const int nb = QB == 2 ? qb ^ 1 : 0;
-                    mbar_expect_tx(&sm.bar[nb], qbytes);
-                    bulk_g2s(&sm.q[nb][0][0], rn.q + (size_t)rn.e * NS * NP, qbytes, &sm.bar[nb]);
-                }
-                if (kBulkDq && A.mode == MODE_STAGE) {  // this element's register, for the end of the stage
-                    const uint32_t dqb = NS * NP * sizeof(T);
-                    const void* dsrc = reinterpret_cast<const char*>(BATCH ? sm.ref[buf].dq : A.dq) + (size_t)e * dqb;
-                    mbar_expect_tx(&sm.bard, dqb);
-                    bulk_g2s(&sm.dqs[0][0], dsrc, dqb, &sm.bard);
+                    fence_proxy_async();
+                    mbar_expect_tx(&sm.bar, qbytes);
+                    bulk_g2s(&sm.q[0][0], rn.q + (size_t)rn.e * NS * NP, qbytes, &sm.bar);
                 }
             }
             if (rn.e >= 0) fetch_part(rn, t, sm.geo[buf ^ 1], sm.nb[buf ^ 1]);
-        }
-        if constexpr (!BATCH && RB200_PIPE_PF > 0) {
-            // the registers (and state) of the coming elements into L2, so that the late
-            // loads of their stages hit L2 instead of HBM
-            const int64_t ef = es + (int64_t)RB200_PIPE_PF * gridDim.x;
-            if (t == 32 && ef < A.E && (A.mode == MODE_STAGE || A.mode == MODE_TENDENCY_INC)) {
-                const uint32_t dqb = NS * NP * (dq_is_f32 ? 4 : 8);
-                bulk_prefetch_l2(reinterpret_cast<const char*>(A.dq) + (size_t)ef * dqb, dqb);
-                if (RB200_PIPE_PF >= 2) bulk_prefetch_l2(A.q_in + (size_t)ef * NS * NP, qbytes);
-            }
         }
         // the element's state buffers (one state: the kernel parameters)
         const double* const qin_e = BATCH ? sm.ref[buf].q : A.q_in;
@@ -484,7 +431,7 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q, COMBO>()
                 for (int s = 0; s < NS; ++s) cp_async8(&sm.slot[s][slot], qn + s * NP);
             }
         }
-        if (kStageDq && !kBulkDq && A.mode == MODE_STAGE) {  // the element's FP32 register, for the end of the stage
+        if (kStageDq && A.mode == MODE_STAGE) {  // the element's FP32 register, for the end of the stage
             const char* src = reinterpret_cast<const char*>(dq_e) + (size_t)e * NS * NP * sizeof(T);
             char* dst = reinterpret_cast<char*>(&sm.dqs[0][0]);
             for (int c = t; c < NS * NP * (int)sizeof(T) / 16; c += NT) cp_async16(dst + 16 * c, src + 16 * c);
@@ -564,13 +511,13 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q, COMBO>()
 #pragma unroll
             for (int h = 0; h < NPT; ++h) {
                 const int kk = k0 + KS * h;
-                // e/2 and p/2 of the own node again from shared memory: they are not used
-                // in the pair loop and would hold registers across it
-                if constexpr (RB200_PIPE_OWN_RELOAD) {
-                T ov[NAUX];
-                load_aux(ov, t + NT * h);
-                own[h][4] = ov[4];
-                own[h][5] = ov[5];
+                if constexpr (sizeof(T) == 4) {
+                    // FP32: e/2 and p/2 of the own node again from shared memory: they are not
+                    // used in the pair loop and would hold registers across it (80 a thread)
+                    T ov[NAUX];
+                    load_aux(ov, t + NT * h);
+                    own[h][4] = ov[4];
+                    own[h][5] = ov[5];
                 }
                 const T o5 = own[h][5];
                 acc[h][1] = fma(own[h][1], acc[h][0], acc[h][1]);
@@ -600,7 +547,9 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q, COMBO>()
                 for (int s = 0; s < NS; ++s) sm.slot[s][slot] = (double)((T)nfp[s * NFP] * fsc);
                 continue;
             }
-            if constexpr (RB200_PIPE_FACE_LEAN) {
+            if constexpr (sizeof(T) == 4) {
+                // FP32: fluxes field by field from the two sides' primitives, so that no flux
+                // arrays stay live beside the accumulators (80 registers, no spills)
             // q- and its primitives from the staged partner values of the element
             T rm, um0, um1, um2, pm, Em;
             {
@@ -750,61 +699,6 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q, COMBO>()
             }
         }
         __syncthreads();  // #2: face-slot contributions ready
-        if (kBulkDq && A.mode == MODE_STAGE) {
-            if (__syncthreads_or(!bounded_wait(&sm.bard, phase_d))) {
-                if (t == 0) atomicExch(A.status, kStatusTimeout);
-                return;
-            }
-            phase_d ^= 1;
-        }
-#if RB200_PIPE_UPD_STREAM
-        // ---- own nodes: dq = rka*dq + volume - faces (x, y, z order); q_out = q + rkb*dt*dq.
-        // The old state and register are read field by field next to their use, so that
-        // they hold no registers beside the accumulators.
-        const size_t g0 = (size_t)e * NS * NP + t;
-        // distinct buffers (q_in != q_out by contract; dq is read and written at the same
-        // index by the same thread): no aliasing, so loads may move above earlier stores
-        double* __restrict__ const qout_e = BATCH ? sm.ref[buf].q_out : A.q_out;
-        const double* __restrict__ const qin_r = qin_e;
-        const double rkb_dt = BATCH ? sm.ref[buf].rkb_dt : A.rkb_dt;
-#pragma unroll
-        for (int h = 0; h < NPT; ++h) {
-            const int kk = k0 + KS * h;
-            int slots[3] = {-1, -1, -1};
-            if (ii == 0) slots[0] = jj + Q * kk;
-            else if (ii == NQ - 1) slots[0] = NFP + jj + Q * kk;
-            if (jj == 0) slots[1] = 2 * NFP + ii + Q * kk;
-            else if (jj == NQ - 1) slots[1] = 3 * NFP + ii + Q * kk;
-            if (kk == 0) slots[2] = 4 * NFP + ii + Q * jj;
-            else if (kk == NQ - 1) slots[2] = 5 * NFP + ii + Q * jj;
-#pragma unroll
-            for (int s = 0; s < NS; ++s) {
-                const size_t g = g0 + NT * h + s * NP;
-                T dqold = T(0);
-                if (kStageDq && A.mode == MODE_STAGE)
-                    dqold = sm.dqs[kStageDq ? s : 0][kStageDq ? t + NT * h : 0];
-                else if (A.mode == MODE_STAGE || A.mode == MODE_TENDENCY_INC)
-                    dqold = dq_is_f32 ? (T)__ldg(reinterpret_cast<const float*>(dq_e) + g)
-                                      : (T)__ldg(reinterpret_cast<const double*>(dq_e) + g);
-                T v = acc[h][s];
-                if (A.mode == MODE_STAGE) v = (T)A.rka * dqold + v;
-                else if (A.mode == MODE_TENDENCY_INC) v = (T)((double)dqold + (double)v);
-#pragma unroll
-                for (int d = 0; d < 3; ++d)
-                    if (slots[d] >= 0) v = v - (T)sm.slot[s][slots[d]];
-                if (stage) {
-                    double qold;
-                    if constexpr (QB == 2) qold = sm.q[qb][s][t + NT * h];
-                    else qold = __ldg(qin_r + g);
-                    if (dq_is_f32) reinterpret_cast<float*>(dq_e)[g] = (float)v;
-                    else reinterpret_cast<double*>(dq_e)[g] = (double)v;
-                    qout_e[g] = qold + rkb_dt * (double)v;
-                } else {
-                    reinterpret_cast<double*>(dq_e)[g] = (double)v;
-                }
-            }
-        }
-#else
         // ---- own old state and register, read now so that the loads overlap the faces
         const size_t g0 = (size_t)e * NS * NP + t;
         double* const qout_e = BATCH ? sm.ref[buf].q_out : A.q_out;
@@ -816,8 +710,7 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q, COMBO>()
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
                 const size_t g = g0 + NT * h + s * NP;
-                if constexpr (QB == 2) qold[h][s] = stage ? sm.q[qb][s][t + NT * h] : 0.0;
-                else qold[h][s] = stage ? __ldg(qin_e + g) : 0.0;
+                qold[h][s] = stage ? __ldg(qin_e + g) : 0.0;
                 if (kStageDq && A.mode == MODE_STAGE)
                     dqold[h][s] = sm.dqs[kStageDq ? s : 0][kStageDq ? t + NT * h : 0];
                 else if (A.mode == MODE_STAGE || A.mode == MODE_TENDENCY_INC)
@@ -856,7 +749,6 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q, COMBO>()
                 }
             }
         }
-#endif
     }
 }
 

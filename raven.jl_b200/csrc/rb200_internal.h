@@ -124,6 +124,9 @@ struct PipeCurvedArgs;  // pipelined_curved.cuh
 // Persistent pipelined kernel for 3-D Nq = 8 curved grids (FP32 bulk, Kennedy-Gruber, stage modes).
 cudaError_t launch_pipelined_curved(const PipeCurvedArgs& a, int grid, cudaStream_t s);
 int pipelined_curved_blocks_per_sm();
+// The same in FP64 (Kennedy-Gruber, stage modes).
+cudaError_t launch_pipelined_curved64(const PipeCurvedArgs& a, int grid, cudaStream_t s);
+int pipelined_curved64_blocks_per_sm();
 
 // Reductions and face-map expansion (reduce.cu).
 cudaError_t launch_weighted_sums(const double* q, const double* elem_geo, const double* vgeo, const double* w,

@@ -194,3 +194,57 @@ def test_curved_pipelined_fp32_bulk_steps(rb, cuda_ok, warp, per):
     dg.set_kernel_path("auto")
     for s in range(law.ns):
         assert rel_err(qa.numpy()[:, s], qb.numpy()[:, s]) <= 1e-6, s
+
+
+@pytest.mark.parametrize("warp,per", [(O.WARP_SINE, (1, 1, 1)), (O.WARP_SINE, (1, 0, 1)),
+                                      (O.WARP_IDENTITY_CURVED, (1, 1, 0))], ids=["sine", "sine-open-y", "identity"])
+def test_curved_pipelined_fp64_steps(rb, cuda_ok, warp, per):
+    """The curved-grid pipelined kernel in FP64 (Kennedy-Gruber) against the oracle after
+    three steps (1e-12 relative per field, the register 1e-11) on a grid with more
+    elements than CTAs, and against the generic curved kernel after five steps, the last
+    three replayed from a CUDA graph (1e-12)."""
+    og = O.Grid(3, 8, (8, 8, 7), [0.0] * 3, [10.0] * 3, per, warp, 0.1 if warp == O.WARP_SINE else 0.0)
+    g = wrap_oracle_grid(og)
+    law, form = product_scheme(rb, "eul_kg", 3)
+    dg = rb.DGSEM(law=law, grid=g, volume_form=form, surface_numericalflux=rb.RusanovFlux(), precision="fp64")
+    olaw = oracle_law("eul_kg", 3)
+    assert dg.geometry == "curved" and dg.pipelined_ctas > 0 and og.E > dg.pipelined_ctas
+    q = initial_state(og, olaw, "eul_kg", seed=17, amp=0.01)
+    qo, dqo = q.copy(order="F"), og.state(olaw)
+    for i in range(3):
+        og.lsrk54_step(olaw, qo, dqo, i * 1e-3, 1e-3)
+    qg = rb.GridArray.from_numpy(q)
+    solver = rb.LSRK54(dg, qg, 1e-3)
+    solver.dostep(qg, 3)
+    dg.sync_status()
+    for s in range(law.ns):
+        assert rel_err(qg.numpy()[:, s], qo[:, s]) <= 1e-12, s
+    assert rel_err(solver.dq.numpy(), dqo) <= 1e-11
+    qa = rb.GridArray.from_numpy(q)
+    rb.LSRK54(dg, qa, 1e-3).dostep(qa, 5)
+    dg.sync_status()
+    dg.set_kernel_path("generic")
+    qb = rb.GridArray.from_numpy(q)
+    rb.LSRK54(dg, qb, 1e-3).dostep(qb, 5)
+    dg.set_kernel_path("auto")
+    for s in range(law.ns):
+        assert rel_err(qa.numpy()[:, s], qb.numpy()[:, s]) <= 1e-12, s
+
+
+def test_curved_pipelined_fp64_central_surface_flux(rb, cuda_ok):
+    """The FP64 curved pipelined kernel with the central surface flux, one step against
+    the oracle (1e-12)."""
+    og = O.Grid(3, 8, (3, 3, 2), [0.0] * 3, [10.0] * 3, (1, 1, 1), O.WARP_SINE, 0.1)
+    g = wrap_oracle_grid(og)
+    law, form = product_scheme(rb, "eul_kg", 3)
+    dg = rb.DGSEM(law=law, grid=g, volume_form=form, surface_numericalflux=rb.CentralFlux(), precision="fp64")
+    assert dg.pipelined_ctas > 0
+    olaw = O.Law(O.LAW_EULER, 3, form=O.FORM_FLUXDIFF, volume_flux=O.FLUX_KG, surface_flux=O.FLUX_CENTRAL)
+    q = initial_state(og, olaw, "eul_kg", seed=18, amp=0.02)
+    qo, dqo = q.copy(order="F"), og.state(olaw)
+    og.lsrk54_step(olaw, qo, dqo, 0.0, 1e-3)
+    qg = rb.GridArray.from_numpy(q)
+    rb.LSRK54(dg, qg, 1e-3).dostep(qg, 1)
+    dg.sync_status()
+    for s in range(law.ns):
+        assert rel_err(qg.numpy()[:, s], qo[:, s]) <= 1e-12, s
