@@ -204,3 +204,27 @@ def test_config1_exact_100_steps(rb, cuda_ok):
     err_q = field_errors(q, c.q_ref, c.law)
     assert max(err_q) <= FP64_TOL, f"state after 100 steps beyond {FP64_TOL}: {err_q}"
     assert register_error(dq, c.dq_ref, term_scale(c.grid, c.law, c.q0)) <= FP64_DQ_TOL
+
+
+def test_config5_adapted_one_step(rb, cuda_ok):
+    """Config 5 as the bench sets it up: a 4^3 forest refined twice within radius 0.25 of
+    the centre (2:1 balanced, hanging faces coupled by mortars), N = 5, density pulse,
+    FP32 bulk (1e-6 after one step), and the same grid in FP64 (1e-12), against the
+    oracle's mortar restatement on the product's own grid arrays."""
+    w = dict(bench.WORKLOADS["euler3d_kg_n5_adapted_fp32bulk"])
+    grid, law, dg32, q0, dt = bench.setup(rb, w, 0)
+    assert grid.mortars.shape[1] > 0 and dg32.pipelined_ctas > 0
+    og = O.Grid.from_arrays(3, w["N"] + 1, grid.points, grid.volume_metrics, grid.surface_metrics, grid.vmapM,
+                            grid.vmapP, grid.boundarycodes, grid.mortars, grid.tohalves)
+    olaw = oracle_scheme(w)
+    qo, dqo = np.asfortranarray(q0.copy()), og.state(olaw)
+    og.lsrk54_step(olaw, qo, dqo, 0.0, dt)
+    dg64 = rb.DGSEM(law=law, grid=grid, volume_form=rb.FluxDifferencingForm(rb.KennedyGruberFlux()),
+                    surface_numericalflux=rb.RusanovFlux(), precision="fp64", device=0)
+    for dg, tol in ((dg32, FP32_TOL), (dg64, FP64_TOL)):
+        q = rb.GridArray.from_numpy(q0)
+        dq = q.similar()
+        dg.lsrk54_steps(q, dq, 0.0, dt, 1)
+        dg.sync_status()
+        err = field_errors(q.numpy(), qo, law)
+        assert max(err) <= tol, f"{dg.precision} adapted state after one step beyond {tol}: {err}"
