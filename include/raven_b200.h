@@ -104,6 +104,12 @@ rb200_status rb200_tendency(rb200_handle* h, double* dq, const double* q, double
 rb200_status rb200_lsrk54_step(rb200_handle* h, double* q, double* dq, double time, double dt, int32_t nsteps,
                                void* stream);
 
+/* nsteps of dostep!(q, LSRK144(dg, q, dt))  (odesolvers.jl:51-61, 68-71, 191-239): the
+ * same fused stages with the 14-stage, fourth-order low-storage coefficients of
+ * coefficients_lsrk144.  Arguments as for rb200_lsrk54_step. */
+rb200_status rb200_lsrk144_step(rb200_handle* h, double* q, double* dq, double time, double dt, int32_t nsteps,
+                                void* stream);
+
 /* Same as rb200_lsrk54_step for a state held in HOST memory: copies q in, runs the
  * steps, copies q back, synchronously.  The LSRK register lives on the device. */
 rb200_status rb200_lsrk54_step_host(rb200_handle* h, double* q_host, double time, double dt, int32_t nsteps,
@@ -173,6 +179,11 @@ rb200_status rb200_entropy_product(rb200_handle* h, const double* p, const doubl
  * sums per iterate on the host. */
 rb200_status rb200_rlsrk54_step(rb200_handle* h, double* q, double* dq, double* gamma, double time, double dt,
                                 int32_t nsteps, void* stream);
+
+/* `nsteps` steps of RLSRK144(dg, q, dt) (odesolvers.jl:158-161): the relaxation step of
+ * rb200_rlsrk54_step over the 14 LSRK(14,4) stages.  Arguments as for rb200_rlsrk54_step. */
+rb200_status rb200_rlsrk144_step(rb200_handle* h, double* q, double* dq, double* gamma, double time, double dt,
+                                 int32_t nsteps, void* stream);
 
 /* Snapshot / resume of the time-stepper state.  The reference keeps (q, dq, time, dt)
  * in its LSRK struct (odesolvers.jl:32-49; RLSRK adds gamma, :73-84) and has no

@@ -1,4 +1,4 @@
-# RavenB200Ext -- Raven.jl's DGSEM tendency and LSRK(5,4) stepping on libravenb200.so.
+# RavenB200Ext -- Raven.jl's DGSEM tendency and LSRK stepping on libravenb200.so.
 #
 # A package extension for Raven.jl (hooked in through Raven's Project.toml [weakdeps] /
 # [extensions], like RavenCUDAExt: see julia/Project.extension.toml).  It keeps Raven's
@@ -7,7 +7,8 @@
 #   (dg::DGSEM)(dq, q, t; increment)            src/balancelaws/dgsem.jl:84-126
 #   solve!(q, timeend, solver; after_step,       src/balancelaws/odesolvers.jl:9-30
 #          after_stage, adjust_final)
-#   dostep!(q, ::LSRK / ::RLSRK, after_stage)    odesolvers.jl:51-61, 118-151
+#   dostep!(q, ::LSRK / ::RLSRK, after_stage)    odesolvers.jl:51-61, 118-151, for the
+#     5-stage (LSRK54, RLSRK54) and 14-stage (LSRK144, RLSRK144) tables
 #   weightednorm(dg, q, p; componentwise)        src/balancelaws/measures.jl:6-21
 #   entropyintegral, entropyproduct              measures.jl:23-33
 #
@@ -18,8 +19,9 @@
 #   * dostep!(q, solver, f::Function) runs the five stages one by one (rb200_lsrk54_stage),
 #     writes each stage's result back into q and calls f(stagetime, q) after each, as the
 #     reference does; a callback that changes q in place is seen by the next stage;
-#   * RLSRK54 runs its stages, entropy products and relaxation fused in the library; a
-#     stage callback raises an error instead of being ignored.
+#   * LSRK144 has the fused step only, and RLSRK54 / RLSRK144 run their stages, entropy
+#     products and relaxation fused in the library; for these a stage callback raises an
+#     error instead of being ignored.
 #
 # Not run in this repository: no Julia exists on its build or GPU machines.  The Python
 # binding (raven.jl_b200/_lib.py) drives the same entry points in the GPU tests.
@@ -118,8 +120,19 @@ function (b::B200DGSEM)(dq, q, time; increment = true)
     return dq
 end
 
-const B200LSRK = LSRK{FT,AT,5,<:B200DGSEM} where {FT,AT}
-const B200RLSRK = RLSRK{FT,AT,5,<:B200DGSEM} where {FT,AT}
+const B200LSRK = LSRK{FT,AT,NS,<:B200DGSEM} where {FT,AT,NS}
+const B200RLSRK = RLSRK{FT,AT,NS,<:B200DGSEM} where {FT,AT,NS}
+
+# the fused entry points, one per coefficient table of NS stages (ccall takes a constant
+# symbol, so the table is chosen by dispatch)
+const LSRKSig = (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, Float64, Float64, Int32, Ptr{Cvoid})
+const RLSRKSig = (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, Ref{Float64}, Float64, Float64, Int32, Ptr{Cvoid})
+fused_lsrk(::Val{5}, args...) = ccall((:rb200_lsrk54_step, lib), Cint, LSRKSig, args...)
+fused_lsrk(::Val{14}, args...) = ccall((:rb200_lsrk144_step, lib), Cint, LSRKSig, args...)
+fused_lsrk(::Val{NS}, args...) where {NS} = error("raven_b200: no fused LSRK scheme with ", NS, " stages")
+fused_rlsrk(::Val{5}, args...) = ccall((:rb200_rlsrk54_step, lib), Cint, RLSRKSig, args...)
+fused_rlsrk(::Val{14}, args...) = ccall((:rb200_rlsrk144_step, lib), Cint, RLSRKSig, args...)
+fused_rlsrk(::Val{NS}, args...) where {NS} = error("raven_b200: no fused RLSRK scheme with ", NS, " stages")
 
 # solve! (odesolvers.jl:9-30) for the B200 solvers: the same loop, with `nothing` as the
 # default stage callback so that dostep! can run the fused step
@@ -140,11 +153,10 @@ function solve!(q, timeend, solver::Union{B200LSRK,B200RLSRK}; after_step::Funct
     end
 end
 
-# the five stages fused on the device (rb200_lsrk54_step)
-function dostep!(q, lsrk::B200LSRK, ::Nothing)
-    st = ccall((:rb200_lsrk54_step, lib), Cint,
-               (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, Float64, Float64, Int32, Ptr{Cvoid}),
-               lsrk.rhs!.handle, pointer(parent(q)), pointer(parent(lsrk.dq)), lsrk.time, lsrk.dt, 1, stream())
+# all stages fused on the device (rb200_lsrk54_step / rb200_lsrk144_step)
+function dostep!(q, lsrk::LSRK{FT,AT,NS,<:B200DGSEM}, ::Nothing) where {FT,AT,NS}
+    st = fused_lsrk(Val(NS), lsrk.rhs!.handle, pointer(parent(q)), pointer(parent(lsrk.dq)), lsrk.time,
+                    lsrk.dt, 1, stream())
     check(st, lsrk.rhs!.handle)
     lsrk.time += lsrk.dt
 end
@@ -155,7 +167,7 @@ const RKC54 = (0 // 1, 1432997174477 // 9575080441755, 2526269341429 // 68203639
 
 # stage by stage (rb200_lsrk54_stage), after_stage(stagetime, q) after each
 # (odesolvers.jl:51-60)
-function dostep!(q, lsrk::B200LSRK{FT}, after_stage::Function) where {FT}
+function dostep!(q, lsrk::LSRK{FT,AT,5,<:B200DGSEM}, after_stage::Function) where {FT,AT}
     out = similar(parent(q))
     for stage = 1:5
         stagetime = lsrk.time + FT(RKC54[stage]) * lsrk.dt
@@ -171,20 +183,22 @@ function dostep!(q, lsrk::B200LSRK{FT}, after_stage::Function) where {FT}
     lsrk.time += lsrk.dt
 end
 
-# RLSRK54 (odesolvers.jl:118-151): the stages, entropy products and the relaxation solve
-# run in the library; γ is read from and written back to the RLSRK struct
-function dostep!(q, r::B200RLSRK, ::Nothing)
+dostep!(q, lsrk::LSRK{FT,AT,14,<:B200DGSEM}, ::Function) where {FT,AT} =
+    error("raven_b200: LSRK144 runs its stages fused on the device; after_stage is not supported")
+
+# RLSRK54 / RLSRK144 (odesolvers.jl:118-151): the stages, entropy products and the
+# relaxation solve run in the library; γ is read from and written back to the RLSRK struct
+function dostep!(q, r::RLSRK{FT,AT,NS,<:B200DGSEM}, ::Nothing) where {FT,AT,NS}
     γ = Ref(Float64(r.γ))
-    st = ccall((:rb200_rlsrk54_step, lib), Cint,
-               (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, Ref{Float64}, Float64, Float64, Int32, Ptr{Cvoid}),
-               r.rhs!.handle, pointer(parent(q)), pointer(parent(r.dq)), γ, r.time, r.dt, 1, stream())
+    st = fused_rlsrk(Val(NS), r.rhs!.handle, pointer(parent(q)), pointer(parent(r.dq)), γ, r.time, r.dt, 1,
+                     stream())
     check(st, r.rhs!.handle)
     r.γ = γ[]
     r.time += r.dt
 end
 
 dostep!(q, r::B200RLSRK, ::Function) =
-    error("raven_b200: RLSRK54 runs its stages fused on the device; after_stage is not supported")
+    error("raven_b200: RLSRK runs its stages fused on the device; after_stage is not supported")
 
 function entropyintegral(b::B200DGSEM, q)
     out = Ref(0.0)

@@ -81,11 +81,14 @@ def lib():
         L.og_initial_condition.argtypes = [P, P, ctypes.c_int, P, ctypes.c_double, P]
         L.og_tendency.argtypes = [P, P, P, P, ctypes.c_double, ctypes.c_int, ctypes.c_int64, ctypes.c_int64]
         L.og_lsrk54_step.argtypes = [P, P, P, P, ctypes.c_double, ctypes.c_double]
+        L.og_lsrk144_step.argtypes = [P, P, P, P, ctypes.c_double, ctypes.c_double]
         L.og_solve.restype = ctypes.c_int64
         L.og_solve.argtypes = [P, P, P, ctypes.c_double, ctypes.c_double]
         L.og_entropy_sums.argtypes = [P, P, P, P, ctypes.c_double, P, P]
         L.og_rlsrk54_step.restype = ctypes.c_int
         L.og_rlsrk54_step.argtypes = [P, P, P, P, P, ctypes.c_double, ctypes.c_double]
+        L.og_rlsrk144_step.restype = ctypes.c_int
+        L.og_rlsrk144_step.argtypes = [P, P, P, P, P, ctypes.c_double, ctypes.c_double]
         L.og_solve_rlsrk.restype = ctypes.c_int64
         L.og_solve_rlsrk.argtypes = [P, P, P, ctypes.c_double, ctypes.c_double, P]
         L.og_weightednorm.restype = ctypes.c_double
@@ -230,6 +233,9 @@ class Grid:
     def lsrk54_step(self, law, q, dq, time, dt):
         lib().og_lsrk54_step(self.h, ctypes.byref(law.c), _ptr(q), _ptr(dq), time, dt)
 
+    def lsrk144_step(self, law, q, dq, time, dt):
+        lib().og_lsrk144_step(self.h, ctypes.byref(law.c), _ptr(q), _ptr(dq), time, dt)
+
     def solve(self, law, q, dt, timeend):
         return lib().og_solve(self.h, ctypes.byref(law.c), _ptr(q), dt, timeend)
 
@@ -247,6 +253,10 @@ class Grid:
         """One RLSRK(5,4) step in place; gamma is a 1-element float64 array carried
         between steps.  Returns the Newton iterations."""
         return lib().og_rlsrk54_step(self.h, ctypes.byref(law.c), _ptr(q), _ptr(dq), _ptr(gamma), time, dt)
+
+    def rlsrk144_step(self, law, q, dq, gamma, time, dt):
+        """One RLSRK(14,4) step in place (see rlsrk54_step)."""
+        return lib().og_rlsrk144_step(self.h, ctypes.byref(law.c), _ptr(q), _ptr(dq), _ptr(gamma), time, dt)
 
     def solve_rlsrk(self, law, q, dt, timeend):
         gamma = np.ones(1)

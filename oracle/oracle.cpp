@@ -1204,18 +1204,59 @@ static const double RKB[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0
                               1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
                               2277821191437.0 / 14882151754819.0};
 
-extern "C" void og_lsrk54_step(const og_grid* g, const og_law* law, double* q, double* dq, double time,
-                               double dt) {
+// LSRK(14,4) (odesolvers.jl:191-239, coefficients_lsrk144): the reference's Float64
+// literals (rka[1] is the integer 0)
+static const double RKA144[14] = {0.0,
+                                  -0.7188012108672410,
+                                  -0.7785331173421570,
+                                  -0.0053282796654044,
+                                  -0.8552979934029281,
+                                  -3.9564138245774565,
+                                  -1.5780575380587385,
+                                  -2.0837094552574054,
+                                  -0.7483334182761610,
+                                  -0.7032861106563359,
+                                  0.0013917096117681,
+                                  -0.0932075369637460,
+                                  -0.9514200470875948,
+                                  -7.1151571693922548};
+static const double RKB144[14] = {0.0367762454319673, 0.3136296607553959, 0.1531848691869027,
+                                  0.0030097086818182, 0.3326293790646110, 0.2440251405350864,
+                                  0.3718879239592277, 0.6204126221582444, 0.1524043173028741,
+                                  0.0760894927419266, 0.0077604214040978, 0.0024647284755382,
+                                  0.0780348340049386, 5.5059777270269628};
+
+struct LsrkScheme {
+    int stages;
+    const double* a;
+    const double* b;
+};
+static const LsrkScheme kScheme54{5, RKA, RKB}, kScheme144{14, RKA144, RKB144};
+
+// dostep!(q, lsrk, after_stage) (odesolvers.jl:51-61): per stage dq .*= a; rhs!(dq, q);
+// q .+= b dt dq
+static void lsrk_step(const og_grid* g, const og_law* law, const LsrkScheme& sc, double* q, double* dq,
+                      double time, double dt) {
     const int64_t n = (int64_t)g->np * num_states(g, law) * g->E;
-    for (int st = 0; st < 5; ++st) {
-        const double a = RKA[st];
+    for (int st = 0; st < sc.stages; ++st) {
+        const double a = sc.a[st];
 #pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < n; ++i) dq[i] = dq[i] * a;
         og_tendency(g, law, dq, q, time, 1, 0, g->E);
-        const double c = RKB[st] * dt;
+        const double c = sc.b[st] * dt;
 #pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < n; ++i) q[i] = q[i] + c * dq[i];
     }
+}
+
+extern "C" void og_lsrk54_step(const og_grid* g, const og_law* law, double* q, double* dq, double time,
+                               double dt) {
+    lsrk_step(g, law, kScheme54, q, dq, time, dt);
+}
+
+extern "C" void og_lsrk144_step(const og_grid* g, const og_law* law, double* q, double* dq, double time,
+                                double dt) {
+    lsrk_step(g, law, kScheme144, q, dq, time, dt);
 }
 
 extern "C" int64_t og_solve(const og_grid* g, const og_law* law, double* q, double dt, double timeend) {
@@ -1340,9 +1381,10 @@ extern "C" void og_entropy_sums(const og_grid* g, const og_law* law, const doubl
 }
 
 // rkb_full: the b coefficients of the standard Butcher form (odesolvers.jl:91-97)
-static void rkb_full(double* bf) {
-    bf[4] = RKB[4];
-    for (int i = 3; i >= 0; --i) bf[i] = RKA[i + 1] * bf[i + 1] + RKB[i];
+static void rkb_full(const LsrkScheme& sc, double* bf) {
+    const int n = sc.stages;
+    bf[n - 1] = sc.b[n - 1];
+    for (int i = n - 2; i >= 0; --i) bf[i] = sc.a[i + 1] * bf[i + 1] + sc.b[i];
 }
 
 // The relaxation solve r(γ) = η(q0 + γk) - η0 - γ dη = 0 with r'(γ) = v(q0 + γk).k - dη
@@ -1375,24 +1417,23 @@ static int relaxation_newton(Eval eval, double* gamma) {
     return it;
 }
 
-extern "C" int og_rlsrk54_step(const og_grid* g, const og_law* law, double* q, double* dq, double* gamma,
-                               double time, double dt) {
-    (void)time;
+static int rlsrk_step(const og_grid* g, const og_law* law, const LsrkScheme& sc, double* q, double* dq,
+                      double* gamma, double time, double dt) {
     const int64_t n = (int64_t)g->np * num_states(g, law) * g->E;
     std::vector<double> q0(q, q + n), k(n);
-    double bf[5], sums[2];
-    rkb_full(bf);
+    double bf[14], sums[2];
+    rkb_full(sc, bf);
     og_entropy_sums(g, law, q0.data(), nullptr, 0.0, nullptr, sums);
     const double eta0 = sums[0];
     double deta = -0.0;
-    for (int st = 0; st < 5; ++st) {
-        const double a = RKA[st];
+    for (int st = 0; st < sc.stages; ++st) {
+        const double a = sc.a[st];
         for (int64_t i = 0; i < n; ++i) dq[i] = dq[i] * a;
         og_tendency(g, law, k.data(), q, time, 0, 0, g->E);
         for (int64_t i = 0; i < n; ++i) dq[i] = dq[i] + k[i];
         og_entropy_sums(g, law, q, nullptr, 0.0, k.data(), sums);
         deta = deta + bf[st] * dt * sums[1];
-        const double c = RKB[st] * dt;
+        const double c = sc.b[st] * dt;
         for (int64_t i = 0; i < n; ++i) q[i] = q[i] + c * dq[i];
     }
     for (int64_t i = 0; i < n; ++i) k[i] = q[i] - q0[i];
@@ -1405,6 +1446,16 @@ extern "C" int og_rlsrk54_step(const og_grid* g, const og_law* law, double* q, d
     const int its = relaxation_newton(eval, gamma);
     for (int64_t i = 0; i < n; ++i) q[i] = q0[i] + *gamma * k[i];
     return its;
+}
+
+extern "C" int og_rlsrk54_step(const og_grid* g, const og_law* law, double* q, double* dq, double* gamma,
+                               double time, double dt) {
+    return rlsrk_step(g, law, kScheme54, q, dq, gamma, time, dt);
+}
+
+extern "C" int og_rlsrk144_step(const og_grid* g, const og_law* law, double* q, double* dq, double* gamma,
+                                double time, double dt) {
+    return rlsrk_step(g, law, kScheme144, q, dq, gamma, time, dt);
 }
 
 extern "C" int64_t og_solve_rlsrk(const og_grid* g, const og_law* law, double* q, double dt, double timeend,

@@ -92,6 +92,8 @@ void og_tendency(const og_grid* g, const og_law* law, double* dq, const double* 
  * full grid pass 0, E. */
 void og_lsrk54_step(const og_grid* g, const og_law* law, double* q, double* dq, double time,
                     double dt);
+/* One LSRK(14,4) step (odesolvers.jl:191-239), same arguments. */
+void og_lsrk144_step(const og_grid* g, const og_law* law, double* q, double* dq, double time, double dt);
 
 /* Raven's solve!(q, timeend, LSRK54(dg, q, dt)) with adjust_final; returns steps taken. */
 int64_t og_solve(const og_grid* g, const og_law* law, double* q, double dt, double timeend);
@@ -114,6 +116,9 @@ void og_entropy_sums(const og_grid* g, const og_law* law, const double* base, co
  * between steps (1 at the start).  Returns the Newton iterations taken. */
 int og_rlsrk54_step(const og_grid* g, const og_law* law, double* q, double* dq, double* gamma, double time,
                     double dt);
+/* One RLSRK(14,4) step (odesolvers.jl:158-161), same arguments. */
+int og_rlsrk144_step(const og_grid* g, const og_law* law, double* q, double* dq, double* gamma, double time,
+                     double dt);
 
 /* solve!(q, timeend, RLSRK54(dg, q, dt)) with adjust_final; returns steps taken. */
 int64_t og_solve_rlsrk(const og_grid* g, const og_law* law, double* q, double dt, double timeend, double* gamma);

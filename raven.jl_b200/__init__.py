@@ -38,7 +38,8 @@ from .grids import Grid, brick_tree_order, jl_range, lobatto_operators
 __all__ = [
     "LobattoCell", "brick", "BrickGrid", "GridManager", "generate", "Grid", "AdvectionLaw", "EulerLaw",
     "RusanovFlux", "CentralFlux", "KennedyGruberFlux", "EntropyConservativeFlux", "RoeFlux", "MatrixFlux", "WeakForm",
-    "FluxDifferencingForm", "GridArray", "DGSEM", "LSRK54", "RLSRK54", "solve", "weightednorm", "integrals",
+    "FluxDifferencingForm", "GridArray", "DGSEM", "LSRK54", "LSRK144", "RLSRK54", "RLSRK144", "solve",
+    "weightednorm", "integrals",
     "entropyintegral", "entropyproduct", "snapshot", "restore",
     "jl_range", "RB200Error", "brick_tree_order", "adapt", "AdaptRefine", "AdaptNone", "AdaptCoarsen",
     "ForestGrid",
@@ -394,6 +395,11 @@ class DGSEM:
         _lib.check(_lib.lib().rb200_lsrk54_step(self._h, q.ptr(), dq.ptr() if dq is not None else None,
                                                 float(time), float(dt), int(nsteps), _stream_ptr()), self._h)
 
+    def lsrk144_steps(self, q, dq, time, dt, nsteps):
+        """nsteps LSRK(14,4) steps (odesolvers.jl:191-239), fused stages."""
+        _lib.check(_lib.lib().rb200_lsrk144_step(self._h, q.ptr(), dq.ptr() if dq is not None else None,
+                                                 float(time), float(dt), int(nsteps), _stream_ptr()), self._h)
+
     def lsrk54_steps_host(self, q_host, time, dt, nsteps):
         """nsteps LSRK(5,4) steps on a host array (Np, Ns, E) column-major, in place."""
         if not (q_host.flags["F_CONTIGUOUS"] and q_host.dtype == np.float64):
@@ -450,6 +456,20 @@ class LSRK54:
             self.time += self.dt
 
 
+class LSRK144(LSRK54):
+    """LSRK144(rhs!, q, dt; t0 = 0) (src/balancelaws/odesolvers.jl:68-71, 191-239): the
+    14-stage fourth-order low-storage scheme on the same fused stage kernels.  Its stages
+    run fused only; a stage callback raises instead of being ignored."""
+
+    def dostep(self, q, nsteps=1, after_stage=None):
+        """dostep!(q, lsrk, after_stage) (odesolvers.jl:51-61), `nsteps` times."""
+        if after_stage is not None:
+            raise NotImplementedError("LSRK144 runs its 14 stages fused on the device; after_stage is not supported")
+        self.dg.lsrk144_steps(q, self.dq, self.time, self.dt, nsteps)
+        for _ in range(nsteps):
+            self.time += self.dt
+
+
 class RLSRK54:
     """RLSRK54(rhs!, q, dt; t0 = 0) (src/balancelaws/odesolvers.jl:73-161): LSRK(5,4) with
     relaxation, so that the entropy integral changes by exactly the stages' entropy
@@ -468,13 +488,25 @@ class RLSRK54:
         The stages and the relaxation run fused on the device, so a stage callback cannot
         be honoured: `after_stage` raises instead of being ignored."""
         if after_stage is not None:
-            raise NotImplementedError("RLSRK54 runs its stages fused on the device; after_stage is not supported")
+            raise NotImplementedError(f"{type(self).__name__} runs its stages fused on the device; "
+                                      "after_stage is not supported")
         g = ctypes.c_double(self.gamma)
-        _lib.check(_lib.lib().rb200_rlsrk54_step(self.dg._h, q.ptr(), self.dq.ptr(), ctypes.byref(g), self.time,
-                                                 self.dt, int(nsteps), _stream_ptr()), self.dg._h)
+        _lib.check(self._entry()(self.dg._h, q.ptr(), self.dq.ptr(), ctypes.byref(g), self.time, self.dt,
+                                 int(nsteps), _stream_ptr()), self.dg._h)
         self.gamma = g.value
         for _ in range(nsteps):
             self.time += self.dt
+
+    def _entry(self):
+        return _lib.lib().rb200_rlsrk54_step
+
+
+class RLSRK144(RLSRK54):
+    """RLSRK144(rhs!, q, dt; t0 = 0) (src/balancelaws/odesolvers.jl:158-161): relaxation
+    over the 14 stages of LSRK(14,4).  FP64 operators only."""
+
+    def _entry(self):
+        return _lib.lib().rb200_rlsrk144_step
 
 
 def solve(q, timeend, solver, after_step=None, after_stage=None, adjust_final=True):

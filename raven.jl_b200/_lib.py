@@ -30,6 +30,7 @@ EXPORTED = [
     "rb200_destroy",
     "rb200_tendency",
     "rb200_lsrk54_step",
+    "rb200_lsrk144_step",
     "rb200_lsrk54_step_host",
     "rb200_lsrk54_stage",
     "rb200_lsrk54_stage_range",
@@ -42,6 +43,7 @@ EXPORTED = [
     "rb200_entropy_integral",
     "rb200_entropy_product",
     "rb200_rlsrk54_step",
+    "rb200_rlsrk144_step",
     "rb200_snapshot_bytes",
     "rb200_snapshot",
     "rb200_restore",
@@ -156,6 +158,7 @@ def lib():
     L.rb200_destroy.argtypes = [P]
     L.rb200_tendency.argtypes = [P, P, P, D, I32, P]
     L.rb200_lsrk54_step.argtypes = [P, P, P, D, D, I32, P]
+    L.rb200_lsrk144_step.argtypes = [P, P, P, D, D, I32, P]
     L.rb200_lsrk54_step_host.argtypes = [P, P, D, D, I32, P]
     L.rb200_lsrk54_stage.argtypes = [P, P, P, P, I32, D, D, P]
     L.rb200_lsrk54_stage_range.argtypes = [P, P, P, P, I32, I64, I64, D, D, P]
@@ -168,6 +171,7 @@ def lib():
     L.rb200_entropy_integral.argtypes = [P, P, P, P]
     L.rb200_entropy_product.argtypes = [P, P, P, P, P]
     L.rb200_rlsrk54_step.argtypes = [P, P, P, P, D, D, I32, P]
+    L.rb200_rlsrk144_step.argtypes = [P, P, P, P, D, D, I32, P]
     L.rb200_snapshot_bytes.argtypes = [P, ctypes.POINTER(ctypes.c_size_t)]
     L.rb200_snapshot.argtypes = [P, P, P, D, D, D, P, ctypes.c_size_t, P]
     L.rb200_restore.argtypes = [P, P, ctypes.c_size_t, P, P, ctypes.POINTER(D), ctypes.POINTER(D), ctypes.POINTER(D), P]

@@ -56,6 +56,7 @@ struct rb200_handle {
     const double* graph_q = nullptr;
     const void* graph_dq = nullptr;
     double graph_dt = 0.0;
+    const double* graph_rka = nullptr;  // a coefficients of the captured graph's scheme
     int use_graphs = 1;
     int pipe_grid = 0;            // CTAs of the pipelined kernel (0: not eligible)
     int pipe_curved_grid = 0;     // CTAs of the curved-grid pipelined kernel, FP32 bulk or FP64 (0: not eligible)
@@ -65,10 +66,10 @@ struct rb200_handle {
     int64_t* d_mortars = nullptr;
     double* d_ncflux = nullptr;
     MortarArgs mortar{};
-    // RLSRK(5,4) workspace (rb200_rlsrk54_step): q0, the stage tendency k, and device sums
+    // RLSRK workspace (rb200_rlsrk54_step, rb200_rlsrk144_step): q0, the stage tendency k, and device sums
     double* d_rq0 = nullptr;
     double* d_rk = nullptr;
-    double* d_rsums = nullptr;  // (eta, prod) pairs: [0] eta0, [1..5] stages, [6] relaxation solve
+    double* d_rsums = nullptr;  // (eta, prod) pairs: [0] eta0, [1..stages] the stages
     std::string err;
 };
 
@@ -80,6 +81,37 @@ const double RKA[5] = {0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 
 const double RKB[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
                        1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
                        2277821191437.0 / 14882151754819.0};
+
+// LSRK(14,4) coefficients (odesolvers.jl:191-239, coefficients_lsrk144): the reference's
+// Float64 literals.
+const double RKA144[14] = {0.0,
+                           -0.7188012108672410,
+                           -0.7785331173421570,
+                           -0.0053282796654044,
+                           -0.8552979934029281,
+                           -3.9564138245774565,
+                           -1.5780575380587385,
+                           -2.0837094552574054,
+                           -0.7483334182761610,
+                           -0.7032861106563359,
+                           0.0013917096117681,
+                           -0.0932075369637460,
+                           -0.9514200470875948,
+                           -7.1151571693922548};
+const double RKB144[14] = {0.0367762454319673, 0.3136296607553959, 0.1531848691869027, 0.0030097086818182,
+                           0.3326293790646110, 0.2440251405350864, 0.3718879239592277, 0.6204126221582444,
+                           0.1524043173028741, 0.0760894927419266, 0.0077604214040978, 0.0024647284755382,
+                           0.0780348340049386, 5.5059777270269628};
+
+// A low-storage Runge-Kutta scheme: its stage count and its a and b coefficients.
+struct Scheme {
+    int stages;
+    const double* rka;
+    const double* rkb;
+};
+constexpr int kMaxStages = 14;
+const Scheme kLSRK54{5, RKA, RKB};
+const Scheme kLSRK144{14, RKA144, RKB144};
 
 struct DeviceGuard {
     int prev = -1;
@@ -236,21 +268,21 @@ StageArgs base_args(const rb200_handle* h) {
     return a;
 }
 
-// Enqueues `nsteps` LSRK(5,4) steps with q_in/q_out alternating between q and the
+// Enqueues `nsteps` steps of the scheme with q_in/q_out alternating between q and the
 // handle's second state buffer; returns the buffer holding the result.
-rb200_status enqueue_steps(rb200_handle* h, double* q, void* dq, double dt, int32_t nsteps, cudaStream_t st,
-                           double** result) {
+rb200_status enqueue_steps(rb200_handle* h, const Scheme& sc, double* q, void* dq, double dt, int32_t nsteps,
+                           cudaStream_t st, double** result) {
     StageArgs a = base_args(h);
     a.dq = dq;
     double* cur = q;
     double* oth = h->d_qtmp;
     for (int32_t step = 0; step < nsteps; ++step) {
-        for (int stg = 0; stg < 5; ++stg) {
+        for (int stg = 0; stg < sc.stages; ++stg) {
             a.q_in = cur;
             a.q_out = oth;
-            a.mode = RKA[stg] == 0.0 ? MODE_STAGE_FIRST : MODE_STAGE;
-            a.rka = RKA[stg];
-            a.rkb_dt = RKB[stg] * dt;
+            a.mode = sc.rka[stg] == 0.0 ? MODE_STAGE_FIRST : MODE_STAGE;
+            a.rka = sc.rka[stg];
+            a.rkb_dt = sc.rkb[stg] * dt;
             cudaError_t e = launch_any(h, a, st);
             if (e != cudaSuccess) return cuda_fail(h, e, "stage kernel launch");
             double* t = cur;
@@ -262,7 +294,8 @@ rb200_status enqueue_steps(rb200_handle* h, double* q, void* dq, double dt, int3
     return RB200_OK;
 }
 
-rb200_status run_steps(rb200_handle* h, double* q, void* dq, double dt, int32_t nsteps, cudaStream_t st) {
+rb200_status run_steps(rb200_handle* h, const Scheme& sc, double* q, void* dq, double dt, int32_t nsteps,
+                       cudaStream_t st) {
     const size_t nstate = (size_t)h->np * h->ns * h->E;
     if (!h->d_qtmp) {
         rb200_status s = dev_alloc(h, &h->d_qtmp, nstate);
@@ -275,9 +308,10 @@ rb200_status run_steps(rb200_handle* h, double* q, void* dq, double dt, int32_t 
     if (h->use_graphs && nsteps >= 4) {
         // two steps (an even number of stages, so the state is back in q) run eagerly:
         // kernel attributes get configured outside the capture
-        if ((rs = enqueue_steps(h, q, dq, dt, 2, st, &cur)) != RB200_OK) return rs;
+        if ((rs = enqueue_steps(h, sc, q, dq, dt, 2, st, &cur)) != RB200_OK) return rs;
         done = 2;
-        if (!h->graph_exec || h->graph_q != q || h->graph_dq != dq || h->graph_dt != dt) {
+        if (!h->graph_exec || h->graph_q != q || h->graph_dq != dq || h->graph_dt != dt ||
+            h->graph_rka != sc.rka) {
             free_graph(h);
             cudaError_t e = cudaSuccess;
             if (!h->cap_stream) e = cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking);
@@ -286,7 +320,7 @@ rb200_status run_steps(rb200_handle* h, double* q, void* dq, double dt, int32_t 
             e = cudaStreamBeginCapture(h->cap_stream, cudaStreamCaptureModeThreadLocal);
             if (e != cudaSuccess) return cuda_fail(h, e, "graph capture");
             double* gres = nullptr;
-            rs = enqueue_steps(h, q, dq, dt, 2, h->cap_stream, &gres);
+            rs = enqueue_steps(h, sc, q, dq, dt, 2, h->cap_stream, &gres);
             e = cudaStreamEndCapture(h->cap_stream, &graph);
             if (rs != RB200_OK) {
                 if (graph) cudaGraphDestroy(graph);
@@ -301,6 +335,7 @@ rb200_status run_steps(rb200_handle* h, double* q, void* dq, double dt, int32_t 
             h->graph_q = q;
             h->graph_dq = dq;
             h->graph_dt = dt;
+            h->graph_rka = sc.rka;
         }
         for (; done + 2 <= nsteps; done += 2) {
             cudaError_t e = cudaGraphLaunch(h->graph_exec, st);
@@ -308,7 +343,7 @@ rb200_status run_steps(rb200_handle* h, double* q, void* dq, double dt, int32_t 
         }
     }
     if (done < nsteps) {
-        if ((rs = enqueue_steps(h, q, dq, dt, nsteps - done, st, &cur)) != RB200_OK) return rs;
+        if ((rs = enqueue_steps(h, sc, q, dq, dt, nsteps - done, st, &cur)) != RB200_OK) return rs;
     }
     if (cur != q) {
         cudaError_t e = cudaMemcpyAsync(q, cur, nstate * sizeof(double), cudaMemcpyDeviceToDevice, st);
@@ -344,19 +379,21 @@ rb200_status entropy_sums_host(rb200_handle* h, const double* base, const double
 }
 
 // rkb_full: the b coefficients of the standard Butcher form (odesolvers.jl:91-97)
-void rkb_full(double* bf) {
-    bf[4] = RKB[4];
-    for (int i = 3; i >= 0; --i) bf[i] = RKA[i + 1] * bf[i + 1] + RKB[i];
+void rkb_full(const Scheme& sc, double* bf) {
+    const int n = sc.stages;
+    bf[n - 1] = sc.rkb[n - 1];
+    for (int i = n - 2; i >= 0; --i) bf[i] = sc.rka[i + 1] * bf[i + 1] + sc.rkb[i];
 }
 
-// One RLSRK(5,4) step (odesolvers.jl:118-151).  The relaxation solve r(gamma) = 0 with
+// One RLSRK step of the scheme (odesolvers.jl:118-151).  The relaxation solve r(gamma) = 0 with
 // r(gamma) = eta(q0 + gamma k) - eta0 - gamma deta and r'(gamma) = v(q0 + gamma k).k - deta
 // takes Newton steps from the previous gamma, as the reference's NLsolve trust-region
 // method does for a scalar problem whose steps stay inside the region: a step is kept
 // when it reduces r^2 by more than 1e-4 of the predicted reduction; the solve ends at
 // |r| <= 10 eps (the reference's ftol) or at the first step that is not kept (the
 // residual is then at round-off), after at most 1000 iterations.
-rb200_status rlsrk_step(rb200_handle* h, double* q, double* dq, double* gamma, double dt, cudaStream_t s) {
+rb200_status rlsrk_step(rb200_handle* h, const Scheme& sc, double* q, double* dq, double* gamma, double dt,
+                        cudaStream_t s) {
     const int64_t n = (int64_t)h->np * h->ns * h->E;
     const RelaxGeo G = relax_geo(h);
     cudaError_t e = cudaMemcpyAsync(h->d_rq0, q, n * sizeof(double), cudaMemcpyDeviceToDevice, s);
@@ -366,24 +403,25 @@ rb200_status rlsrk_step(rb200_handle* h, double* q, double* dq, double* gamma, d
     StageArgs a = base_args(h);
     a.mode = MODE_TENDENCY_SET;
     a.dq = h->d_rk;
-    for (int st = 0; st < 5; ++st) {
+    for (int st = 0; st < sc.stages; ++st) {
         a.q_in = q;
         e = launch_any(h, a, s);  // k = RHS(q)
         if (e == cudaSuccess)
-            e = launch_rlsrk_stage(G, q, dq, h->d_rk, RKA[st], RKB[st] * dt, h->d_partial, h->red_blocks,
+            e = launch_rlsrk_stage(G, q, dq, h->d_rk, sc.rka[st], sc.rkb[st] * dt, h->d_partial, h->red_blocks,
                                    h->d_rsums + 2 * (1 + st), s);
         if (e != cudaSuccess) return cuda_fail(h, e, "relaxation stage");
     }
     e = launch_state_diff(q, h->d_rq0, h->d_rk, n, s);  // k = q - q0
-    double sums[12];
-    if (e == cudaSuccess) e = cudaMemcpyAsync(sums, h->d_rsums, sizeof(sums), cudaMemcpyDeviceToHost, s);
+    double sums[2 * (1 + kMaxStages)];
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(sums, h->d_rsums, 2 * (1 + sc.stages) * sizeof(double), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(h, e, "relaxation stages");
-    double bf[5];
-    rkb_full(bf);
+    double bf[kMaxStages];
+    rkb_full(sc, bf);
     const double eta0 = sums[0];
     double deta = -0.0;
-    for (int st = 0; st < 5; ++st) deta = deta + bf[st] * dt * sums[2 * (1 + st) + 1];
+    for (int st = 0; st < sc.stages; ++st) deta = deta + bf[st] * dt * sums[2 * (1 + st) + 1];
     const double ftol = 10 * 2.220446049250313e-16;
     auto eval = [&](double g, double* F, double* J) -> rb200_status {
         double s2[2];
@@ -690,15 +728,26 @@ rb200_status rb200_tendency(rb200_handle* h, double* dq, const double* q, double
     return RB200_OK;
 }
 
-rb200_status rb200_lsrk54_step(rb200_handle* h, double* q, double* dq, double time, double dt, int32_t nsteps,
+static rb200_status lsrk_steps(rb200_handle* h, const Scheme& sc, double* q, double* dq, double dt, int32_t nsteps,
                                void* stream) {
-    (void)time;
     if (!h) return RB200_ERR_BAD_ARG;
     if (!q || (!dq && h->prec == RB200_PRECISION_FP64)) return fail(h, RB200_ERR_BAD_ARG, "null state pointer");
     if (nsteps < 0 || !std::isfinite(dt)) return fail(h, RB200_ERR_BAD_ARG, "bad nsteps or dt");
     if (h->E_active == 0 || nsteps == 0) return RB200_OK;
     DeviceGuard guard(h->device);
-    return run_steps(h, q, dq, dt, nsteps, (cudaStream_t)stream);
+    return run_steps(h, sc, q, dq, dt, nsteps, (cudaStream_t)stream);
+}
+
+rb200_status rb200_lsrk54_step(rb200_handle* h, double* q, double* dq, double time, double dt, int32_t nsteps,
+                               void* stream) {
+    (void)time;
+    return lsrk_steps(h, kLSRK54, q, dq, dt, nsteps, stream);
+}
+
+rb200_status rb200_lsrk144_step(rb200_handle* h, double* q, double* dq, double time, double dt, int32_t nsteps,
+                                void* stream) {
+    (void)time;
+    return lsrk_steps(h, kLSRK144, q, dq, dt, nsteps, stream);
 }
 
 // One stage of LSRK(5,4) (odesolvers.jl:163-189) from q_in to q_out on elements
@@ -770,7 +819,7 @@ rb200_status rb200_lsrk54_step_host(rb200_handle* h, double* q_host, double time
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = cudaMemcpyAsync(h->d_hq, q_host, n * sizeof(double), cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return cuda_fail(h, e, "host-to-device copy");
-    if ((st = run_steps(h, h->d_hq, h->d_hdq, dt, nsteps, s)) != RB200_OK) return st;
+    if ((st = run_steps(h, kLSRK54, h->d_hq, h->d_hdq, dt, nsteps, s)) != RB200_OK) return st;
     e = cudaMemcpyAsync(q_host, h->d_hq, n * sizeof(double), cudaMemcpyDeviceToHost, s);
     if (e != cudaSuccess) return cuda_fail(h, e, "device-to-host copy");
     e = cudaStreamSynchronize(s);
@@ -860,24 +909,35 @@ rb200_status rb200_entropy_product(rb200_handle* h, const double* p, const doubl
     return st;
 }
 
-rb200_status rb200_rlsrk54_step(rb200_handle* h, double* q, double* dq, double* gamma, double time, double dt,
+static rb200_status rlsrk_steps(rb200_handle* h, const Scheme& sc, double* q, double* dq, double* gamma, double dt,
                                 int32_t nsteps, void* stream) {
-    (void)time;
     if (!h) return RB200_ERR_BAD_ARG;
     if (!q || !dq || !gamma) return fail(h, RB200_ERR_BAD_ARG, "null pointer");
     if (nsteps < 0 || !std::isfinite(dt) || !std::isfinite(*gamma)) return fail(h, RB200_ERR_BAD_ARG, "bad nsteps, dt or gamma");
     if (h->prec != RB200_PRECISION_FP64)
-        return fail(h, RB200_ERR_UNSUPPORTED, "RLSRK54 keeps its LSRK register in FP64: create the handle in FP64");
+        return fail(h, RB200_ERR_UNSUPPORTED, "RLSRK keeps its LSRK register in FP64: create the handle in FP64");
     if (h->E == 0 || nsteps == 0) return RB200_OK;
     DeviceGuard guard(h->device);
     const size_t n = (size_t)h->np * h->ns * h->E;
     rb200_status st;
     if (!h->d_rq0 && (st = dev_alloc(h, &h->d_rq0, n)) != RB200_OK) return st;
     if (!h->d_rk && (st = dev_alloc(h, &h->d_rk, n)) != RB200_OK) return st;
-    if (!h->d_rsums && (st = dev_alloc(h, &h->d_rsums, 16)) != RB200_OK) return st;
+    if (!h->d_rsums && (st = dev_alloc(h, &h->d_rsums, 2 * (1 + kMaxStages))) != RB200_OK) return st;
     for (int32_t i = 0; i < nsteps; ++i)
-        if ((st = rlsrk_step(h, q, dq, gamma, dt, (cudaStream_t)stream)) != RB200_OK) return st;
+        if ((st = rlsrk_step(h, sc, q, dq, gamma, dt, (cudaStream_t)stream)) != RB200_OK) return st;
     return RB200_OK;
+}
+
+rb200_status rb200_rlsrk54_step(rb200_handle* h, double* q, double* dq, double* gamma, double time, double dt,
+                                int32_t nsteps, void* stream) {
+    (void)time;
+    return rlsrk_steps(h, kLSRK54, q, dq, gamma, dt, nsteps, stream);
+}
+
+rb200_status rb200_rlsrk144_step(rb200_handle* h, double* q, double* dq, double* gamma, double time, double dt,
+                                 int32_t nsteps, void* stream) {
+    (void)time;
+    return rlsrk_steps(h, kLSRK144, q, dq, gamma, dt, nsteps, stream);
 }
 
 // ---------------------------------------------------------------------------------

@@ -221,10 +221,17 @@ def test_config5_adapted_one_step(rb, cuda_ok):
     og.lsrk54_step(olaw, qo, dqo, 0.0, dt)
     dg64 = rb.DGSEM(law=law, grid=grid, volume_form=rb.FluxDifferencingForm(rb.KennedyGruberFlux()),
                     surface_numericalflux=rb.RusanovFlux(), precision="fp64", device=0)
+    # the pulse starts at rest under uniform pressure, so the momenta after one step are
+    # round-off-sized in FP64 (the pressure gradient cancels): all fields are measured
+    # against the magnitude of the state, not against their own (near-zero) size
+    scale = float(np.abs(qo).max())
+    errs = {}
     for dg, tol in ((dg32, FP32_TOL), (dg64, FP64_TOL)):
         q = rb.GridArray.from_numpy(q0)
         dq = q.similar()
         dg.lsrk54_steps(q, dq, 0.0, dt, 1)
         dg.sync_status()
-        err = field_errors(q.numpy(), qo, law)
-        assert max(err) <= tol, f"{dg.precision} adapted state after one step beyond {tol}: {err}"
+        got = q.numpy()
+        errs[dg.precision] = ([float(np.abs(got[:, s] - qo[:, s]).max()) / scale for s in range(law.ns)], tol)
+    for prec, (err, tol) in errs.items():
+        assert max(err) <= tol, f"{prec} adapted state after one step beyond {tol}: {err}"

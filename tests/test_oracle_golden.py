@@ -129,3 +129,36 @@ def test_oracle_weightednorm_p(p):
     if p == 2:
         t2, c2 = g.weightednorm(q, L.ns)
         assert tot == pytest.approx(t2, rel=1e-15) and np.allclose(comp, c2, rtol=1e-15, atol=0)
+
+
+def test_oracle_lsrk144_matches_lsrk54_golden():
+    """LSRK144 (odesolvers.jl:191-239) in the setting of the reference's 2-D advection wave
+    test (K = 5, N = 4, weak form, t = 0.7, the test's dt): the 14-stage fourth-order
+    scheme gives the L2 error of the LSRK54 golden value to 1e-3 relative (the spatial
+    error dominates; the two schemes' time errors differ by ~2e-4 of it), and its state
+    differs from LSRK54's by time-discretisation error only."""
+    entry = next(e for e in GOLD["errors"] if e["test"] == "wave_2d" and e["law"] == "advection"
+                 and e["form"] == "weak" and e["level"] == 1)
+    K, N = 5, 4
+    L = O.Law(O.LAW_ADVECTION, 2, form=O.FORM_WEAK)
+    g = O.Grid(2, N + 1, [K, K], [-1.0, -1.0], [1.0, 1.0], [True, True])
+    dt = 0.25 * (2.0 / K) / N / math.sqrt(2)
+    T = 0.7
+    q54, q144 = g.initial_condition(L, 0), g.initial_condition(L, 0)
+    dq54, dq144 = g.state(L), g.state(L)
+    t, n = 0.0, 0
+    while True:
+        final = t + dt >= T
+        h = T - t if final else dt
+        g.lsrk54_step(L, q54, dq54, t, h)
+        g.lsrk144_step(L, q144, dq144, t, h)
+        t += h
+        n += 1
+        if final:
+            break
+    qe = g.initial_condition(L, 0, t=T)
+    e54, _ = g.weightednorm(q54 - qe, L.ns)
+    e144, _ = g.weightednorm(q144 - qe, L.ns)
+    assert e54 == pytest.approx(entry["expected"], rel=entry["rtol"])
+    assert e144 == pytest.approx(entry["expected"], rel=1e-3)
+    assert np.abs(q144 - q54).max() < 1e-5  # time error; the spatial error is ~1e-3 in max norm
