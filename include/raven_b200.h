@@ -88,7 +88,10 @@ typedef struct rb200_handle rb200_handle;
 
 /* DGSEM(; law, grid, surface_numericalflux, volume_form)  (dgsem.jl:46-81).
  * Uploads the grid once; compresses vmapM/vmapP into a per-face neighbour table
- * after checking, node by node, that it reproduces them. */
+ * after checking, node by node, that it reproduces them.  A grid of an unstructured
+ * coarse grid, whose faces may meet rotated or on another face of the neighbour
+ * (lobattocells.jl:2177-2206), keeps vmapP as a table read by the kernels; its faces
+ * must each map onto one face of one element (RB200_ERR_SHAPE otherwise). */
 rb200_status rb200_create(const rb200_desc* desc, rb200_handle** out);
 rb200_status rb200_destroy(rb200_handle* h);
 
@@ -201,7 +204,8 @@ rb200_status rb200_restore(rb200_handle* h, const void* host, size_t bytes, doub
                            double* dt, double* gamma, void* stream);
 
 /* Rebuilds vmapP (1-based, (2*dim*nq^(dim-1), E) int64) on the device from the
- * neighbour table the kernels use, for bit-exact comparison with facemaps(grid).vmapP. */
+ * neighbour table the kernels use (or from the vmapP table they read, on a grid with
+ * rotated faces), for bit-exact comparison with facemaps(grid).vmapP. */
 rb200_status rb200_face_vmapP(rb200_handle* h, int64_t* vmapP_out, void* stream);
 
 /* Mortars of an adapted (non-conforming) grid, after rb200_create.  The reference's

@@ -32,6 +32,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import RB200Error
+from .coarse import CoarseGrid, UnstructuredGrid, coarsegrid, cubeshellgrid
 from .forest import AdaptCoarsen, AdaptNone, AdaptRefine, Forest, ForestGrid
 from .grids import Grid, brick_tree_order, jl_range, lobatto_operators
 
@@ -42,7 +43,7 @@ __all__ = [
     "weightednorm", "integrals",
     "entropyintegral", "entropyproduct", "snapshot", "restore",
     "jl_range", "RB200Error", "brick_tree_order", "adapt", "AdaptRefine", "AdaptNone", "AdaptCoarsen",
-    "ForestGrid",
+    "ForestGrid", "CoarseGrid", "coarsegrid", "cubeshellgrid", "UnstructuredGrid",
 ]
 
 # --------------------------------------------------------------------------- cells and grids
@@ -98,17 +99,27 @@ def brick(coordinates, periodic=None):
 
 class GridManager:
     """GridManager(cell, coarsegrid; min_level) (src/gridmanager.jl:53-94): a forest of
-    trees on the brick, each refined uniformly to min_level, adaptable with adapt."""
+    trees on the brick, each refined uniformly to min_level, adaptable with adapt.  On
+    an unstructured coarse grid (CoarseGrid, cubeshellgrid) every cell is a tree,
+    refined uniformly to min_level; adapting such a forest is not implemented."""
 
     def __init__(self, cell, coarsegrid, min_level=0):
-        if len(coarsegrid.coordinates) != cell.dim:
-            raise ValueError("cell and coarse grid dimensions differ")
         self.cell = cell
         self.coarsegrid = coarsegrid
+        self.min_level = int(min_level)
+        if isinstance(coarsegrid, CoarseGrid):
+            if coarsegrid.dim != cell.dim:
+                raise ValueError("cell and coarse grid dimensions differ")
+            self.forest = None
+            return
+        if len(coarsegrid.coordinates) != cell.dim:
+            raise ValueError("cell and coarse grid dimensions differ")
         K = [len(c) - 1 for c in coarsegrid.coordinates]
         self.forest = Forest(cell.dim, K, coarsegrid.periodic, min_level=min_level)
 
     def __len__(self):
+        if self.forest is None:
+            return len(self.coarsegrid) << (self.cell.dim * self.min_level)
         return len(self.forest)
 
 
@@ -116,6 +127,8 @@ def adapt(gm, flags):
     """adapt!(gm, flags) (src/gridmanager.jl:160-173): refine (AdaptRefine), keep
     (AdaptNone) or coarsen (AdaptCoarsen, whole families) each leaf, then balance 2:1
     across faces."""
+    if gm.forest is None:
+        raise NotImplementedError("adapting a forest on an unstructured coarse grid is not implemented")
     gm.forest.adapt(flags)
 
 
@@ -128,6 +141,8 @@ def generate(arg, gm=None):
         gm, warp = arg, None
     else:
         warp = arg
+    if gm.forest is None:
+        return UnstructuredGrid(gm.cell, gm.coarsegrid, gm.min_level, warp=warp)
     if all(L[1] == 0 for L in gm.forest.leaves):
         return Grid(gm.cell, gm.coarsegrid, warp=warp)
     if warp is not None:

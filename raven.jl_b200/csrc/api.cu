@@ -10,6 +10,10 @@
 //    neighbour per element face.  Every node of every face is checked against the
 //    given vmapP before the table is accepted, so the kernels' implied indexing is
 //    the reference's indexing bit for bit (rb200_face_vmapP rebuilds it on the GPU).
+//    A grid whose faces do not all meet aligned, face x- against face x+ and so on
+//    (rotated faces of an unstructured coarse grid, lobattocells.jl:2177-2206), keeps
+//    vmapP itself as an int32 table; the generic stage kernel then reads qP = q[vmapP]
+//    node by node, and the handle takes the per-node (curved) geometry path.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -40,6 +44,7 @@ struct rb200_handle {
     double* d_sgeo = nullptr;
     double* d_w = nullptr;
     int32_t* d_nbr = nullptr;
+    int32_t* d_vmapP = nullptr;  // general connectivity only: vmapP - 1 per face node
     double* d_qtmp = nullptr;
     float* d_dq32 = nullptr;
     double* d_hq = nullptr;   // device copy of a host state (rb200_lsrk54_step_host)
@@ -168,7 +173,8 @@ void free_all(rb200_handle* h) {
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     h->cap_stream = nullptr;
     void* ptrs[] = {h->d_elem_geo, h->d_vgeo, h->d_sgeo,    h->d_w,    h->d_nbr,   h->d_qtmp,
-                    h->d_dq32,     h->d_hq,   h->d_hdq,     h->d_partial, h->d_sums, h->d_status};
+                    h->d_dq32,     h->d_hq,   h->d_hdq,     h->d_partial, h->d_sums, h->d_status,
+                    h->d_vmapP};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->d_mortars) cudaFree(h->d_mortars);
@@ -182,6 +188,7 @@ void free_all(rb200_handle* h) {
     h->d_elem_geo = h->d_vgeo = h->d_sgeo = h->d_w = h->d_qtmp = h->d_hq = h->d_hdq = h->d_partial = h->d_sums =
         nullptr;
     h->d_nbr = nullptr;
+    h->d_vmapP = nullptr;
     h->d_dq32 = nullptr;
     h->d_status = nullptr;
 }
@@ -258,6 +265,7 @@ StageArgs base_args(const rb200_handle* h) {
     a.sgeo = h->d_sgeo;
     a.nbr = h->d_nbr;
     a.ncflux = h->d_ncflux;
+    a.vmapP = h->d_vmapP;
     a.E = h->E_active;
     a.surface_rusanov = h->sflux == RB200_FLUX_RUSANOV ? 1 : 0;
     a.surface_flux = h->sflux;
@@ -589,6 +597,7 @@ rb200_status rb200_create(const rb200_desc* d, rb200_handle** out) {
 
     // ------------------------------------------------------------- connectivity
     std::vector<int32_t> nbr((size_t)nf * E, -1);
+    bool general = false;  // some face meets its neighbour rotated or on another face
     for (int64_t e = 0; e < E; ++e)
         for (int f = 0; f < nf; ++f) {
             const size_t base = (size_t)nf * nfp * e + (size_t)f * nfp;
@@ -612,12 +621,38 @@ rb200_status rb200_create(const rb200_desc* d, rb200_handle** out) {
                     nbr[(size_t)nf * e + f] = -1;
                     continue;
                 }
-                return bail(fail(h, RB200_ERR_UNSUPPORTED,
-                                 "face connectivity is not an aligned conforming neighbour (rotated faces are not "
-                                 "implemented)"));
+                // a conforming neighbour in another orientation or on another face: every
+                // node must name a node of one other element, on one of its faces
+                const int64_t tot = (int64_t)np * E;
+                const int64_t e2 = ne;
+                ok = ne >= 0 && ne < E;
+                for (int j = 0; j < nfp && ok; ++j) {
+                    const int64_t g = d->vmapP[base + j] - 1;
+                    ok = g >= 0 && g < tot && g / np == e2;
+                    if (ok) {
+                        const int n2 = (int)(g % np);
+                        const int i0 = n2 % nq, i1 = (n2 / nq) % nq, i2 = dim == 3 ? n2 / (nq * nq) : 0;
+                        ok = i0 == 0 || i0 == nq - 1 || i1 == 0 || i1 == nq - 1 ||
+                             (dim == 3 && (i2 == 0 || i2 == nq - 1));
+                    }
+                }
+                if (!ok)
+                    return bail(fail(h, RB200_ERR_SHAPE,
+                                     "vmapP: a face's nodes do not all lie on one face of one other element"));
+                general = true;
             }
             nbr[(size_t)nf * e + f] = (int32_t)ne;
         }
+    std::vector<int32_t> vmapP32;
+    if (general) {
+        if ((int64_t)np * E > (int64_t)INT32_MAX)
+            return bail(fail(h, RB200_ERR_UNSUPPORTED, "general face connectivity needs Np*E < 2^31"));
+        vmapP32.resize((size_t)nf * nfp * E);
+        for (size_t k = 0; k < vmapP32.size(); ++k) vmapP32[k] = (int32_t)(d->vmapP[k] - 1);
+        // the kernels with implied face indexing (bricks) do not apply: per-node geometry
+        affine = false;
+        h->geom = GEOM_CURVED;
+    }
 
     // ----------------------------------------------------------------- upload
     DeviceGuard guard(h->device);
@@ -627,6 +662,11 @@ rb200_status rb200_create(const rb200_desc* d, rb200_handle** out) {
     cudaError_t ce = cudaMemcpy(h->d_nbr, nbr.data(), nbr.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
     if (ce == cudaSuccess) ce = cudaMemcpy(h->d_w, h->w, nq * sizeof(double), cudaMemcpyHostToDevice);
     if (ce != cudaSuccess) return bail(cuda_fail(h, ce, "upload"));
+    if (general) {
+        if ((st = dev_alloc(h, &h->d_vmapP, vmapP32.size())) != RB200_OK) return bail(st);
+        ce = cudaMemcpy(h->d_vmapP, vmapP32.data(), vmapP32.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+        if (ce != cudaSuccess) return bail(cuda_fail(h, ce, "upload"));
+    }
     if (affine) {
         if ((st = dev_alloc(h, &h->d_elem_geo, eg.size())) != RB200_OK) return bail(st);
         ce = cudaMemcpy(h->d_elem_geo, eg.data(), eg.size() * sizeof(double), cudaMemcpyHostToDevice);
@@ -682,7 +722,7 @@ rb200_status rb200_create(const rb200_desc* d, rb200_handle** out) {
         h->pipe_grid = per_sm > 0 ? per_sm * nsm : 0;
         cudaGetLastError();
     }
-    if (dim == 3 && nq == 8 && !affine && h->combo == EUL_KG && !entropy_flux && h->d_vgeo && h->d_sgeo &&
+    if (dim == 3 && nq == 8 && !affine && !general && h->combo == EUL_KG && !entropy_flux && h->d_vgeo && h->d_sgeo &&
         aligned16(h->d_vgeo) && aligned16(h->d_sgeo)) {
         // curved 3-D Nq = 8 Kennedy-Gruber: the curved pipelined kernel of the handle's precision
         int dev = 0, nsm = 0;
@@ -1074,7 +1114,9 @@ rb200_status rb200_face_vmapP(rb200_handle* h, int64_t* vmapP_out, void* stream)
     if (!h) return RB200_ERR_BAD_ARG;
     if (!vmapP_out) return fail(h, RB200_ERR_BAD_ARG, "null pointer");
     DeviceGuard guard(h->device);
-    cudaError_t e = launch_face_vmapP(h->d_nbr, h->dim, h->nq, h->E, vmapP_out, (cudaStream_t)stream);
+    cudaError_t e = h->d_vmapP ? launch_copy_vmapP(h->d_vmapP, (int64_t)h->nf * h->nfp * h->E, vmapP_out,
+                                                   (cudaStream_t)stream)
+                               : launch_face_vmapP(h->d_nbr, h->dim, h->nq, h->E, vmapP_out, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "vmapP kernel launch");
     return RB200_OK;
 }

@@ -61,6 +61,9 @@ struct StageArgs {
     const int32_t* nbr;      // (2*dim, E): neighbour element across each face, -1 = boundary,
                              // -2 = a mortar face (its flux is in ncflux)
     const double* ncflux;    // mortar face fluxes ((2*dim, E) faces x (Ns, Nfp)), or null
+    const int32_t* vmapP;    // general connectivity (rotated faces, any neighbour face): per face
+                             // node (2*dim*Nfp, E) the 0-based global node e'*Np + n' across the
+                             // face; null on grids whose faces meet aligned (implied indexing)
     int64_t E;                // elements e_begin..E-1 are computed
     int64_t e_begin;
     int32_t mode;
@@ -137,6 +140,8 @@ cudaError_t launch_weighted_pnorm(const double* q, const double* elem_geo, const
                                   int dim, int nq, int ns, int64_t E, int geom, double p, double* partial,
                                   int nblocks, double* out_dev, cudaStream_t s);
 cudaError_t launch_face_vmapP(const int32_t* nbr, int dim, int nq, int64_t E, int64_t* out, cudaStream_t s);
+// out[k] = vmapP0[k] + 1: the 1-based vmapP of a grid kept with general connectivity
+cudaError_t launch_copy_vmapP(const int32_t* vmapP0, int64_t n, int64_t* out, cudaStream_t s);
 
 // Entropy measures and the RLSRK(5,4) step (relaxation.cu).  Sums land in out[0..1]
 // (device): (sum MJ eta, sum MJ v.k); the stage kernel writes only out[1].

@@ -264,6 +264,19 @@ cudaError_t launch_face_vmapP(const int32_t* nbr, int dim, int nq, int64_t E, in
     return cudaGetLastError();
 }
 
+__global__ void copy_vmapP_kernel(const int32_t* __restrict__ v, int64_t n, int64_t* __restrict__ out) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        out[t] = (int64_t)v[t] + 1;
+}
+
+cudaError_t launch_copy_vmapP(const int32_t* vmapP0, int64_t n, int64_t* out, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    int64_t blocks = (n + 255) / 256;
+    if (blocks > 4096) blocks = 4096;
+    copy_vmapP_kernel<<<(unsigned)blocks, 256, 0, s>>>(vmapP0, n, out);
+    return cudaGetLastError();
+}
+
 }  // namespace rb200
 
 // ---------------------------------------------------------------------------------

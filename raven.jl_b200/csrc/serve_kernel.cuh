@@ -57,6 +57,7 @@ __global__ void __launch_bounds__(Shape<DIM, NQ, EPBX>::THREADS,
         P.nbr = sd.nbr;
         P.rkb_dt = B.rkb * sd.dt;
         P.ncflux = nullptr;
+        P.vmapP = nullptr;
         e = c.first + g + el;
         active = g + el < c.count;
     };

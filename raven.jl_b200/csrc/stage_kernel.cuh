@@ -129,10 +129,11 @@ struct ElemPtrs {
     const int32_t* nbr;
     double rkb_dt;
     const double* ncflux;
+    const int32_t* vmapP;  // general connectivity, or null (StageArgs::vmapP)
 };
 
 __device__ __forceinline__ ElemPtrs elem_ptrs(const StageArgs& A) {
-    return ElemPtrs{A.q_in, A.q_out, A.dq, A.elem_geo, A.vgeo, A.sgeo, A.nbr, A.rkb_dt, A.ncflux};
+    return ElemPtrs{A.q_in, A.q_out, A.dq, A.elem_geo, A.vgeo, A.sgeo, A.nbr, A.rkb_dt, A.ncflux, A.vmapP};
 }
 
 // Weak-form advection on an unwarped element (the stage of stage_element, refactored for
@@ -526,20 +527,29 @@ __device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs
             const int f = 2 * dir + side;
             const int stride = dir == 0 ? 1 : (dir == 1 ? NQ : NQ * NQ);
             const int ne = __ldg(P.nbr + (size_t)NF * e + f);
+            // in-face index of this node (column-major over the face dims)
+            int j;
+            if (DIM == 2) j = (dir == 0) ? id[1] : id[0];
+            else j = (dir == 0) ? id[1] + NQ * id[2] : (dir == 1 ? id[0] + NQ * id[2] : id[0] + NQ * id[1]);
             T qp[NS];
             if (ne >= 0) {
-                const int nn = n + (side == 0 ? (NQ - 1) * stride : -(NQ - 1) * stride);
-                const double* qn = P.q_in + (size_t)ne * NS * NP + nn;
+                const double* qn;
+                if (!AFF && P.vmapP) {
+                    // qP = q[vmapP] (dgsem.jl:756-770): the neighbour's node may sit on any of
+                    // its faces, in any orientation
+                    const int32_t gn = __ldg(P.vmapP + ((size_t)e * NF + f) * NFP + j);
+                    const int32_t en = gn / NP;
+                    qn = P.q_in + (size_t)en * NS * NP + (gn - en * NP);
+                } else {
+                    const int nn = n + (side == 0 ? (NQ - 1) * stride : -(NQ - 1) * stride);
+                    qn = P.q_in + (size_t)ne * NS * NP + nn;
+                }
 #pragma unroll
                 for (int s = 0; s < NS; ++s) qp[s] = (T)__ldg(qn + s * NP);
             } else {
 #pragma unroll
                 for (int s = 0; s < NS; ++s) qp[s] = q[s];  // default boundarystate (balancelaw.jl:77)
             }
-            // in-face index of this node (column-major over the face dims)
-            int j;
-            if (DIM == 2) j = (dir == 0) ? id[1] : id[0];
-            else j = (dir == 0) ? id[1] + NQ * id[2] : (dir == 1 ? id[0] + NQ * id[2] : id[0] + NQ * id[1]);
             T nv[DIM];
             double wsJ;
             if constexpr (AFF) {

@@ -101,13 +101,20 @@ def test_create_checks_face_maps_node_by_node(rb, small_grid):
     import numpy as np
 
     g = small_grid
-    bad = g.vmapP.copy()
-    bad[1, 0], bad[2, 0] = bad[2, 0], bad[1, 0]  # a rotated face
-    d, keep = _desc(rb, g)
-    keep.append(np.asfortranarray(bad))
-    d.vmapP = keep[-1].ctypes.data_as(ctypes.c_void_p)
-    st, msg = _create(rb, d)
-    assert st == 6 and "rotated" in msg
+    # a face node mapped to an interior node of the neighbour, or to a node of a third
+    # element, is no face connectivity (a permutation within the neighbour's face is:
+    # that is a rotated face, kept as a vmapP table, which needs a device to upload)
+    ne = (g.vmapP[0, 0] - 1) // g.np
+    interior = ne * g.np + (g.nq + 1) + (g.nq * g.nq if g.dim == 3 else 0) + 1
+    third = [e for e in range(g.E) if e not in (0, ne)][0]
+    for val in (interior, third * g.np + 1):
+        bad = g.vmapP.copy()
+        bad[1, 0] = val
+        d, keep = _desc(rb, g)
+        keep.append(np.asfortranarray(bad))
+        d.vmapP = keep[-1].ctypes.data_as(ctypes.c_void_p)
+        st, msg = _create(rb, d)
+        assert st == 2 and "one face of one other element" in msg
     badM = g.vmapM.copy()
     badM[0, 0] += 1
     d, keep = _desc(rb, g)
