@@ -73,6 +73,7 @@ def lib():
         L.og_grid_from_arrays.restype = P
         L.og_grid_from_arrays.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int64, P, P, P, P, P, P]
         L.og_grid_set_mortars.argtypes = [P, P, ctypes.c_int64, P, P, P, P]
+        L.og_grid_set_curved_mortars.argtypes = [P, ctypes.c_int]
         for name in ("og_grid_sizes", "og_grid_points", "og_grid_vmet", "og_grid_smet", "og_grid_vmapM",
                      "og_grid_vmapP", "og_grid_boundary", "og_grid_tree_coords"):
             getattr(L, name).argtypes = [P, P]
@@ -154,10 +155,11 @@ class Grid:
 
     @classmethod
     def from_arrays(cls, dim, nq, points, volume_metrics, surface_metrics, vmapM, vmapP, boundarycodes,
-                    mortars=None, tohalves=None):
+                    mortars=None, tohalves=None, curved=False):
         """A grid from the arrays of a generated grid (adapted grids); with mortars
         ((2 + 2^(dim-1), M) int64 0-based) and tohalves (I_lower, I_upper, P_lower,
-        P_upper) the hanging faces are coupled through mortars."""
+        P_upper) the hanging faces are coupled through mortars, with the small faces'
+        own geometry when `curved` (a warped adapted grid)."""
         self = cls.__new__(cls)
         keep = [np.asfortranarray(a, dtype=np.float64) for a in (points, volume_metrics, surface_metrics)]
         keep += [np.asfortranarray(a, dtype=np.int64) for a in (vmapM, vmapP, boundarycodes)]
@@ -171,6 +173,7 @@ class Grid:
             m = np.asfortranarray(mortars, dtype=np.int64)
             ops = [np.ascontiguousarray(a, dtype=np.float64) for a in tohalves]
             lib().og_grid_set_mortars(self.h, _ptr(m), m.shape[1], *[_ptr(a) for a in ops])
+            lib().og_grid_set_curved_mortars(self.h, int(bool(curved)))
             self._keep += [m] + ops
         return self
 

@@ -133,6 +133,7 @@ struct og_grid {
     std::vector<int64_t> mortars;
     std::vector<double> IL, IU, PL, PU;
     std::vector<uint8_t> ncface;   // (nfaces, E): 1 on faces coupled through a mortar
+    int curved_mortars = 0;        // 1: warped grid, mortar fluxes with the small faces' geometry
 };
 
 // Correctly rounded value of lo + (hi-lo)*i/K (Julia `range(lo, stop=hi, length=K+1)`).
@@ -1067,6 +1068,7 @@ static void mortar_fluxes(const og_grid* g, const Phys& Ph, const double* q, dou
         const int64_t* col = &g->mortars[(size_t)mcols * m];
         const int64_t eC = col[0];
         const int fC = (int)col[1], fF = fC ^ 1;
+        const int nsm = g->nsmet;
         double n[3] = {0, 0, 0};
         n[fC / 2] = (fC % 2) ? 1.0 : -1.0;
         std::vector<double> qC((size_t)ns * nfp), nfm((size_t)nsmall * ns * nfp);
@@ -1092,15 +1094,29 @@ static void mortar_fluxes(const og_grid* g, const Phys& Ph, const double* q, dou
                     qi[s] = acc;
                     qf[s] = q[(size_t)np * ns * eF + (size_t)np * s + v];
                 }
+                double sigma = 1.0;
+                if (g->curved_mortars) {
+                    // warped grid: the small face's own normal (flipped to point out of the
+                    // large element) and surface measure 2^(dim-1) wsJ / W (mortar.cu)
+                    const double* sm = &g->smet[(size_t)nsm * ((size_t)nf * nfp * eF + (size_t)fF * nfp + j)];
+                    for (int d = 0; d < dim; ++d) n[d] = -sm[d];
+                    const double W = dim == 3 ? g->w[j1] * g->w[j2] : g->w[j1];
+                    sigma = (double)nsmall * sm[dim + 1] / W;
+                }
                 surfaceflux(Ph, n, qi, qf, nfl);
                 for (int s = 0; s < ns; ++s) {
-                    nfm[((size_t)k * ns + s) * nfp + j] = nfl[s];
+                    nfm[((size_t)k * ns + s) * nfp + j] = g->curved_mortars ? sigma * nfl[s] : nfl[s];
                     ncflux[(((size_t)nf * eF + fF) * ns + s) * nfp + j] = -nfl[s];
                 }
             }
         }
         for (int j = 0; j < nfp; ++j) {
             const int j1 = j % nq, j2 = j / nq;
+            double unscale = 1.0;  // curved: 1 / sJ of the large face = W / wsJ_C
+            if (g->curved_mortars) {
+                const double W = dim == 3 ? g->w[j1] * g->w[j2] : g->w[j1];
+                unscale = W / g->smet[(size_t)nsm * ((size_t)nf * nfp * eC + (size_t)fC * nfp + j) + dim + 1];
+            }
             for (int s = 0; s < ns; ++s) {
                 double acc = 0.0;
                 for (int k = 0; k < nsmall; ++k) {
@@ -1113,6 +1129,7 @@ static void mortar_fluxes(const og_grid* g, const Phys& Ph, const double* q, dou
                         acc = std::fma(dim == 3 ? Pb[j2 * nq + b] : one, t, acc);
                     }
                 }
+                if (g->curved_mortars) acc = acc * unscale;
                 ncflux[(((size_t)nf * eC + fC) * ns + s) * nfp + j] = acc;
             }
         }
@@ -1193,6 +1210,8 @@ extern "C" void og_grid_set_mortars(og_grid* g, const int64_t* mortars, int64_t 
         for (int k = 2; k < mcols; ++k) g->ncface[(size_t)g->nfaces * col[k] + (col[1] ^ 1)] = 1;
     }
 }
+
+extern "C" void og_grid_set_curved_mortars(og_grid* g, int curved) { g->curved_mortars = curved != 0; }
 
 // ---------------------------------------------------------------------------------
 // LSRK(5,4) (src/balancelaws/odesolvers.jl:9-66, 163-189)

@@ -70,6 +70,9 @@ og_grid* og_grid_from_arrays(int dim, int nq, int64_t E, const double* points, c
  * (nq, nq) row-major interpolation to / projection from the two halves. */
 void og_grid_set_mortars(og_grid* g, const int64_t* mortars, int64_t M, const double* IL, const double* IU,
                          const double* PL, const double* PU);
+/* Warped adapted grid: mortar fluxes with the small faces' own normals and surface
+ * measures, projected so that the coupling conserves (a project-defined extension). */
+void og_grid_set_curved_mortars(og_grid* g, int curved);
 
 /* Standalone LGL operators for nq points (computed in __float128, rounded). */
 void og_lgl(int nq, double* r, double* w, double* D);

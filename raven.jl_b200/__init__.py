@@ -136,7 +136,7 @@ def generate(arg, gm=None):
     """generate(gm) or generate(warp, gm) (src/gridmanager.jl:1084-1208).  `warp` maps
     the coordinate arrays (x, y[, z]) to new ones; a warped grid gets curved metrics.
     A forest that is not one level-0 leaf per tree gives an adapted grid (ForestGrid)
-    whose hanging faces are coupled by mortars."""
+    whose hanging faces are coupled by mortars, warped or not."""
     if gm is None:
         gm, warp = arg, None
     else:
@@ -145,9 +145,7 @@ def generate(arg, gm=None):
         return UnstructuredGrid(gm.cell, gm.coarsegrid, gm.min_level, warp=warp)
     if all(L[1] == 0 for L in gm.forest.leaves):
         return Grid(gm.cell, gm.coarsegrid, warp=warp)
-    if warp is not None:
-        raise NotImplementedError("warped adapted grids are not generated")
-    return ForestGrid(gm.cell, gm.forest, gm.coarsegrid.coordinates)
+    return ForestGrid(gm.cell, gm.forest, gm.coarsegrid.coordinates, warp=warp)
 
 
 # ------------------------------------------------------------------------ laws and fluxes

@@ -1128,8 +1128,8 @@ rb200_status rb200_set_mortars(rb200_handle* h, const int64_t* mortars, int64_t 
     if (h->nmortars > 0) return fail(h, RB200_ERR_BAD_ARG, "mortars are already set");
     if (num_mortars == 0) return RB200_OK;
     if (h->E_active != h->E) return fail(h, RB200_ERR_UNSUPPORTED, "mortars on a grid with ghost elements");
-    if (h->geom != GEOM_AFFINE)
-        return fail(h, RB200_ERR_UNSUPPORTED, "mortars are implemented for unwarped (affine) elements only");
+    if (h->d_vmapP)
+        return fail(h, RB200_ERR_UNSUPPORTED, "mortars on a grid with general (rotated) face connectivity");
     const int nf = h->nf, mcols = 2 + (h->dim == 3 ? 4 : 2);
     DeviceGuard guard(h->device);
     std::vector<int32_t> nbr((size_t)nf * h->E);
@@ -1166,13 +1166,15 @@ rb200_status rb200_set_mortars(rb200_handle* h, const int64_t* mortars, int64_t 
     a.surface_flux = h->sflux;
     a.gamma = h->gamma;
     for (int d = 0; d < 3; ++d) a.adv[d] = h->adv[d];
+    a.sgeo = h->geom == GEOM_CURVED ? h->d_sgeo : nullptr;
+    std::memcpy(a.w, h->w, sizeof(a.w));
     const int q2 = h->nq * h->nq;
     std::memcpy(a.IL, IL, q2 * sizeof(double));
     std::memcpy(a.IU, IU, q2 * sizeof(double));
     std::memcpy(a.PL, PL, q2 * sizeof(double));
     std::memcpy(a.PU, PU, q2 * sizeof(double));
     h->nmortars = num_mortars;
-    h->pipe_curved_grid = 0;  // the curved kernel has no mortar faces (mortars need affine grids anyway)
+    h->pipe_curved_grid = 0;  // the curved pipelined kernel has no mortar faces
     free_graph(h);
     return RB200_OK;
 }

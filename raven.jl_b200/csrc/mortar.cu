@@ -10,6 +10,13 @@
 //   small element's face gets its negative;
 // * the large face gets the lumped L2 projection of the small faces' fluxes, so the
 //   flux integrals match and the coupling conserves.
+// On a curved (warped) grid the small face's own geometry is used: the flux at a small
+// face node is taken with the negative of that face's outward normal, and what is
+// projected onto the large face is the flux scaled by the small face's surface measure,
+// sigma_k = 2^(dim-1) wsJ_k / W (W the tensor LGL weight of the node), which is divided
+// by the large face's sJ = wsJ_C / W afterwards.  With the projection's property
+// W . (P g) = (W / 2^(dim-1)) . g this keeps sum wsJ_C * flux_C = sum_k sum wsJ_k *
+// flux_k, i.e. the coupling conserves on curved faces too.
 // The fluxes are left in a per-face buffer that the stage kernel subtracts like any
 // other face flux (wsJ * nf * MJI).
 //
@@ -85,6 +92,55 @@ __device__ __forceinline__ void face_flux(const MortarArgs& A, int dir, T sn, co
     }
 }
 
+// Surface flux with a general unit normal n (curved faces): the same fluxes as the
+// stage kernel's face phase.
+template <int DIM, bool EULER, typename T>
+__device__ __forceinline__ void face_flux_n(const MortarArgs& A, const T* n, const T* qm, const T* qp, T* nf) {
+    constexpr int NS = EULER ? DIM + 2 : 1;
+    if constexpr (!EULER) {
+        T an = (T)A.adv[0] * n[0];
+#pragma unroll
+        for (int d = 1; d < DIM; ++d) an += (T)A.adv[d] * n[d];
+        const T fc = (an * qm[0] + an * qp[0]) * T(0.5);
+        nf[0] = A.surface_rusanov ? fc - (fabs(an) * (qp[0] - qm[0])) * T(0.5) : fc;
+    } else if (A.surface_flux == kFluxKG || A.surface_flux == kFluxEC || A.surface_flux == kFluxRoe ||
+               A.surface_flux == kFluxMatrix) {
+        euler_entropy_surface_flux<DIM, T>(A.surface_flux, n, qm, qp, (T)A.gamma, nf);
+    } else {
+        const T gm1 = (T)(A.gamma - 1.0);
+        T Fn[2][NS], ws[2];
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            const T* qq = side == 0 ? qm : qp;
+            const T rho = qq[0], rhoe = qq[DIM + 1];
+            T u[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) u[d] = qq[1 + d] / rho;
+            T rr = qq[1] * qq[1];
+#pragma unroll
+            for (int d = 1; d < DIM; ++d) rr = rr + qq[1 + d] * qq[1 + d];
+            const T p = gm1 * (rhoe - rr / (T(2) * rho));
+            T un = u[0] * n[0], mn = qq[1] * n[0];
+#pragma unroll
+            for (int d = 1; d < DIM; ++d) {
+                un += u[d] * n[d];
+                mn += qq[1 + d] * n[d];
+            }
+            Fn[side][0] = mn;
+#pragma unroll
+            for (int b = 0; b < DIM; ++b) Fn[side][1 + b] = mn * u[b] + p * n[b];
+            Fn[side][DIM + 1] = un * (rhoe + p);
+            ws[side] = fabs(un) + dsqrt((T)A.gamma * p / rho);
+        }
+        const T mx = fmax(ws[0], ws[1]);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const T fc = (Fn[0][s] + Fn[1][s]) * T(0.5);
+            nf[s] = A.surface_rusanov ? fc - (mx * (qp[s] - qm[s])) * T(0.5) : fc;
+        }
+    }
+}
+
 // Volume node of in-face index j on face f (x-, x+, y-, y+, z-, z+), lobattocells.jl:2012-2053.
 template <int DIM, int NQ>
 __device__ __forceinline__ int face_vol_node(int f, int j) {
@@ -138,15 +194,38 @@ __global__ void __launch_bounds__((DIM == 3 ? 4 : 2) * Pow<NQ, DIM - 1>::v)
                 qi[s] = acc;
                 qf[s] = (T)__ldg(A.q + ((size_t)eF * NS + s) * NP + v);
             }
-            face_flux<DIM, EULER, T>(A, dir, sn, qi, qf, nf);
+            if (A.sgeo) {
+                // curved: the small face's own normal, flipped to point out of the large
+                // element, and its surface measure for the projection
+                const double* sg = A.sgeo + (((size_t)eF * NF + fF) * NFP + j) * (DIM + 1);
+                T n[DIM];
 #pragma unroll
-            for (int s = 0; s < NS; ++s) {
-                nfm[k][s][j] = nf[s];
-                A.ncflux[(((size_t)eF * NF + fF) * NS + s) * NFP + j] = -(double)nf[s];
+                for (int d = 0; d < DIM; ++d) n[d] = -(T)__ldg(sg + d);
+                face_flux_n<DIM, EULER, T>(A, n, qi, qf, nf);
+                const double W = DIM == 3 ? A.w[j1] * A.w[j2] : A.w[j1];
+                const T sigma = (T)((double)NSMALL * __ldg(sg + DIM) / W);
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    nfm[k][s][j] = sigma * nf[s];
+                    A.ncflux[(((size_t)eF * NF + fF) * NS + s) * NFP + j] = -(double)nf[s];
+                }
+            } else {
+                face_flux<DIM, EULER, T>(A, dir, sn, qi, qf, nf);
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    nfm[k][s][j] = nf[s];
+                    A.ncflux[(((size_t)eF * NF + fF) * NS + s) * NFP + j] = -(double)nf[s];
+                }
             }
         }
         __syncthreads();
         if (t < NFP) {
+            // curved: divide by the large face's sJ = wsJ_C / W
+            T unscale = T(1);
+            if (A.sgeo) {
+                const double W = DIM == 3 ? A.w[j1] * A.w[j2] : A.w[j1];
+                unscale = (T)(W / __ldg(A.sgeo + (((size_t)eC * NF + fC) * NFP + t) * (DIM + 1) + DIM));
+            }
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
                 T acc = T(0);
@@ -162,6 +241,7 @@ __global__ void __launch_bounds__((DIM == 3 ? 4 : 2) * Pow<NQ, DIM - 1>::v)
                         acc = fma(DIM == 3 ? (T)Pb[j2 * NQ + b] : T(1), tt, acc);
                     }
                 }
+                if (A.sgeo) acc = acc * unscale;
                 A.ncflux[(((size_t)eC * NF + fC) * NS + s) * NFP + t] = (double)acc;
             }
         }

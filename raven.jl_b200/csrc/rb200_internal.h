@@ -89,6 +89,10 @@ struct MortarArgs {
     double adv[3];
     double IL[kMaxNq * kMaxNq], IU[kMaxNq * kMaxNq];  // to the halves, [i*nq + j]
     double PL[kMaxNq * kMaxNq], PU[kMaxNq * kMaxNq];  // projections back, [j*nq + i]
+    // curved (warped) grids: the per-face-node (n, wsJ) rows of the stage kernel
+    // ((dim+1, 2*dim*Nfp, E)), null on affine grids; and the LGL weights
+    const double* sgeo;
+    double w[kMaxNq];
 };
 cudaError_t launch_mortars(int dim, int nq, int euler, int fp32, const MortarArgs& a, cudaStream_t s);
 

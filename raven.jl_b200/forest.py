@@ -207,9 +207,13 @@ class ForestGrid:
     vmapP, boundarycodes in Raven's parent layouts), plus:
       mortars  (2 + 2^(dim-1), M) int64, 0-based: large element, its face, then the
                small elements in the order of their position on the face;
-      tohalves (I_lower, I_upper, P_lower, P_upper), the mortar operators."""
+      tohalves (I_lower, I_upper, P_lower, P_upper), the mortar operators.
 
-    def __init__(self, cell, forest, coordinates):
+    With `warp` (a function of the coordinate arrays, as for Grid) the points are warped
+    after they are generated and the metrics are the curved ones (gridmanager.jl:1159-1174);
+    the mortars then couple the hanging faces with the small faces' own geometry."""
+
+    def __init__(self, cell, forest, coordinates, warp=None):
         dim, nq = cell.dim, cell.nq
         self.cell, self.forest = cell, forest
         self.dim, self.nq = dim, nq
@@ -217,7 +221,7 @@ class ForestGrid:
         self.nfp = nq ** (dim - 1)
         self.nfaces = 2 * dim
         self.E = E = len(forest)
-        self.isunwarpedbrick = True
+        self.isunwarpedbrick = warp is None
         r, w = cell.r, cell.w
         coords = [np.asarray(c, dtype=np.float64) for c in coordinates]
         # points: x = muladd(dx, muladd(h, r + 1, cr), c1) with h = 2^-(level+1) and cr the
@@ -234,7 +238,19 @@ class ForestGrid:
                 cr = Fraction(a[d], 1 << LMAX)
                 line = np.array([_fma_exact(dx, float(h * Fraction(r[i] + 1) + cr), c1) for i in range(nq)])
                 pts[:, d, e] = line[idx[d]]
+        if warp is not None:
+            out = warp(*[pts[:, d, :] for d in range(dim)])
+            for d in range(dim):
+                pts[:, d, :] = out[d]
         self.points = pts
+        if warp is not None:
+            from .grids import Grid
+
+            self.volume_metrics = Grid._curved_metrics(self)
+            self._face_maps()
+            self._surface_metrics()
+            self.tohalves = tohalves_operators(nq)
+            return
         # brick metrics from the element's own corners
         last = [nq - 1, nq * (nq - 1), nq * nq * (nq - 1)]
         dX = np.stack([pts[last[d], d, :] - pts[0, d, :] for d in range(dim)])

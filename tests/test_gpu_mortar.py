@@ -97,6 +97,44 @@ def test_mortar_tendency_fp32_bulk(rb, F, case):
         assert rel_err(got[:, s], ref[:, s]) <= 5e-5, s
 
 
+@pytest.mark.parametrize("lw", LAWS, ids=lambda l: l[0])
+@pytest.mark.parametrize("case", [GRIDS[0], GRIDS[2], GRIDS[4]], ids=lambda c: f"{c[0]}d-nq{c[1]}")
+def test_warped_mortar_tendency_and_steps(rb, F, case, lw):
+    """Warped adapted grids (curved mortars): tendency 1e-12 and conservation on the GPU,
+    FP64 steps 1e-12, FP32-bulk tendency 5e-5."""
+    from test_forest_host import periodic_warp
+
+    dim, nq, K, per, levels = case
+    grid, _ = _adapted(rb, F, dim, nq, K, (True,) * dim, levels, warp=periodic_warp(K, 0.05))
+    assert grid.mortars.size > 0 and not grid.isunwarpedbrick
+    dg, law, olaw = _product(rb, grid, lw)
+    og = _oracle(grid)
+    q = _state(grid, olaw, 8)
+    ref = og.tendency(olaw, q)
+    qg, dqg = rb.GridArray.from_numpy(q), rb.GridArray.from_numpy(np.zeros_like(q))
+    dg(dqg, qg, 0.0, increment=False)
+    dg.sync_status()
+    got = dqg.numpy()
+    MJ = grid.volume_weights()
+    for s in range(olaw.ns):
+        assert rel_err(got[:, s], ref[:, s]) <= 1e-12, s
+        assert abs((MJ * got[:, s]).sum()) <= 1e-13 * np.abs(MJ * got[:, s]).sum()
+    dt, steps = 1e-3, 6
+    qo, dqo = np.asfortranarray(q.copy()), og.state(olaw)
+    for i in range(steps):
+        og.lsrk54_step(olaw, qo, dqo, i * dt, dt)
+    qs = rb.GridArray.from_numpy(q)
+    rb.LSRK54(dg, qs, dt).dostep(qs, steps)
+    dg.sync_status()
+    for s in range(olaw.ns):
+        assert rel_err(qs.numpy()[:, s], qo[:, s]) <= 1e-12, s
+    dg32, _, _ = _product(rb, grid, lw, precision="fp32_bulk")
+    d32 = rb.GridArray.from_numpy(np.zeros_like(q))
+    dg32(d32, rb.GridArray.from_numpy(q), 0.0, increment=False)
+    for s in range(olaw.ns):
+        assert rel_err(d32.numpy()[:, s], ref[:, s]) <= 5e-5, s
+
+
 def test_mortar_setup_errors(rb, F):
     grid, _ = _adapted(rb, F, 2, 4, (3, 2), (True, True), 2)
     bad = grid.mortars.copy()
