@@ -26,6 +26,7 @@ process (`fp32_bulk`), its accuracy against the FP64 form and the exact solution
 """
 
 import argparse
+import ctypes
 import importlib.util
 import json
 import math
@@ -256,7 +257,15 @@ def profiled_traffic(name):
     return profiled_figure(name, "dram_bytes_per_launch")
 
 
-FP64_NOMINAL_TFLOPS = 37.0  # B200 datasheet FP64 (no measured FP64 peak is available)
+FP64_NOMINAL_TFLOPS = 37.0  # B200 datasheet FP64, used only if the measurement fails
+
+
+def measured_fp64_tflops(rb):
+    """FP64 fma throughput of this GPU (rb200_probe_fp64_rate: 8 CTAs per SM x 256
+    threads x 8 independent fma chains, CUDA events, best of 3), or None."""
+    out = ctypes.c_double(0.0)
+    st = rb._lib.lib().rb200_probe_fp64_rate(1 << 16, ctypes.byref(out), None)
+    return out.value if st == 0 and out.value > 0 else None
 
 
 def stage_bytes_per_launch(w, nodes, ns):
@@ -1080,8 +1089,12 @@ def main(argv=None):
         # the second roofline of the FP64 path: FP64 flops the kernel executes (ncu counters
         # of the committed summary, DFMA = 2) per launch over the launch time
         tf = flops_node * nodes / (ms / 1e3 / launches) / 1e12
-        fp64_pipe = {"achieved": tf, "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s", "frac": tf / FP64_NOMINAL_TFLOPS,
-                     "peak_source": "nominal (datasheet)", "flops_per_node_stage": flops_node}
+        peak64 = measured_fp64_tflops(rb)
+        src = "measured (rb200_probe_fp64_rate, after the timed region)"
+        if peak64 is None:
+            peak64, src = FP64_NOMINAL_TFLOPS, "nominal (datasheet)"
+        fp64_pipe = {"achieved": tf, "peak": peak64, "unit": "TFLOP/s", "frac": tf / peak64,
+                     "peak_source": src, "flops_per_node_stage": flops_node}
     # a short serving stream (config 4's generator) on the same GPU, after the timed work
     serving = None
     if args.serving_requests > 0 and args.workload == DEFAULT and w["K"] == WORKLOADS[DEFAULT]["K"]:

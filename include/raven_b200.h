@@ -245,6 +245,12 @@ rb200_status rb200_sync_status(rb200_handle* h, void* stream);
  * Synchronous on `stream`; allocates and frees 4 bytes of device memory. */
 rb200_status rb200_probe_bounded_wait(int64_t polls, void* stream);
 
+/* Measures the device's FP64 fma throughput: a grid of 8 CTAs per SM x 256 threads,
+ * each thread running 8 independent chains of `iters` fmas (4..2^26, a multiple of 4),
+ * timed with CUDA events on `stream` (best of 3 after a warm-up launch).  Writes
+ * TFLOP/s (2 flops per fma) to *tflops_out.  Synchronous. */
+rb200_status rb200_probe_fp64_rate(int64_t iters, double* tflops_out, void* stream);
+
 /* Handle properties: info[0]=dim, [1]=nq, [2]=Ns, [3]=E, [4]=geometry kind
  * (0 affine brick, 1 curved), [5]=precision, [6]=kernel launches per LSRK step,
  * [7]=algorithmic HBM bytes per node per stage, [8]=CTAs of the pipelined kernel of the

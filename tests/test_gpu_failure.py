@@ -31,3 +31,16 @@ def test_bounded_wait_times_out_and_the_context_survives(rb, cuda_ok):
     dg(dqg, qg, 0.0, increment=False)
     dg.sync_status()  # the handle's own status word saw no timeout
     assert rel_err(dqg.numpy(), ref) <= 1e-12
+
+
+def test_fp64_rate_probe(rb, cuda_ok):
+    """The FP64 throughput probe behind the bench's arithmetic roofline: a plausible
+    B200 figure (nominal 37-40 TFLOP/s), and argument checks before any device call."""
+    import ctypes
+
+    L = rb._lib.lib()
+    out = ctypes.c_double(0.0)
+    assert L.rb200_probe_fp64_rate(3, ctypes.byref(out), None) == 1
+    assert L.rb200_probe_fp64_rate(1 << 12, None, None) == 1
+    assert L.rb200_probe_fp64_rate(1 << 14, ctypes.byref(out), None) == 0
+    assert 10.0 < out.value < 100.0
