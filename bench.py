@@ -405,6 +405,67 @@ def fp32_bulk_leg(rb, w, grid, law, q0, dt, args, ms64, local, stream, barrier, 
     return out
 
 
+# The other configurations, timed in the default run after its own legs so that one record
+# holds them all: (label, workload, steps; None = the run's --steps).
+OTHER_CONFIGS = [
+    ("config 1: 2-D advection 16^2, N=4, 100 steps", "adv2d_weak_n4_16_fp64", 100),
+    ("config 3: warped 32^3 Euler KG, FP32 bulk", "euler3d_kg_n7_32_fp32bulk_warped", None),
+    ("config 3's FP64 comparison run: the same warped grid in FP64", "euler3d_kg_n7_32_fp64_warped", None),
+    ("config 5: adapted 3-D Euler KG, N=5, FP32 bulk", "euler3d_kg_n5_adapted_fp32bulk", 100),
+]
+
+
+def other_configs_leg(rb, args, local, stream, barrier, dist, world):
+    """Each of OTHER_CONFIGS timed like the main line (warm-up, CUDA events over the
+    steps), with its roofline where its state is larger than L2."""
+    out = []
+    problems = {}
+    for label, name, steps in OTHER_CONFIGS:
+        w = dict(WORKLOADS[name])
+        key = (w["dim"], w["N"], w["K"], w["law"], w["warp"], bool(w.get("adapted")))
+        if key not in problems:
+            problems = {key: problem(rb, w)}  # keep one grid alive at a time
+        grid, law, form, q0, dt = problems[key]
+        dg = rb.DGSEM(law=law, grid=grid, volume_form=form, surface_numericalflux=rb.RusanovFlux(),
+                      precision=w["precision"], device=local)
+        n = steps or args.steps
+        q = rb.GridArray.from_numpy(q0)
+        dq = q.similar()
+        dg.lsrk54_steps(q, dq, 0.0, dt, args.warmup)
+        sampler = ClockSampler(local)
+        sampler.start()
+        time.sleep(0.2)
+        ms = timed_steps(dg, q, dq, args.warmup * dt, dt, n, stream, barrier, dist)
+        sampler.stop()
+        nodes, ns = grid.np * grid.E, law.ns
+        launches = int(dg.info[6]) * n  # stage kernels (and mortar kernels) per step
+        rec = {
+            "label": label,
+            "config": config_json(name, w, grid),
+            "steps": n,
+            "warmup": args.warmup,
+            "ms_per_step": ms / n,
+            "value": world * nodes * ns * 5 * n / (ms / 1e3),
+            "unit": UNIT,
+            "gpu_launches": launches,
+            "kernel": kernel_name(w, dg),
+            "clocks": sampler.summary(),
+        }
+        if w["K"] >= 32:
+            peak, peak_kind = measured_peaks()
+            bytes_launch = stage_bytes_per_launch(w, nodes, ns)
+            achieved = bytes_launch / (ms / 1e3 / (5 * n)) / 1e9
+            rec["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                               "frac": achieved / peak, "peak_source": peak_kind,
+                               "algorithmic_bytes_per_launch": bytes_launch, "traffic": profiled_traffic(name)}
+        else:
+            rec["roofline"] = None
+            rec["note"] = "state is L2-resident (a few MB): no HBM roofline"
+        out.append(rec)
+        del q, dq, dg
+    return out
+
+
 def adapted_oracle(w):
     """The adapted workload's grid and initial state for the oracle: the forest and its
     arrays are generated on the host (setup, untimed), the oracle couples the hanging
@@ -931,6 +992,8 @@ def main(argv=None):
     p.add_argument("--no-fp32-leg", action="store_true", help="skip the FP32-bulk sub-measurement")
     p.add_argument("--serving-requests", type=int, default=40,
                    help="requests of the short serving stream of the default line (0: skip)")
+    p.add_argument("--no-other-configs", action="store_true",
+                   help="skip timing the other configurations (1, 3, 5) in the default run")
     args = p.parse_args(argv)
     if args.workload == SERVE_WORKLOAD:
         return run_serving(args)
@@ -979,7 +1042,7 @@ def main(argv=None):
     ms = timed_steps(dg, q, dq, args.warmup * dt, dt, args.steps, stream, barrier, dist)
     sampler.stop()
     value = world * nodes * ns * 5 * args.steps / (ms / 1e3)
-    launches = 5 * args.steps
+    launches = int(dg.info[6]) * args.steps  # stage kernels (and mortar kernels) per step
 
     # the FP32-bulk form of the same workload, timed the same way in the same process
     fp32_leg = None
@@ -1070,7 +1133,7 @@ def main(argv=None):
 
     peak, peak_kind = measured_peaks()
     bytes_launch = stage_bytes_per_launch(w, nodes, ns)
-    achieved = bytes_launch / (ms / 1e3 / launches) / 1e9
+    achieved = bytes_launch / (ms / 1e3 / (5 * args.steps)) / 1e9  # per stage-kernel launch
     traffic = profiled_traffic(args.workload)
     roofline = {
         "bound": "hbm",
@@ -1088,7 +1151,7 @@ def main(argv=None):
     if flops_node and w["precision"] == "fp64":
         # the second roofline of the FP64 path: FP64 flops the kernel executes (ncu counters
         # of the committed summary, DFMA = 2) per launch over the launch time
-        tf = flops_node * nodes / (ms / 1e3 / launches) / 1e12
+        tf = flops_node * nodes / (ms / 1e3 / (5 * args.steps)) / 1e12
         peak64 = measured_fp64_tflops(rb)
         src = "measured (rb200_probe_fp64_rate, after the timed region)"
         if peak64 is None:
@@ -1103,6 +1166,14 @@ def main(argv=None):
                            "state on the host; at 200/s the stream offers more work than the GPU drains, "
                            "so latency there includes queueing; the lower rate is below the drain rate",
                    "streams": serving_leg(rb, local, args.serving_requests, (200.0, 10.0), args.seed)}
+
+    others = None
+    if (world == 1 and not args.no_other_configs and args.workload == DEFAULT
+            and w["K"] == WORKLOADS[DEFAULT]["K"]):
+        if serving is None:
+            del q, dq
+        del dg
+        others = other_configs_leg(rb, args, local, stream, barrier, dist, world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1133,6 +1204,7 @@ def main(argv=None):
             "vs_fp64": fp64_cmp,
             "fp32_bulk": fp32_leg,
             "serving": serving,
+            "other_configs": others,
             "dt": dt,
         }
         print(json.dumps(line))

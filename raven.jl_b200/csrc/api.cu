@@ -1202,7 +1202,7 @@ rb200_status rb200_get_info(const rb200_handle* h, int64_t* info, int32_t n) {
     int64_t per_node = h->ns * (2 * bytes_q + 2 * bytes_dq);
     if (h->geom == GEOM_CURVED)
         per_node += (h->dim * h->dim + 1) * 8 + (int64_t)h->nf * h->nfp * (h->dim + 1) * 8 / h->np;
-    const int64_t v[9] = {h->dim, h->nq, h->ns, h->E, h->geom, h->prec, 5, per_node,
+    const int64_t v[9] = {h->dim, h->nq, h->ns, h->E, h->geom, h->prec, h->nmortars > 0 ? 10 : 5, per_node,
                           h->geom == GEOM_CURVED ? h->pipe_curved_grid : h->pipe_grid};
     for (int i = 0; i < n && i < 9; ++i) info[i] = v[i];
     return RB200_OK;
