@@ -234,6 +234,14 @@ rb200_status rb200_set_mortars(rb200_handle* h, const int64_t* mortars, int64_t 
  * other configuration runs the generic stage kernel. */
 rb200_status rb200_set_kernel_path(rb200_handle* h, int32_t path);
 
+/* DGSEM(; directions)  (dgsem.jl:46-81): the volume term (dgsem.jl:257-348, 514-608) and
+ * the surface term (dgsem.jl:756-782) are computed for the directions in `mask` only (bit
+ * d = direction d + 1, e.g. 3 = directions (1, 2) of a 3-D grid, 4 = direction 3).  The
+ * default is every direction; a proper subset runs the generic stage kernel.  mask must
+ * be a non-empty subset of 1:dim (BAD_ARG otherwise).  Applies to every later tendency
+ * and step of the handle. */
+rb200_status rb200_set_directions(rb200_handle* h, int32_t mask);
+
 /* Synchronizes `stream` and returns RB200_ERR_TIMEOUT if a kernel of this handle gave
  * up a bounded wait since the handle was created, RB200_OK otherwise. */
 rb200_status rb200_sync_status(rb200_handle* h, void* stream);

@@ -4,7 +4,8 @@
 # [extensions], like RavenCUDAExt: see julia/Project.extension.toml).  It keeps Raven's
 # Grid, GridArray{SVector{Ns,FT}} (CuArray-backed) and balance laws; only the device work
 # behind these calls is redirected to the C ABI of include/raven_b200.h:
-#   (dg::DGSEM)(dq, q, t; increment)            src/balancelaws/dgsem.jl:84-126
+#   (dg::DGSEM)(dq, q, t; increment)            src/balancelaws/dgsem.jl:84-126, with the
+#     DGSEM's directions (dgsem.jl:46-81)
 #   solve!(q, timeend, solver; after_step,       src/balancelaws/odesolvers.jl:9-30
 #          after_stage, adjust_final)
 #   dostep!(q, ::LSRK / ::RLSRK, after_stage)    odesolvers.jl:51-61, 118-151, for the
@@ -103,6 +104,12 @@ function B200DGSEM(dg::DGSEM; precision = :fp64)
                          pointer(bc), CUDA.deviceid(CUDA.device()))
         st = ccall((:rb200_create, lib), Cint, (Ref{RB200Desc}, Ref{Ptr{Cvoid}}), desc, h)
         check(st, h[])
+    end
+    # DGSEM(; directions) (dgsem.jl:46-81): the volume and surface terms of those directions
+    dirs = Raven.BalanceLaws.directions(dg)
+    if length(dirs) < ndims(cell)
+        mask = Int32(sum(1 << (d - 1) for d in dirs))
+        check(ccall((:rb200_set_directions, lib), Cint, (Ptr{Cvoid}, Int32), h[], mask), h[])
     end
     b = B200DGSEM(dg, h[])
     finalizer(x -> ccall((:rb200_destroy, lib), Cint, (Ptr{Cvoid},), x.handle), b)

@@ -74,6 +74,7 @@ def lib():
         L.og_grid_from_arrays.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int64, P, P, P, P, P, P]
         L.og_grid_set_mortars.argtypes = [P, P, ctypes.c_int64, P, P, P, P]
         L.og_grid_set_curved_mortars.argtypes = [P, ctypes.c_int]
+        L.og_grid_set_directions.argtypes = [P, ctypes.c_int]
         for name in ("og_grid_sizes", "og_grid_points", "og_grid_vmet", "og_grid_smet", "og_grid_vmapM",
                      "og_grid_vmapP", "og_grid_boundary", "og_grid_tree_coords"):
             getattr(L, name).argtypes = [P, P]
@@ -232,6 +233,10 @@ class Grid:
         lib().og_tendency(self.h, ctypes.byref(law.c), _ptr(dq), _ptr(q), t, int(increment), e0,
                           self.E if e1 is None else e1)
         return dq
+
+    def set_directions(self, directions):
+        """DGSEM(; directions): 1-based directions whose terms are computed."""
+        lib().og_grid_set_directions(self.h, sum(1 << (int(d) - 1) for d in directions))
 
     def lsrk54_step(self, law, q, dq, time, dt):
         lib().og_lsrk54_step(self.h, ctypes.byref(law.c), _ptr(q), _ptr(dq), time, dt)

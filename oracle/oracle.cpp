@@ -134,6 +134,7 @@ struct og_grid {
     std::vector<double> IL, IU, PL, PU;
     std::vector<uint8_t> ncface;   // (nfaces, E): 1 on faces coupled through a mortar
     int curved_mortars = 0;        // 1: warped grid, mortar fluxes with the small faces' geometry
+    int dir_mask = 0;              // DGSEM(; directions) as a bit mask (dgsem.jl:46-81); 0 = all
 };
 
 // Correctly rounded value of lo + (hi-lo)*i/K (Julia `range(lo, stop=hi, length=K+1)`).
@@ -923,6 +924,9 @@ static void element_tendency(const og_grid* g, const Phys& Ph, double* dq, const
     };
     auto ijk = [&](int n, int* idx) { idx[0] = n % nq; idx[1] = (n / nq) % nq; idx[2] = n / (nq * nq); };
     auto lin = [&](int i, int j, int k) { return i + nq * (j + nq * k); };
+    // `d in directions` (dgsem.jl:257-348, 203-227, 756-782)
+    const int dmask = g->dir_mask ? g->dir_mask : (1 << dim) - 1;
+    auto in_dirs = [&](int d) { return ((dmask >> d) & 1) != 0; };
 
     if (Ph.L.form == OG_FORM_WEAK) {
         // volumeterm! (dgsem.jl:257-348)
@@ -952,6 +956,7 @@ static void element_tendency(const og_grid* g, const Phys& Ph, double* dq, const
                 for (int d = 0; d < dim; ++d) Dd[d] = Dm(a, id[d]) * mji;
                 for (int s = 0; s < ns; ++s) {
                     for (int d = 0; d < dim; ++d) {
+                        if (!in_dirs(d)) continue;
                         int nb = (d == 0) ? lin(a, id[1], id[2]) : (d == 1 ? lin(id[0], a, id[2]) : lin(id[0], id[1], a));
                         acc[s] += Dd[d] * lF[((size_t)nb * dim + d) * ns + s];
                     }
@@ -966,10 +971,13 @@ static void element_tendency(const og_grid* g, const Phys& Ph, double* dq, const
         // esvolumeterm_dir! per direction (dgsem.jl:203-227, 514-608)
         scratch.resize((size_t)np * 3);
         double* lg = scratch.data();
+        int first_dir = 0;
+        while (!in_dirs(first_dir)) ++first_dir;
         for (int dir = 0; dir < dim; ++dir) {
+            if (!in_dirs(dir)) continue;
             for (int n = 0; n < np; ++n)
                 for (int d = 0; d < dim; ++d) lg[n * 3 + d] = MJ(n) * dRdX(n, dir, d);
-            bool inc = (dir == 0) ? increment : true;
+            bool inc = (dir == first_dir) ? increment : true;
             for (int n = 0; n < np; ++n) {
                 int id3[3];
                 ijk(n, id3);
@@ -1003,6 +1011,7 @@ static void element_tendency(const og_grid* g, const Phys& Ph, double* dq, const
     // surfaceterm! (dgsem.jl:733-784): faces in order x-, x+, y-, y+, z-, z+
     const int nfp = g->nfp, nf = g->nfaces, nsm = g->nsmet;
     for (int face = 0; face < nf; ++face) {
+        if (!in_dirs(face / 2)) continue;
         for (int i = 0; i < nfp; ++i) {
             size_t j = (size_t)nf * nfp * e + (size_t)face * nfp + i;
             int64_t idm = g->vmapM[j] - 1;
@@ -1212,6 +1221,11 @@ extern "C" void og_grid_set_mortars(og_grid* g, const int64_t* mortars, int64_t 
 }
 
 extern "C" void og_grid_set_curved_mortars(og_grid* g, int curved) { g->curved_mortars = curved != 0; }
+
+extern "C" void og_grid_set_directions(og_grid* g, int mask) {
+    const int all = (1 << g->dim) - 1;
+    g->dir_mask = (mask == all) ? 0 : (mask & all);
+}
 
 // ---------------------------------------------------------------------------------
 // LSRK(5,4) (src/balancelaws/odesolvers.jl:9-66, 163-189)

@@ -73,6 +73,9 @@ void og_grid_set_mortars(og_grid* g, const int64_t* mortars, int64_t M, const do
 /* Warped adapted grid: mortar fluxes with the small faces' own normals and surface
  * measures, projected so that the coupling conserves (a project-defined extension). */
 void og_grid_set_curved_mortars(og_grid* g, int curved);
+/* DGSEM(; directions): volume and surface terms of the directions in `mask` only (bit d =
+ * direction d + 1; all when mask covers every direction). */
+void og_grid_set_directions(og_grid* g, int mask);
 
 /* Standalone LGL operators for nq points (computed in __float128, rounded). */
 void og_lgl(int nq, double* r, double* w, double* D);

@@ -291,12 +291,16 @@ def _stream_ptr():
 
 
 class DGSEM:
-    """DGSEM(; law, grid, surface_numericalflux, volume_form) (src/balancelaws/dgsem.jl:46-81).
+    """DGSEM(; law, grid, surface_numericalflux, volume_form, directions) (src/balancelaws/dgsem.jl:46-81).
 
+    directions: the 1-based directions whose volume and surface terms are computed, as
+    Raven's `directions = 1:ndims(law)` (default: all), e.g. (1, 2) or (3,) for a split
+    into horizontal and vertical operators.
     precision: "fp64" (plain FP64) or "fp32_bulk" (FP32 volume/surface arithmetic, FP64
     geometry, state accumulation and reductions)."""
 
-    def __init__(self, *, law, grid, surface_numericalflux, volume_form=None, precision="fp64", device=None):
+    def __init__(self, *, law, grid, surface_numericalflux, volume_form=None, directions=None, precision="fp64",
+                 device=None):
         torch = _torch()
         if not torch.cuda.is_available():
             raise RuntimeError("raven_b200.DGSEM needs a CUDA device (no CPU fallback)")
@@ -305,6 +309,12 @@ class DGSEM:
             raise ValueError("law and grid dimensions differ")
         if precision not in ("fp64", "fp32_bulk"):
             raise ValueError("precision must be 'fp64' or 'fp32_bulk'")
+        if directions is None:
+            directions = tuple(range(1, grid.dim + 1))
+        directions = tuple(int(d) for d in directions)
+        if not directions or any(d < 1 or d > grid.dim for d in directions) or len(set(directions)) != len(directions):
+            raise ValueError(f"directions must be distinct values in 1:{grid.dim}")
+        self.directions = directions
         self.law, self.grid, self.volume_form = law, grid, volume_form
         self.surface_numericalflux = surface_numericalflux
         self.precision = precision
@@ -349,6 +359,14 @@ class DGSEM:
             ops = [np.ascontiguousarray(a, dtype=np.float64) for a in grid.tohalves]
             st = L.rb200_set_mortars(h, m.ctypes.data_as(ctypes.c_void_p), m.shape[1],
                                      *[a.ctypes.data_as(ctypes.c_void_p) for a in ops])
+            if st != 0:
+                msg = L.rb200_last_error(h).decode()
+                L.rb200_destroy(h)
+                self._h = None
+                raise RB200Error(st, msg)
+        if len(directions) < grid.dim:
+            mask = sum(1 << (d - 1) for d in directions)
+            st = L.rb200_set_directions(h, mask)
             if st != 0:
                 msg = L.rb200_last_error(h).decode()
                 L.rb200_destroy(h)

@@ -54,6 +54,7 @@ EXPORTED = [
     "rb200_sync_status",
     "rb200_probe_bounded_wait",
     "rb200_probe_fp64_rate",
+    "rb200_set_directions",
     "rb200_weighted_sums_noalloc",
     "rb200_server_create",
     "rb200_server_submit",
@@ -183,6 +184,7 @@ def lib():
     L.rb200_sync_status.argtypes = [P, P]
     L.rb200_probe_bounded_wait.argtypes = [I64, P]
     L.rb200_probe_fp64_rate.argtypes = [I64, P, P]
+    L.rb200_set_directions.argtypes = [P, I32]
     L.rb200_weighted_sums_noalloc.argtypes = [P, P, I32, I32, I64, P, P]
     L.rb200_last_error.argtypes = [P]
     L.rb200_last_error.restype = ctypes.c_char_p

@@ -54,6 +54,7 @@ struct rb200_handle {
     int32_t* d_status = nullptr;  // bounded-wait error word written by the kernels
     int red_blocks = 0;
     int kernel_path = 0;          // 0 automatic, 1 generic stage kernel only
+    int dir_mask = 0;             // DGSEM(; directions) as a bit mask; 0 = all directions
     // CUDA graph of two LSRK steps (10 stage launches) for one (q, dq, dt), replayed by
     // rb200_lsrk54_step; captured on a stream of the handle, launched on the caller's
     cudaStream_t cap_stream = nullptr;
@@ -205,7 +206,9 @@ cudaError_t launch_any(rb200_handle* h, const StageArgs& a, cudaStream_t st) {
         if (e != cudaSuccess) return e;
     }
     const bool stage_mode = a.mode >= MODE_STAGE;
-    if (h->pipe_curved_grid > 0 && h->kernel_path == 0 && stage_mode && aligned16(a.q_in) && aligned16(a.q_out) &&
+    // the pipelined kernels compute every direction; a direction subset runs the generic one
+    const bool all_dirs = h->dir_mask == 0;
+    if (all_dirs && h->pipe_curved_grid > 0 && h->kernel_path == 0 && stage_mode && aligned16(a.q_in) && aligned16(a.q_out) &&
         aligned16(a.dq)) {
         PipeCurvedArgs c;
         std::memset(&c, 0, sizeof(c));
@@ -229,7 +232,7 @@ cudaError_t launch_any(rb200_handle* h, const StageArgs& a, cudaStream_t st) {
         return h->prec == RB200_PRECISION_FP64 ? launch_pipelined_curved64(c, grid, st)
                                                : launch_pipelined_curved(c, grid, st);
     }
-    const bool eligible = h->kernel_path == 0 && h->pipe_grid > 0 && aligned16(a.q_in) && aligned16(a.dq) &&
+    const bool eligible = all_dirs && h->kernel_path == 0 && h->pipe_grid > 0 && aligned16(a.q_in) && aligned16(a.dq) &&
                           (!stage_mode || aligned16(a.q_out)) &&
                           (h->prec == RB200_PRECISION_FP64 || stage_mode);
     if (!eligible) return launch_stage(h->dim, h->nq, h->combo, h->geom, h->prec, a, st);
@@ -266,6 +269,7 @@ StageArgs base_args(const rb200_handle* h) {
     a.nbr = h->d_nbr;
     a.ncflux = h->d_ncflux;
     a.vmapP = h->d_vmapP;
+    a.dir_mask = h->dir_mask;
     a.E = h->E_active;
     a.surface_rusanov = h->sflux == RB200_FLUX_RUSANOV ? 1 : 0;
     a.surface_flux = h->sflux;
@@ -1181,7 +1185,24 @@ rb200_status rb200_set_mortars(rb200_handle* h, const int64_t* mortars, int64_t 
 
 rb200_status rb200_set_kernel_path(rb200_handle* h, int32_t path) {
     if (!h || path < 0 || path > 1) return RB200_ERR_BAD_ARG;
+    if (path != h->kernel_path) {
+        DeviceGuard guard(h->device);
+        free_graph(h);  // a captured step holds the other kernel
+    }
     h->kernel_path = path;
+    return RB200_OK;
+}
+
+rb200_status rb200_set_directions(rb200_handle* h, int32_t mask) {
+    if (!h) return RB200_ERR_BAD_ARG;
+    const int32_t all = (1 << h->dim) - 1;
+    if (mask < 1 || mask > all) return fail(h, RB200_ERR_BAD_ARG, "directions: a non-empty subset of 1:dim");
+    const int32_t m = mask == all ? 0 : mask;
+    if (m != h->dir_mask) {
+        DeviceGuard guard(h->device);
+        free_graph(h);  // a captured step holds the old directions
+    }
+    h->dir_mask = m;
     return RB200_OK;
 }
 
@@ -1203,7 +1224,7 @@ rb200_status rb200_get_info(const rb200_handle* h, int64_t* info, int32_t n) {
     if (h->geom == GEOM_CURVED)
         per_node += (h->dim * h->dim + 1) * 8 + (int64_t)h->nf * h->nfp * (h->dim + 1) * 8 / h->np;
     const int64_t v[9] = {h->dim, h->nq, h->ns, h->E, h->geom, h->prec, h->nmortars > 0 ? 10 : 5, per_node,
-                          h->geom == GEOM_CURVED ? h->pipe_curved_grid : h->pipe_grid};
+                          h->dir_mask ? 0 : (h->geom == GEOM_CURVED ? h->pipe_curved_grid : h->pipe_grid)};
     for (int i = 0; i < n && i < 9; ++i) info[i] = v[i];
     return RB200_OK;
 }

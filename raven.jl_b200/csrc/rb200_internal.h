@@ -69,6 +69,8 @@ struct StageArgs {
     int32_t mode;
     int32_t surface_rusanov;  // 1 Rusanov, 0 central (with surface_flux Rusanov or central)
     int32_t surface_flux;     // kFlux*: the entropy family (EC, KG, Roe, matrix) runs its own kernels
+    int32_t dir_mask;         // DGSEM(; directions): bit d set = direction d's volume and face terms
+                              // are computed (dgsem.jl:46-81, 257-348, 733-784); 0 reads as all
     double rka;
     double rkb_dt;
     double gamma;

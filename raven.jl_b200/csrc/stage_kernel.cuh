@@ -177,9 +177,11 @@ __device__ __forceinline__ void stage_element_adv_brick(const StageArgs& A, cons
 
     // ---- volume term
     const T* qe = sq + el * NP;
+    const int dmask = A.dir_mask ? A.dir_mask : 7;
     T acc = T(0);
 #pragma unroll
     for (int dir = 0; dir < DIM; ++dir) {
+        if (!((dmask >> dir) & 1)) continue;
         const int stride = dir == 0 ? 1 : (dir == 1 ? NQ : NQ * NQ);
         const int idd = id[dir];
         const int base = n - idd * stride;
@@ -208,6 +210,7 @@ __device__ __forceinline__ void stage_element_adv_brick(const StageArgs& A, cons
     for (int dir = 0; dir < DIM; ++dir) {
         const int idd = id[dir];
         if (idd != 0 && idd != NQ - 1) continue;
+        if (!((dmask >> dir) & 1)) continue;
         const int side = idd == 0 ? 0 : 1;
         const int f = 2 * dir + side;
         const int stride = dir == 0 ? 1 : (dir == 1 ? NQ : NQ * NQ);
@@ -398,9 +401,11 @@ __device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs
     T acc[NS];
 #pragma unroll
     for (int s = 0; s < NS; ++s) acc[s] = T(0);
+    const int dmask = A.dir_mask ? A.dir_mask : 7;  // DGSEM(; directions)
 
 #pragma unroll
     for (int dir = 0; dir < DIM; ++dir) {
+        if (!((dmask >> dir) & 1)) continue;
         const int stride = dir == 0 ? 1 : (dir == 1 ? NQ : NQ * NQ);
         const int idd = id[dir];
         const int base = n - idd * stride;
@@ -521,6 +526,7 @@ __device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs
     for (int dir = 0; dir < DIM; ++dir) {
         const int idd = id[dir];
         if (idd != 0 && idd != NQ - 1) continue;
+        if (!((dmask >> dir) & 1)) continue;
 #pragma unroll
         for (int side = 0; side < 2; ++side) {
             if ((side == 0 && idd != 0) || (side == 1 && idd != NQ - 1)) continue;

@@ -162,3 +162,26 @@ def test_oracle_lsrk144_matches_lsrk54_golden():
     assert e54 == pytest.approx(entry["expected"], rel=entry["rtol"])
     assert e144 == pytest.approx(entry["expected"], rel=1e-3)
     assert np.abs(q144 - q54).max() < 1e-5  # time error; the spatial error is ~1e-3 in max norm
+
+
+@pytest.mark.parametrize("form,vf", [(O.FORM_WEAK, O.FLUX_CENTRAL), (O.FORM_FLUXDIFF, O.FLUX_KG),
+                                     (O.FORM_FLUXDIFF, O.FLUX_EC)], ids=["weak", "kg", "ec"])
+@pytest.mark.parametrize("dim,warp", [(2, O.WARP_NONE), (3, O.WARP_NONE), (3, O.WARP_SINE)])
+def test_oracle_directions_split_the_tendency(dim, warp, form, vf):
+    """DGSEM(; directions) (dgsem.jl:46-81): the volume and surface terms are sums over
+    directions, so the tendencies of the single directions add up to the full one
+    (1e-13 of its scale), and a subset that holds every direction is the full tendency
+    bit for bit."""
+    nq, K = 4, (3, 2, 2)[:dim]
+    og = O.Grid(dim, nq, K, [0.0] * dim, [10.0] * dim, [True] * dim, warp, 0.1 if warp == O.WARP_SINE else 0.0)
+    law = O.Law(O.LAW_EULER, dim, form=form, volume_flux=vf)
+    q = og.initial_condition(law, 1)
+    q = np.asfortranarray(q * (1 + 0.01 * np.random.default_rng(5).standard_normal(q.shape)))
+    full = og.tendency(law, q)
+    parts = np.zeros_like(full)
+    for d in range(1, dim + 1):
+        og.set_directions([d])
+        parts += og.tendency(law, q)
+    assert np.abs(parts - full).max() <= 1e-13 * np.abs(full).max()
+    og.set_directions(range(1, dim + 1))
+    assert np.array_equal(og.tendency(law, q), full)
