@@ -53,8 +53,8 @@ class LobattoCell:
     """LobattoCell{Float64}(Nq...) (src/lobattocells.jl:89-250); all directions equal."""
 
     def __init__(self, *sizes):
-        if len(sizes) not in (2, 3) or len(set(sizes)) != 1:
-            raise ValueError("LobattoCell needs 2 or 3 equal sizes (cubic cells, dgsem.jl:92)")
+        if len(sizes) not in (1, 2, 3) or len(set(sizes)) != 1:
+            raise ValueError("LobattoCell needs 1, 2 or 3 equal sizes (cubic cells, dgsem.jl:92)")
         self.dim = len(sizes)
         self.nq = int(sizes[0])
         if not 2 <= self.nq <= 8:
@@ -112,12 +112,19 @@ class GridManager:
                 raise ValueError("cell and coarse grid dimensions differ")
             self.forest = None
             return
+        if cell.dim == 1:  # a line: uniform refinement only, as the reference's 1-D forest
+            if len(coarsegrid.coordinates) != 1:
+                raise ValueError("cell and coarse grid dimensions differ")
+            self.forest = None
+            return
         if len(coarsegrid.coordinates) != cell.dim:
             raise ValueError("cell and coarse grid dimensions differ")
         K = [len(c) - 1 for c in coarsegrid.coordinates]
         self.forest = Forest(cell.dim, K, coarsegrid.periodic, min_level=min_level)
 
     def __len__(self):
+        if self.forest is None and self.cell.dim == 1:
+            return (len(self.coarsegrid.coordinates[0]) - 1) << self.min_level
         if self.forest is None:
             return len(self.coarsegrid) << (self.cell.dim * self.min_level)
         return len(self.forest)
@@ -128,7 +135,8 @@ def adapt(gm, flags):
     (AdaptNone) or coarsen (AdaptCoarsen, whole families) each leaf, then balance 2:1
     across faces."""
     if gm.forest is None:
-        raise NotImplementedError("adapting a forest on an unstructured coarse grid is not implemented")
+        raise NotImplementedError("adapting a 1-D forest or a forest on an unstructured coarse grid is not "
+                                  "implemented (gridmanager.jl:158)")
     gm.forest.adapt(flags)
 
 
@@ -141,6 +149,8 @@ def generate(arg, gm=None):
         gm, warp = arg, None
     else:
         warp = arg
+    if gm.forest is None and gm.cell.dim == 1:
+        return Grid(gm.cell, gm.coarsegrid, warp=warp, level=gm.min_level)
     if gm.forest is None:
         return UnstructuredGrid(gm.cell, gm.coarsegrid, gm.min_level, warp=warp)
     if all(L[1] == 0 for L in gm.forest.leaves):

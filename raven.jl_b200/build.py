@@ -22,7 +22,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-I", CSRC,
               "-I", INCLUDE]
-DIMS_NQS = [(d, q) for d in (2, 3) for q in range(2, 9)]
+DIMS_NQS = [(d, q) for d in (1, 2, 3) for q in range(2, 9)]
 
 
 def nvcc():

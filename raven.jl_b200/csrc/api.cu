@@ -143,6 +143,7 @@ rb200_status cuda_fail(rb200_handle* h, cudaError_t e, const char* where) {
 // 0-based volume node of face f at in-face index j (cellfaceindices, lobattocells.jl:2012-2053)
 int face_node(int dim, int nq, int f, int j) {
     const int dir = f / 2, c = (f % 2) ? nq - 1 : 0;
+    if (dim == 1) return c;
     if (dim == 2) return dir == 0 ? c + nq * j : j + nq * c;
     const int j1 = j % nq, j2 = j / nq;
     if (dir == 0) return c + nq * (j1 + nq * j2);
@@ -501,8 +502,7 @@ rb200_status rb200_create(const rb200_desc* d, rb200_handle** out) {
         *out = h;
         return s;
     };
-    if (d->dim != 2 && d->dim != 3)
-        return bail(fail(h, RB200_ERR_UNSUPPORTED, "dim must be 2 or 3 (1-D grids are not implemented)"));
+    if (d->dim < 1 || d->dim > 3) return bail(fail(h, RB200_ERR_UNSUPPORTED, "dim must be 1, 2 or 3"));
     if (d->nq < 2 || d->nq > kMaxNq) return bail(fail(h, RB200_ERR_UNSUPPORTED, "nq must be in 2..8"));
     if (d->num_elements < 0 || d->num_elements > (int64_t)INT32_MAX)
         return bail(fail(h, RB200_ERR_BAD_ARG, "num_elements out of range"));
@@ -510,7 +510,7 @@ rb200_status rb200_create(const rb200_desc* d, rb200_handle** out) {
         return bail(fail(h, RB200_ERR_BAD_ARG, "null host array in descriptor"));
     h->dim = d->dim;
     h->nq = d->nq;
-    h->np = d->dim == 2 ? d->nq * d->nq : d->nq * d->nq * d->nq;
+    h->np = d->dim == 1 ? d->nq : d->dim == 2 ? d->nq * d->nq : d->nq * d->nq * d->nq;
     h->nfp = h->np / d->nq;
     h->nf = 2 * d->dim;
     h->E = d->num_elements;
@@ -589,7 +589,8 @@ rb200_status rb200_create(const rb200_desc* d, rb200_handle** out) {
                     if (s[k] != want) affine = false;
                 }
                 double wsJ;
-                if (dim == 2) wsJ = sJ * h->w[j];
+                if (dim == 1) wsJ = sJ;  // one node a face: weight 1 (lobattocells.jl:2656)
+                else if (dim == 2) wsJ = sJ * h->w[j];
                 else wsJ = (sJ * h->w[j % nq]) * h->w[j / nq];
                 if (s[dim + 1] != wsJ) affine = false;
             }

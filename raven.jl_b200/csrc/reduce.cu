@@ -26,7 +26,7 @@ __global__ void __launch_bounds__(kRedThreads) weighted_sums_kernel(const double
                                                                     int ns, int64_t E, int geom,
                                                                     double* __restrict__ partial) {
     __shared__ double red[kRedThreads];
-    const int np = dim == 2 ? nq * nq : nq * nq * nq;
+    const int np = dim == 1 ? nq : dim == 2 ? nq * nq : nq * nq * nq;
     const int nvg = dim * dim + 2;
     for (int s = 0; s < ns; ++s) {
         double a2 = 0.0, a1 = 0.0;
@@ -35,7 +35,8 @@ __global__ void __launch_bounds__(kRedThreads) weighted_sums_kernel(const double
                 double mj;
                 if (geom == GEOM_AFFINE) {
                     const int i = n % nq, j = (n / nq) % nq, k = n / (nq * nq);
-                    mj = wgt[i] * wgt[j];
+                    mj = wgt[i];
+                    if (dim >= 2) mj = mj * wgt[j];
                     if (dim == 3) mj = mj * wgt[k];
                     mj = mj * elem_geo[4 * e + 3];
                 } else {
@@ -72,7 +73,7 @@ __global__ void __launch_bounds__(kRedThreads) weighted_pnorm_kernel(const doubl
                                                                      int ns, int64_t E, int geom, double p, int kind,
                                                                      double* __restrict__ partial) {
     __shared__ double red[kRedThreads];
-    const int np = dim == 2 ? nq * nq : nq * nq * nq;
+    const int np = dim == 1 ? nq : dim == 2 ? nq * nq : nq * nq * nq;
     const int nvg = dim * dim + 2;
     for (int s = 0; s < ns; ++s) {
         double acc = 0.0;
@@ -86,7 +87,8 @@ __global__ void __launch_bounds__(kRedThreads) weighted_pnorm_kernel(const doubl
                 double mj;
                 if (geom == GEOM_AFFINE) {
                     const int i = n % nq, j = (n / nq) % nq, k = n / (nq * nq);
-                    mj = wgt[i] * wgt[j];
+                    mj = wgt[i];
+                    if (dim >= 2) mj = mj * wgt[j];
                     if (dim == 3) mj = mj * wgt[k];
                     mj = mj * elem_geo[4 * e + 3];
                 } else {
@@ -129,8 +131,8 @@ __global__ void finish_sums_kernel(const double* __restrict__ partial, int nbloc
 
 __global__ void face_vmapP_kernel(const int32_t* __restrict__ nbr, int dim, int nq, int64_t E,
                                   int64_t* __restrict__ out) {
-    const int np = dim == 2 ? nq * nq : nq * nq * nq;
-    const int nfp = dim == 2 ? nq : nq * nq;
+    const int np = dim == 1 ? nq : dim == 2 ? nq * nq : nq * nq * nq;
+    const int nfp = dim == 1 ? 1 : dim == 2 ? nq : nq * nq;
     const int nf = 2 * dim;
     const int64_t total = E * nf * nfp;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
@@ -142,6 +144,7 @@ __global__ void face_vmapP_kernel(const int32_t* __restrict__ nbr, int dim, int 
         // node of face f (side) or of the opposite face (1-side) at in-face index j
         auto facenode = [&](int sd) {
             const int c = sd ? nq - 1 : 0;
+            if (dim == 1) return c;
             if (dim == 2) return dir == 0 ? c + nq * j : j + nq * c;
             const int j1 = j % nq, j2 = j / nq;
             if (dir == 0) return c + nq * (j1 + nq * j2);
@@ -255,7 +258,7 @@ cudaError_t launch_weighted_pnorm(const double* q, const double* elem_geo, const
 }
 
 cudaError_t launch_face_vmapP(const int32_t* nbr, int dim, int nq, int64_t E, int64_t* out, cudaStream_t s) {
-    const int nfp = dim == 2 ? nq : nq * nq;
+    const int nfp = dim == 1 ? 1 : dim == 2 ? nq : nq * nq;
     const int64_t total = E * 2 * dim * nfp;
     if (total == 0) return cudaSuccess;
     int64_t blocks = (total + 255) / 256;

@@ -68,7 +68,8 @@ __device__ __forceinline__ double node_mj(const RelaxGeo& G, int64_t e, int n) {
     if (G.geom == GEOM_AFFINE) {
         const int nq = G.nq;
         const int i = n % nq, j = (n / nq) % nq, k = n / (nq * nq);
-        double mj = G.w[i] * G.w[j];
+        double mj = G.w[i];
+        if (G.dim >= 2) mj = mj * G.w[j];
         if (G.dim == 3) mj = mj * G.w[k];
         return mj * G.elem_geo[4 * e + 3];
     }
@@ -200,6 +201,8 @@ int grid_for(int64_t n) {
 
 cudaError_t launch_entropy_sums(const RelaxGeo& G, const double* base, const double* dir, double c, const double* k,
                                 double* partial, int nblocks, double* out, cudaStream_t s) {
+    if (G.dim == 1) return G.euler ? sums_t<1, true>(G, base, dir, c, k, partial, nblocks, out, s)
+                                   : sums_t<1, false>(G, base, dir, c, k, partial, nblocks, out, s);
     if (G.dim == 2) return G.euler ? sums_t<2, true>(G, base, dir, c, k, partial, nblocks, out, s)
                                    : sums_t<2, false>(G, base, dir, c, k, partial, nblocks, out, s);
     if (G.dim == 3) return G.euler ? sums_t<3, true>(G, base, dir, c, k, partial, nblocks, out, s)
@@ -209,6 +212,8 @@ cudaError_t launch_entropy_sums(const RelaxGeo& G, const double* base, const dou
 
 cudaError_t launch_rlsrk_stage(const RelaxGeo& G, double* q, double* dq, const double* k, double rka, double rkb_dt,
                                double* partial, int nblocks, double* out, cudaStream_t s) {
+    if (G.dim == 1) return G.euler ? stage_t<1, true>(G, q, dq, k, rka, rkb_dt, partial, nblocks, out, s)
+                                   : stage_t<1, false>(G, q, dq, k, rka, rkb_dt, partial, nblocks, out, s);
     if (G.dim == 2) return G.euler ? stage_t<2, true>(G, q, dq, k, rka, rkb_dt, partial, nblocks, out, s)
                                    : stage_t<2, false>(G, q, dq, k, rka, rkb_dt, partial, nblocks, out, s);
     if (G.dim == 3) return G.euler ? stage_t<3, true>(G, q, dq, k, rka, rkb_dt, partial, nblocks, out, s)

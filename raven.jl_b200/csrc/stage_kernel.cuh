@@ -218,7 +218,8 @@ __device__ __forceinline__ void stage_element_adv_brick(const StageArgs& A, cons
         T nf;
         if (ne == -2) {  // mortar face: the flux comes from the mortar kernel
             int j;
-            if (DIM == 2) j = (dir == 0) ? id[1] : id[0];
+            if (DIM == 1) j = 0;
+            else if (DIM == 2) j = (dir == 0) ? id[1] : id[0];
             else j = (dir == 0) ? id[1] + NQ * id[2] : (dir == 1 ? id[0] + NQ * id[2] : id[0] + NQ * id[1]);
             nf = (T)__ldg(P.ncflux + ((size_t)e * NF + f) * NFP + j);
         } else {
@@ -535,7 +536,8 @@ __device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs
             const int ne = __ldg(P.nbr + (size_t)NF * e + f);
             // in-face index of this node (column-major over the face dims)
             int j;
-            if (DIM == 2) j = (dir == 0) ? id[1] : id[0];
+            if (DIM == 1) j = 0;
+            else if (DIM == 2) j = (dir == 0) ? id[1] : id[0];
             else j = (dir == 0) ? id[1] + NQ * id[2] : (dir == 1 ? id[0] + NQ * id[2] : id[0] + NQ * id[1]);
             T qp[NS];
             if (ne >= 0) {
@@ -564,7 +566,8 @@ __device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) nv[d] = T(0);
                 nv[dir] = side == 0 ? T(-1) : T(1);
-                if (DIM == 2) wsJ = sJ * A.w[dir == 0 ? id[1] : id[0]];
+                if (DIM == 1) wsJ = sJ;  // one node a face: weight 1 (lobattocells.jl:2656)
+                else if (DIM == 2) wsJ = sJ * A.w[dir == 0 ? id[1] : id[0]];
                 else {
                     const int i1 = dir == 0 ? id[1] : id[0];
                     const int i2 = dir == 2 ? id[1] : id[2];

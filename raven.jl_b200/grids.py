@@ -183,6 +183,8 @@ def brick_tree_order(K):
 def face_node(dim, nq, f, j):
     """0-based volume node of face f at in-face index j (lobattocells.jl:2012-2053)."""
     d, c = f // 2, (nq - 1 if f % 2 else 0)
+    if dim == 1:
+        return c
     if dim == 2:
         return c + nq * j if d == 0 else j + nq * c
     j1, j2 = j % nq, j // nq
@@ -204,9 +206,12 @@ class Grid:
       boundarycodes   (2*dim, E) int64
     """
 
-    def __init__(self, cell, coarse, warp=None):
+    def __init__(self, cell, coarse, warp=None, level=0):
         self.cell = cell
         dim, nq = cell.dim, cell.nq
+        if dim == 1:
+            self._init_line(cell, coarse, warp, level)
+            return
         self.dim, self.nq = dim, nq
         self.np = nq**dim
         self.nfp = nq ** (dim - 1)
@@ -240,6 +245,49 @@ class Grid:
         self.isunwarpedbrick = warp is None
         self.volume_metrics = (self._brick_metrics() if warp is None else self._curved_metrics())
         self._face_maps(K, periodic)
+        self._surface_metrics()
+
+    def _init_line(self, cell, coarse, warp, level):
+        """A 1-D brick refined uniformly to `level` (gridmanager.jl:918-1000, 1-D
+        connectivity; points by linebrickpoints!, lobattocells.jl:695-755): trees in
+        order, 2^level quadrants each; boundary code 1 on the x- end and 2 on the x+ end
+        of a non-periodic line."""
+        if warp is not None:
+            raise NotImplementedError("warped 1-D grids are not generated")
+        nq = cell.nq
+        self.dim, self.nq, self.np, self.nfp, self.nfaces = 1, nq, nq, 1, 2
+        c = np.asarray(coarse.coordinates[0], dtype=np.float64)
+        per = bool(coarse.periodic[0])
+        T = len(c) - 1
+        nq_t = 1 << int(level)
+        self.E = E = T * nq_t
+        self.tree = np.array([np.arange(E) // nq_t, np.zeros(E, int), np.zeros(E, int)])
+        r = cell.r
+        h = 1.0 / (1 << (int(level) + 1))
+        pts = np.zeros((nq, 1, E), order="F")
+        for e in range(E):
+            t, qq = divmod(e, nq_t)
+            cr = qq / nq_t  # ix / 2^30 with ix = qq 2^(30 - level): exact
+            dx = c[t + 1] - c[t]
+            for i in range(nq):
+                pts[i, 0, e] = _fma_exact(dx, _fma_exact(h, r[i] + 1, cr), c[t])
+        self.points = pts
+        self.isunwarpedbrick = True
+        self.volume_metrics = self._brick_metrics()
+        fn = np.array([[0], [nq - 1]])
+        e = np.arange(E)
+        vmapM = (fn[:, :, None] + nq * e[None, None, :] + 1).reshape(2, E)
+        vmapP = vmapM.copy()
+        bc = np.zeros((2, E), dtype=np.int64)
+        left, right = (e - 1) % E, (e + 1) % E
+        vmapP[0, :] = nq * left + (nq - 1) + 1
+        vmapP[1, :] = nq * right + 1
+        if not per:
+            vmapP[0, 0], vmapP[1, E - 1] = vmapM[0, 0], vmapM[1, E - 1]
+            bc[0, 0], bc[1, E - 1] = 1, 2
+        self.vmapM = np.asfortranarray(vmapM.astype(np.int64))
+        self.vmapP = np.asfortranarray(vmapP.astype(np.int64))
+        self.boundarycodes = np.asfortranarray(bc)
         self._surface_metrics()
 
     # ------------------------------------------------------------------ metrics
@@ -357,7 +405,9 @@ class Grid:
             sJ = np.sqrt((n * n).sum(0))
             n = n / sJ
             j = np.arange(nfp)
-            if dim == 2:
+            if dim == 1:
+                wsJ = sJ  # one node a face: weight 1 (lobattocells.jl:2656)
+            elif dim == 2:
                 wsJ = sJ * w[j][:, None]
             else:
                 wsJ = (sJ * w[j % nq][:, None]) * w[j // nq][:, None]

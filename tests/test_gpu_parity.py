@@ -8,7 +8,9 @@ Tolerances (stated here and in the assertion messages):
   * reductions: 1e-13 relative.
 """
 
+import json
 import math
+import os
 
 import numpy as np
 import pytest
@@ -167,26 +169,18 @@ def test_host_buffer_path_equals_device_path(rb, cuda_ok):
 
 # ------------------------------------------------------------ reference goldens on the GPU
 
-GOLDEN_CASES = [
-    ("advection", "wave_2d", "weak", 3.0423062189303111e-04),
-    ("advection", "wave_2d", "fd_central", 3.0423062189285823e-04),
-    ("advection", "wave_3d", "weak", 5.2720204799800677e-04),
-    ("advection", "wave_3d", "fd_central", 5.2720204799799615e-04),
-    ("euler", "isentropicvortex", "weak", 2.1296858506446990e00),
-    ("euler", "isentropicvortex", "fd_ec", 2.0789522602391144e00),
-    ("euler", "wave_2d", "weak", 6.1436068743006696e-04),
-    ("euler", "wave_2d", "fd_ec", 1.2210577822045819e-03),
-    ("euler", "wave_3d", "weak", 3.9411906944785454e-04),
-    ("euler", "wave_3d", "fd_ec", 6.7581626007666136e-04),
-]
+GOLD = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_goldens.json")))
 
 
-@pytest.mark.parametrize("law_name,test,form,expected", GOLDEN_CASES,
-                         ids=[f"{a}-{b}-{c}" for a, b, c, _ in GOLDEN_CASES])
-def test_reference_goldens_through_product_api(rb, cuda_ok, law_name, test, form, expected):
-    """The reference's level-1 golden L2 errors (test/balancelaws/*/*.jl), run end to end
-    through the product API: grid generation, DGSEM on the GPU, solve, weightednorm."""
-    N, K = 4, 5
+@pytest.mark.parametrize("entry", GOLD["errors"],
+                         ids=[f"{e['law']}-{e['test']}-{e['form']}-L{e['level']}" for e in GOLD["errors"]])
+def test_reference_goldens_through_product_api(rb, cuda_ok, entry):
+    """Every golden L2 error of the reference's balance-law tests (test/balancelaws/*/*.jl,
+    all refinement levels, 1-D to 3-D), run end to end through the product API: grid
+    generation, DGSEM on the GPU, solve, weightednorm; to the tolerance the reference
+    test applies."""
+    law_name, test, form, lev = entry["law"], entry["test"], entry["form"], entry["level"]
+    N, K = 4, 5 * 2 ** (lev - 1)
     vf = {"weak": None, "fd_central": rb.CentralFlux(), "fd_ec": rb.EntropyConservativeFlux()}[form]
     vform = rb.WeakForm() if vf is None else rb.FluxDifferencingForm(vf)
     if test == "isentropicvortex":
@@ -201,19 +195,20 @@ def test_reference_goldens_through_product_api(rb, cuda_ok, law_name, test, form
     dg = rb.DGSEM(law=law, grid=grid, volume_form=vform, surface_numericalflux=rb.RusanovFlux())
     og_law = O.Law(O.LAW_ADVECTION if law_name == "advection" else O.LAW_EULER, dim)
     og = O.Grid(dim, N + 1, [K] * dim, lo, hi, [True] * dim)  # only to evaluate initial/exact data
+    cfl = 0.5 if dim == 1 else 0.25
     if test == "isentropicvortex":
         dt, T, kind = 0.25 * (10.0 / K) / N, 5.0, 2
     elif law_name == "advection":
-        dt, T, kind = 0.25 * (2.0 / K) / N / math.sqrt(dim), 0.7, 0
+        dt, T, kind = cfl * (2.0 / K) / N / math.sqrt(dim), 0.7, 0
     else:
-        dt = 0.25 * (2.0 / K) / N / math.sqrt(1.4)
+        dt = cfl * (2.0 / K) / N / math.sqrt(1.4)
         T, kind = (dt if dim == 3 else 0.7), 1
     q = rb.GridArray.from_numpy(og.initial_condition(og_law, kind))
     rb.solve(q, T, rb.LSRK54(dg, q, dt))
     qe = rb.GridArray.from_numpy(og.initial_condition(og_law, kind, t=T))
     qe.data.sub_(q.data)
     err = rb.weightednorm(dg, qe)
-    assert err == pytest.approx(expected, rel=math.sqrt(np.finfo(float).eps))
+    assert err == pytest.approx(entry["expected"], rel=entry["rtol"]), entry["source"]
 
 
 @pytest.mark.parametrize("case", [CASES[0], CASES[10]], ids=[_id(CASES[0]), _id(CASES[10])])
