@@ -83,8 +83,10 @@ def test_create_rejects_bad_arguments_before_touching_the_device(rb, small_grid)
     assert L.rb200_create(None, ctypes.byref(h)) == 1
     d, keep = _desc(rb, small_grid, abi_version=99)
     assert _create(rb, d)[0] == 1
-    d, keep = _desc(rb, small_grid, dim=1)
+    d, keep = _desc(rb, small_grid, dim=4)
     assert _create(rb, d)[0] == 6
+    d, keep = _desc(rb, small_grid, dim=1)  # 1-D is supported: a 2-D grid's face maps do not fit it
+    assert _create(rb, d)[0] == 2
     d, keep = _desc(rb, small_grid, nq=9)
     assert _create(rb, d)[0] == 6
     d, keep = _desc(rb, small_grid, law=7)
