@@ -242,6 +242,20 @@ rb200_status rb200_set_kernel_path(rb200_handle* h, int32_t path);
  * and step of the handle. */
 rb200_status rb200_set_directions(rb200_handle* h, int32_t mask);
 
+/* boundarystate(law, problem, n, q-, aux-, tag)  (balancelaw.jl:22; the reference's
+ * examples overload it per problem, e.g. examples/balancelaws/euler/sod.jl:15-21 and
+ * euler_gravity/gravitywave.jl:16-21).  Sets the exterior state of the boundary faces
+ * whose code (boundarycodes(grid)) is `tag` (1..8):
+ *   kind 0: q+ = q- (the reference's default);
+ *   kind 1: q+ = state (Ns host doubles, copied), a prescribed exterior state;
+ *   kind 2: a reflecting wall, q+ = q- with rho u+ = rho u- - 2 (n . rho u-) n (Euler only).
+ * Faces of other tags keep their condition.  A handle with a non-default condition runs
+ * the generic stage kernel. */
+#define RB200_BC_DEFAULT 0
+#define RB200_BC_PRESCRIBED 1
+#define RB200_BC_WALL 2
+rb200_status rb200_set_boundary_condition(rb200_handle* h, int32_t tag, int32_t kind, const double* state);
+
 /* Synchronizes `stream` and returns RB200_ERR_TIMEOUT if a kernel of this handle gave
  * up a bounded wait since the handle was created, RB200_OK otherwise. */
 rb200_status rb200_sync_status(rb200_handle* h, void* stream);

@@ -75,6 +75,7 @@ def lib():
         L.og_grid_set_mortars.argtypes = [P, P, ctypes.c_int64, P, P, P, P]
         L.og_grid_set_curved_mortars.argtypes = [P, ctypes.c_int]
         L.og_grid_set_directions.argtypes = [P, ctypes.c_int]
+        L.og_grid_set_boundary_condition.argtypes = [P, ctypes.c_int, ctypes.c_int, P]
         for name in ("og_grid_sizes", "og_grid_points", "og_grid_vmet", "og_grid_smet", "og_grid_vmapM",
                      "og_grid_vmapP", "og_grid_boundary", "og_grid_tree_coords"):
             getattr(L, name).argtypes = [P, P]
@@ -233,6 +234,12 @@ class Grid:
         lib().og_tendency(self.h, ctypes.byref(law.c), _ptr(dq), _ptr(q), t, int(increment), e0,
                           self.E if e1 is None else e1)
         return dq
+
+    def set_boundary_condition(self, tag, kind, state=None):
+        """boundarystate of the faces with code `tag`: 0 q+ = q-, 1 q+ = state, 2 a wall."""
+        st = None if state is None else np.ascontiguousarray(state, dtype=np.float64)
+        self._bc_keep = getattr(self, "_bc_keep", []) + [st]
+        lib().og_grid_set_boundary_condition(self.h, int(tag), int(kind), None if st is None else _ptr(st))
 
     def set_directions(self, directions):
         """DGSEM(; directions): 1-based directions whose terms are computed."""

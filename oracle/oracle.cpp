@@ -135,6 +135,10 @@ struct og_grid {
     std::vector<uint8_t> ncface;   // (nfaces, E): 1 on faces coupled through a mortar
     int curved_mortars = 0;        // 1: warped grid, mortar fluxes with the small faces' geometry
     int dir_mask = 0;              // DGSEM(; directions) as a bit mask (dgsem.jl:46-81); 0 = all
+    // boundarystate per boundary tag 1..8 (balancelaw.jl:22 and its overloads in the
+    // reference's examples): 0 q+ = q-, 1 a prescribed state, 2 a reflecting wall
+    int bc_kind[9] = {0};
+    double bc_state[9][5] = {{0}};
 };
 
 // Correctly rounded value of lo + (hi-lo)*i/K (Julia `range(lo, stop=hi, length=K+1)`).
@@ -1037,6 +1041,16 @@ static void element_tendency(const og_grid* g, const Phys& Ph, double* dq, const
                 for (int s = 0; s < ns; ++s) qp[s] = q[(size_t)np * ns * ep + (size_t)np * s + npn];
             } else {
                 for (int s = 0; s < ns; ++s) qp[s] = qm[s];  // balancelaw.jl:77 default boundarystate
+                const int64_t tag = g->bc[(size_t)nf * e + face];
+                const int kind = (tag >= 1 && tag <= 8) ? g->bc_kind[tag] : 0;
+                if (kind == 1) {
+                    for (int s = 0; s < ns; ++s) qp[s] = g->bc_state[tag][s];
+                } else if (kind == 2 && ns == dim + 2) {
+                    // rho u+ = rho u- - 2 (n' rho u-) n (examples/balancelaws/euler_gravity/gravitywave.jl:16-21)
+                    double mn = 0.0;
+                    for (int d = 0; d < dim; ++d) mn = d == 0 ? n[0] * qm[1] : mn + n[d] * qm[1 + d];
+                    for (int d = 0; d < dim; ++d) qp[1 + d] = qm[1 + d] - (2 * mn) * n[d];
+                }
             }
             double nfl[MAXS];
             surfaceflux(Ph, n, qm, qp, nfl);
@@ -1221,6 +1235,12 @@ extern "C" void og_grid_set_mortars(og_grid* g, const int64_t* mortars, int64_t 
 }
 
 extern "C" void og_grid_set_curved_mortars(og_grid* g, int curved) { g->curved_mortars = curved != 0; }
+
+extern "C" void og_grid_set_boundary_condition(og_grid* g, int tag, int kind, const double* state) {
+    if (tag < 1 || tag > 8) return;
+    g->bc_kind[tag] = kind;
+    for (int s = 0; s < 5; ++s) g->bc_state[tag][s] = (kind == 1 && state) ? state[s] : 0.0;
+}
 
 extern "C" void og_grid_set_directions(og_grid* g, int mask) {
     const int all = (1 << g->dim) - 1;

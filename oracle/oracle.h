@@ -76,6 +76,9 @@ void og_grid_set_curved_mortars(og_grid* g, int curved);
 /* DGSEM(; directions): volume and surface terms of the directions in `mask` only (bit d =
  * direction d + 1; all when mask covers every direction). */
 void og_grid_set_directions(og_grid* g, int mask);
+/* boundarystate of the faces with boundary code `tag` (1..8): kind 0 q+ = q-, 1 q+ =
+ * state (Ns doubles), 2 a reflecting wall (Euler). */
+void og_grid_set_boundary_condition(og_grid* g, int tag, int kind, const double* state);
 
 /* Standalone LGL operators for nq points (computed in __float128, rounded). */
 void og_lgl(int nq, double* r, double* w, double* D);

@@ -306,11 +306,16 @@ class DGSEM:
     directions: the 1-based directions whose volume and surface terms are computed, as
     Raven's `directions = 1:ndims(law)` (default: all), e.g. (1, 2) or (3,) for a split
     into horizontal and vertical operators.
+    boundary_conditions: {tag: condition} for the faces with that boundary code, the
+    exterior state Raven's `boundarystate(law, problem, n, q-, aux-, tag)` returns
+    (balancelaw.jl:22 and its overloads in the reference's examples): a sequence of Ns
+    values (a prescribed state), "wall" (reflecting wall, Euler), or None (q+ = q-, the
+    default).
     precision: "fp64" (plain FP64) or "fp32_bulk" (FP32 volume/surface arithmetic, FP64
     geometry, state accumulation and reductions)."""
 
-    def __init__(self, *, law, grid, surface_numericalflux, volume_form=None, directions=None, precision="fp64",
-                 device=None):
+    def __init__(self, *, law, grid, surface_numericalflux, volume_form=None, directions=None,
+                 boundary_conditions=None, precision="fp64", device=None):
         torch = _torch()
         if not torch.cuda.is_available():
             raise RuntimeError("raven_b200.DGSEM needs a CUDA device (no CPU fallback)")
@@ -382,10 +387,40 @@ class DGSEM:
                 L.rb200_destroy(h)
                 self._h = None
                 raise RB200Error(st, msg)
+        for tag, cond in (boundary_conditions or {}).items():
+            try:
+                self.set_boundary_condition(tag, cond)
+            except Exception:
+                L.rb200_destroy(h)
+                self._h = None
+                raise
         info = (ctypes.c_int64 * 9)()
         L.rb200_get_info(h, info, 9)
         self.info = list(info)
         self.geometry = "affine" if info[4] == 0 else "curved"
+        self.pipelined_ctas = int(info[8])
+
+    def set_boundary_condition(self, tag, condition):
+        """The exterior state of the faces with boundary code `tag` (1..8): a sequence of
+        Ns values, "wall", or None (see the class docstring)."""
+        if condition is None:
+            kind, st = 0, None
+        elif isinstance(condition, str):
+            if condition != "wall":
+                raise ValueError("a boundary condition is a state, 'wall' or None")
+            kind, st = 2, None
+        else:
+            st = np.ascontiguousarray(condition, dtype=np.float64).ravel()
+            if st.size != self.law.ns:
+                raise ValueError(f"a prescribed boundary state has {self.law.ns} values")
+            kind = 1
+        _lib.check(_lib.lib().rb200_set_boundary_condition(self._h, int(tag), kind,
+                                                           None if st is None else st.ctypes.data_as(ctypes.c_void_p)),
+                   self._h)
+        self.info = None  # the kernel choice may have changed; re-read below
+        info = (ctypes.c_int64 * 9)()
+        _lib.lib().rb200_get_info(self._h, info, 9)
+        self.info = list(info)
         self.pipelined_ctas = int(info[8])
 
     def set_kernel_path(self, path):

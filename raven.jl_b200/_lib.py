@@ -55,6 +55,7 @@ EXPORTED = [
     "rb200_probe_bounded_wait",
     "rb200_probe_fp64_rate",
     "rb200_set_directions",
+    "rb200_set_boundary_condition",
     "rb200_weighted_sums_noalloc",
     "rb200_server_create",
     "rb200_server_submit",
@@ -185,6 +186,7 @@ def lib():
     L.rb200_probe_bounded_wait.argtypes = [I64, P]
     L.rb200_probe_fp64_rate.argtypes = [I64, P, P]
     L.rb200_set_directions.argtypes = [P, I32]
+    L.rb200_set_boundary_condition.argtypes = [P, I32, I32, P]
     L.rb200_weighted_sums_noalloc.argtypes = [P, P, I32, I32, I64, P, P]
     L.rb200_last_error.argtypes = [P]
     L.rb200_last_error.restype = ctypes.c_char_p

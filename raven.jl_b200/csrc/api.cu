@@ -55,6 +55,11 @@ struct rb200_handle {
     int red_blocks = 0;
     int kernel_path = 0;          // 0 automatic, 1 generic stage kernel only
     int dir_mask = 0;             // DGSEM(; directions) as a bit mask; 0 = all directions
+    // boundarystate per boundary tag (rb200_set_boundary_condition); the face codes kept
+    std::vector<int8_t> bcode;    // (nf, E) boundary codes of the grid
+    int32_t bc_kind[kMaxBcTags + 1] = {0};
+    double bc_state[kMaxBcTags + 1][5] = {{0}};
+    bool has_bc = false;
     // CUDA graph of two LSRK steps (10 stage launches) for one (q, dq, dt), replayed by
     // rb200_lsrk54_step; captured on a stream of the handle, launched on the caller's
     cudaStream_t cap_stream = nullptr;
@@ -208,7 +213,7 @@ cudaError_t launch_any(rb200_handle* h, const StageArgs& a, cudaStream_t st) {
     }
     const bool stage_mode = a.mode >= MODE_STAGE;
     // the pipelined kernels compute every direction; a direction subset runs the generic one
-    const bool all_dirs = h->dir_mask == 0;
+    const bool all_dirs = h->dir_mask == 0 && !h->has_bc;
     if (all_dirs && h->pipe_curved_grid > 0 && h->kernel_path == 0 && stage_mode && aligned16(a.q_in) && aligned16(a.q_out) &&
         aligned16(a.dq)) {
         PipeCurvedArgs c;
@@ -271,6 +276,8 @@ StageArgs base_args(const rb200_handle* h) {
     a.ncflux = h->d_ncflux;
     a.vmapP = h->d_vmapP;
     a.dir_mask = h->dir_mask;
+    std::memcpy(a.bc_kind, h->bc_kind, sizeof(a.bc_kind));
+    std::memcpy(a.bc_state, h->bc_state, sizeof(a.bc_state));
     a.E = h->E_active;
     a.surface_rusanov = h->sflux == RB200_FLUX_RUSANOV ? 1 : 0;
     a.surface_flux = h->sflux;
@@ -602,6 +609,7 @@ rb200_status rb200_create(const rb200_desc* d, rb200_handle** out) {
 
     // ------------------------------------------------------------- connectivity
     std::vector<int32_t> nbr((size_t)nf * E, -1);
+    h->bcode.assign((size_t)nf * E, 0);
     bool general = false;  // some face meets its neighbour rotated or on another face
     for (int64_t e = 0; e < E; ++e)
         for (int f = 0; f < nf; ++f) {
@@ -611,6 +619,7 @@ rb200_status rb200_create(const rb200_desc* d, rb200_handle** out) {
                 if (d->vmapM[base + j] != (int64_t)np * e + face_node(dim, nq, f, j) + 1)
                     return bail(fail(h, RB200_ERR_SHAPE, "vmapM is not Raven's face-node numbering"));
             if (bcode != 0) {
+                h->bcode[(size_t)nf * e + f] = (int8_t)(bcode >= 1 && bcode <= kMaxBcTags ? bcode : 0);
                 nbr[(size_t)nf * e + f] = -1;
                 continue;
             }
@@ -1194,6 +1203,34 @@ rb200_status rb200_set_kernel_path(rb200_handle* h, int32_t path) {
     return RB200_OK;
 }
 
+rb200_status rb200_set_boundary_condition(rb200_handle* h, int32_t tag, int32_t kind, const double* state) {
+    if (!h) return RB200_ERR_BAD_ARG;
+    if (tag < 1 || tag > kMaxBcTags) return fail(h, RB200_ERR_BAD_ARG, "boundary tag must be in 1..8");
+    if (kind != BC_DEFAULT && kind != BC_PRESCRIBED && kind != BC_WALL)
+        return fail(h, RB200_ERR_BAD_ARG, "unknown boundary condition kind");
+    if (kind == BC_WALL && h->law != RB200_LAW_EULER)
+        return fail(h, RB200_ERR_UNSUPPORTED, "a reflecting wall needs the Euler law");
+    if (kind == BC_PRESCRIBED) {
+        if (!state) return fail(h, RB200_ERR_BAD_ARG, "null boundary state");
+        for (int s = 0; s < h->ns; ++s)
+            if (!std::isfinite(state[s])) return fail(h, RB200_ERR_BAD_ARG, "boundary state is not finite");
+    }
+    DeviceGuard guard(h->device);
+    std::vector<int32_t> nbr((size_t)h->nf * h->E);
+    cudaError_t ce = cudaMemcpy(nbr.data(), h->d_nbr, nbr.size() * sizeof(int32_t), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return cuda_fail(h, ce, "boundary condition set-up");
+    for (size_t k = 0; k < nbr.size(); ++k)
+        if (h->bcode[k] == tag) nbr[k] = kind == BC_DEFAULT ? -1 : -(kBcBase + tag);
+    ce = cudaMemcpy(h->d_nbr, nbr.data(), nbr.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    if (ce != cudaSuccess) return cuda_fail(h, ce, "boundary condition upload");
+    h->bc_kind[tag] = kind;
+    for (int s = 0; s < 5; ++s) h->bc_state[tag][s] = (kind == BC_PRESCRIBED && s < h->ns) ? state[s] : 0.0;
+    h->has_bc = false;
+    for (int t = 1; t <= kMaxBcTags; ++t) h->has_bc = h->has_bc || h->bc_kind[t] != BC_DEFAULT;
+    free_graph(h);  // a captured step holds the old arguments
+    return RB200_OK;
+}
+
 rb200_status rb200_set_directions(rb200_handle* h, int32_t mask) {
     if (!h) return RB200_ERR_BAD_ARG;
     const int32_t all = (1 << h->dim) - 1;
@@ -1225,7 +1262,7 @@ rb200_status rb200_get_info(const rb200_handle* h, int64_t* info, int32_t n) {
     if (h->geom == GEOM_CURVED)
         per_node += (h->dim * h->dim + 1) * 8 + (int64_t)h->nf * h->nfp * (h->dim + 1) * 8 / h->np;
     const int64_t v[9] = {h->dim, h->nq, h->ns, h->E, h->geom, h->prec, h->nmortars > 0 ? 10 : 5, per_node,
-                          h->dir_mask ? 0 : (h->geom == GEOM_CURVED ? h->pipe_curved_grid : h->pipe_grid)};
+                          h->dir_mask || h->has_bc ? 0 : (h->geom == GEOM_CURVED ? h->pipe_curved_grid : h->pipe_grid)};
     for (int i = 0; i < n && i < 9; ++i) info[i] = v[i];
     return RB200_OK;
 }

@@ -71,6 +71,11 @@ struct StageArgs {
     int32_t surface_flux;     // kFlux*: the entropy family (EC, KG, Roe, matrix) runs its own kernels
     int32_t dir_mask;         // DGSEM(; directions): bit d set = direction d's volume and face terms
                               // are computed (dgsem.jl:46-81, 257-348, 733-784); 0 reads as all
+    // boundarystate (balancelaw.jl:22) per boundary tag 1..kMaxBcTags: a face whose
+    // neighbour entry is -(kBcBase + tag) takes bc_kind[tag] (BC_PRESCRIBED: q+ = bc_state[tag],
+    // BC_WALL: q+ = q- with the normal momentum reversed); other boundary faces keep q+ = q-
+    int32_t bc_kind[9];
+    double bc_state[9][5];
     double rka;
     double rkb_dt;
     double gamma;
@@ -78,6 +83,10 @@ struct StageArgs {
     double D[kMaxNq * kMaxNq];  // D[i + nq*j] = l_j'(r_i)
     double w[kMaxNq];
 };
+
+constexpr int kMaxBcTags = 8;
+constexpr int kBcBase = 16;
+enum { BC_DEFAULT = 0, BC_PRESCRIBED = 1, BC_WALL = 2 };
 
 // Mortars of an adapted grid (mortar.cu).
 struct MortarArgs {

@@ -227,6 +227,8 @@ __device__ __forceinline__ void stage_element_adv_brick(const StageArgs& A, cons
             if (ne >= 0) {
                 const int nn = n + (side == 0 ? (NQ - 1) * stride : -(NQ - 1) * stride);
                 qp = (T)__ldg(P.q_in + (size_t)ne * NP + nn);
+            } else if (ne <= -kBcBase && A.bc_kind[-ne - kBcBase] == BC_PRESCRIBED) {
+                qp = (T)A.bc_state[-ne - kBcBase][0];
             }
             const T an = (T)A.adv[dir] * (side == 0 ? T(-1) : T(1));
             const T fc = (an * q0 + an * qp) * T(0.5);
@@ -578,6 +580,22 @@ __device__ __forceinline__ void stage_element(const StageArgs& A, const ElemPtrs
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) nv[d] = (T)__ldg(sg + d);
                 wsJ = __ldg(sg + DIM);
+            }
+            if (ne <= -kBcBase) {  // a boundary tag with its own boundarystate
+                const int tag = -ne - kBcBase;
+                if (A.bc_kind[tag] == BC_PRESCRIBED) {
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) qp[s] = (T)A.bc_state[tag][s];
+                } else if constexpr (!C::ADV) {
+                    if (A.bc_kind[tag] == BC_WALL) {
+                        // reflecting wall: rho u+ = rho u- - 2 (n . rho u-) n
+                        T mn = nv[0] * q[1];
+#pragma unroll
+                        for (int d = 1; d < DIM; ++d) mn += nv[d] * q[1 + d];
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) qp[1 + d] = q[1 + d] - (T(2) * mn) * nv[d];
+                    }
+                }
             }
             T nf[NS];
             if (ne == -2) {  // mortar face of an adapted grid: the flux comes from the mortar kernel

@@ -161,3 +161,20 @@ def test_rlsrk144_entropy_conservation_1d(law_kind):
             assert abs(gamma[0] - 1) < 1e-2
     assert drift[True] <= 200 * EPS
     assert drift[True] < 1e-6 * drift[False]
+
+
+def test_oracle_walls_conserve_mass_and_energy():
+    """A closed box with reflecting walls (the boundarystate of the reference's gravity-wave
+    example): mass and energy are conserved by the tendency to round-off."""
+    g = O.Grid(3, 4, [2, 2, 2], [0.0] * 3, [1.0] * 3, [False] * 3)
+    law = O.Law(O.LAW_EULER, 3, form=O.FORM_FLUXDIFF, volume_flux=O.FLUX_KG)
+    g.set_boundary_condition(1, 2)
+    q = g.initial_condition(law, 1)
+    q = np.asfortranarray(q * (1 + 0.02 * np.random.default_rng(9).standard_normal(q.shape)))
+    dq = g.tendency(law, q)
+    MJ = g.volume_metrics()[:, 10, :]
+    for s in (0, 4):
+        assert abs((MJ * dq[:, s, :]).sum()) <= 1e-13 * np.abs(MJ * dq[:, s, :]).sum()
+    g.set_boundary_condition(1, 0)
+    dq0 = g.tendency(law, q)
+    assert abs((MJ * dq0[:, 0, :]).sum()) > 1e-10 * np.abs(MJ * dq0[:, 0, :]).sum()
