@@ -48,7 +48,9 @@ def _compare(rb, og, dg, olaw, law, q, steps=5, dt=1e-3):
 
 def test_sod_shock_tube_prescribed_states(rb, cuda_ok):
     """The reference's Sod example: a 1-D line with the left state on tag 1 and the right
-    state on tag 2 (rho = 1, p = 1 | rho = 1/8, p = 1/10, at rest), Rusanov flux."""
+    state on tag 2 (rho = 1, p = 1 | rho = 1/8, p = 1/10, at rest), Rusanov flux.  The
+    jump is smoothed over a tanh of width 0.03: unlimited DG (here and in the oracle, as
+    in the reference) rings on the sharp jump and loses positivity within 40 steps."""
     nq, K = 5, 32
     og = O.Grid(1, nq, [K], [0.0], [1.0], [False])
     g = wrap_oracle_grid(og)
@@ -60,10 +62,11 @@ def test_sod_shock_tube_prescribed_states(rb, cuda_ok):
     og.set_boundary_condition(1, 1, left)
     og.set_boundary_condition(2, 1, right)
     olaw = O.Law(O.LAW_EULER, 1)
-    xave = og.points()[:, 0, :].mean(0)
+    x = og.points()[:, 0, :]
+    wl = 0.5 * (1 - np.tanh((x - 0.5) / 0.03))
     q = np.zeros((nq, 3, K), order="F")
-    for e in range(K):
-        q[:, :, e] = left if xave[e] < 0.5 else right
+    for s in range(3):
+        q[:, s, :] = right[s] + (left[s] - right[s]) * wl
     dt = 0.25 * (1.0 / K) / (nq - 1) / np.sqrt(1.4)
     qg = _compare(rb, og, dg, olaw, law, q, steps=40, dt=dt)
     rho = qg.numpy()[:, 0]
