@@ -118,6 +118,26 @@ end
 
 stream() = CUDA.stream().handle  # CUDA.jl's task-local stream keeps Julia's ordering
 
+# boundarystate(law, problem, n, q-, aux-, tag) (balancelaw.jl:22) is a Julia method the
+# device kernels cannot call; the two forms the reference's examples use are set per tag
+# instead: a prescribed exterior state (examples/balancelaws/euler/sod.jl:15-21) or a
+# reflecting wall (euler_gravity/gravitywave.jl:16-21); `nothing` restores q+ = q-.
+function set_boundary_condition!(b::B200DGSEM, tag::Integer, cond)
+    if cond === nothing
+        st = ccall((:rb200_set_boundary_condition, lib), Cint, (Ptr{Cvoid}, Int32, Int32, Ptr{Float64}),
+                   b.handle, tag, 0, C_NULL)
+    elseif cond === :wall
+        st = ccall((:rb200_set_boundary_condition, lib), Cint, (Ptr{Cvoid}, Int32, Int32, Ptr{Float64}),
+                   b.handle, tag, 2, C_NULL)
+    else
+        state = Float64.(collect(cond))
+        st = ccall((:rb200_set_boundary_condition, lib), Cint, (Ptr{Cvoid}, Int32, Int32, Ptr{Float64}),
+                   b.handle, tag, 1, state)
+    end
+    check(st, b.handle)
+    return b
+end
+
 # (dg)(dq, q, t; increment): the signature of DGSEM's call (dgsem.jl:84)
 function (b::B200DGSEM)(dq, q, time; increment = true)
     st = ccall((:rb200_tendency, lib), Cint,
