@@ -291,6 +291,34 @@ class GridArray:
             raise ValueError("GridArray data must be a contiguous float64 CUDA tensor")
         return ctypes.c_void_p(self.data.data_ptr())
 
+    # GridArray operations of gridarrays.jl used around the tendency (device tensors, no copies)
+    def components(self):
+        """components(q) (gridarrays.jl:573-615): one view per field, (E, Np) each, writes
+        go to q."""
+        return tuple(self.data[:, s, :] for s in range(self.ns))
+
+    def fill_(self, x):
+        """fill!(q, x) (gridarrays.jl:369-377): every node set to the state x (Ns values,
+        or one value for every field)."""
+        v = np.broadcast_to(np.asarray(x, dtype=np.float64), (self.ns,))
+        for s in range(self.ns):
+            self.data[:, s, :].fill_(float(v[s]))
+        return self
+
+    def sum(self):
+        """sum(q) (gridarrays.jl:663-673): the per-field sums over all nodes (not weighted
+        by MJ; integrals(dg, q) gives the weighted ones)."""
+        return self.data.sum(dim=(0, 2)).cpu().numpy()
+
+    def norm(self):
+        """norm(q) (gridarrays.jl:367): the 2-norm of all entries."""
+        return float(_torch().linalg.vector_norm(self.data).item())
+
+    @property
+    def shape(self):
+        """Raven's parent size (Np, Ns, E)."""
+        return (self.np, self.ns, self.E)
+
 
 def _stream_ptr():
     torch = _torch()

@@ -131,3 +131,26 @@ def test_gather_scatter_points_round_trip(rb, U):
     U.scatter(back, ca, dtoc)
     err = (back.data - x.data).abs().max().item()
     assert err < 10 * np.finfo(float).eps * x.data.abs().max().item()
+
+
+def test_gridarray_operations(rb, cuda_ok):
+    """components, fill!, sum and norm of GridArray (gridarrays.jl:367-377, 573-615,
+    663-673) on the device, against numpy on the same array."""
+    rng = np.random.default_rng(7)
+    a = np.asfortranarray(rng.standard_normal((27, 5, 11)))
+    q = rb.GridArray.from_numpy(a)
+    assert q.shape == a.shape
+    comps = q.components()
+    assert len(comps) == 5
+    for s in range(5):
+        assert np.array_equal(comps[s].cpu().numpy().T, a[:, s, :])
+    comps[2].mul_(2.0)  # a view: writes go to q
+    b = a.copy()
+    b[:, 2, :] *= 2.0
+    assert np.array_equal(q.numpy(), b)
+    assert np.allclose(q.sum(), b.sum(axis=(0, 2)), rtol=1e-13, atol=1e-13)
+    assert q.norm() == pytest.approx(np.linalg.norm(b.ravel()), rel=1e-13)
+    q.fill_([1.0, 2.0, 3.0, 4.0, 5.0])
+    assert np.array_equal(q.numpy()[0, :, 0], [1.0, 2.0, 3.0, 4.0, 5.0])
+    q.fill_(0.5)
+    assert np.all(q.numpy() == 0.5)
