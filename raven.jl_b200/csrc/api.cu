@@ -1021,7 +1021,8 @@ struct SnapHeader {
     int64_t E;
     uint64_t q_bytes, dq_bytes;
     double time, dt, gamma;
-    uint64_t fingerprint;  // the discretization: sizes, law, scheme, D, w, gamma, velocity
+    uint64_t fingerprint;  // the discretization: sizes, law, scheme, D, w, gamma, velocity,
+                           // directions and boundary conditions when set
     uint64_t payload_sum;  // hash of the q bytes, then the dq bytes
     uint64_t reserved[2];
     uint64_t header_sum;   // hash of every byte before this field
@@ -1035,7 +1036,15 @@ static uint64_t snap_fingerprint(const rb200_handle* h) {
     f = snap_hash(h->D, sizeof(double) * h->nq * h->nq, f);
     f = snap_hash(h->w, sizeof(double) * h->nq, f);
     f = snap_hash(&h->gamma, sizeof(double), f);
-    return snap_hash(h->adv, sizeof(h->adv), f);
+    f = snap_hash(h->adv, sizeof(h->adv), f);
+    // a direction subset or boundary conditions change the operator too (hashed only when
+    // set, so a default handle's fingerprint does not depend on them)
+    if (h->dir_mask) f = snap_hash(&h->dir_mask, sizeof(h->dir_mask), f);
+    if (h->has_bc) {
+        f = snap_hash(h->bc_kind, sizeof(h->bc_kind), f);
+        f = snap_hash(h->bc_state, sizeof(h->bc_state), f);
+    }
+    return f;
 }
 
 static size_t snap_dq_bytes(const rb200_handle* h) {

@@ -120,3 +120,21 @@ def test_conditions_switch_kernels_and_errors(rb, cuda_ok):
     with pytest.raises(rb.RB200Error) as ei:
         dga.set_boundary_condition(1, "wall")
     assert ei.value.status == 6
+
+
+def test_snapshot_knows_directions_and_boundary_conditions(rb, cuda_ok):
+    """A snapshot taken with a direction subset or boundary conditions restores only into
+    a handle with the same ones (the fingerprint covers them)."""
+    og, dg, olaw, law = _build(rb, 3, 4, (2, 2, 2), "eul_kg", {1: "wall"})
+    q = rb.GridArray.from_numpy(initial_state(og, olaw, "eul_kg", seed=63))
+    solver = rb.LSRK54(dg, q, 1e-3)
+    solver.dostep(q, 2)
+    snap = rb.snapshot(dg, q, solver)
+    _, same, _, _ = _build(rb, 3, 4, (2, 2, 2), "eul_kg", {1: "wall"})
+    q2 = q.similar()
+    rb.restore(same, snap, q2, rb.LSRK54(same, q2, 1.0))
+    assert np.array_equal(q2.numpy(), q.numpy())
+    _, plain, _, _ = _build(rb, 3, 4, (2, 2, 2), "eul_kg", {})
+    with pytest.raises(rb.RB200Error) as ei:
+        rb.restore(plain, snap, q2, rb.LSRK54(plain, q2, 1.0))
+    assert ei.value.status == 2
