@@ -61,7 +61,7 @@ enum { RB200_PRECISION_FP64 = 0, RB200_PRECISION_FP32_BULK = 1 };
 
 typedef struct rb200_desc {
     int32_t abi_version;      /* RB200_ABI_VERSION */
-    int32_t dim;              /* 2 or 3 */
+    int32_t dim;              /* 1, 2 or 3 */
     int32_t nq;               /* nodes per direction, 2..8 (N = nq-1) */
     int32_t law;              /* RB200_LAW_* */
     int64_t num_elements;     /* E (local elements; no ghosts on one rank) */
