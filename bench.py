@@ -1130,6 +1130,27 @@ def main(argv=None):
             "note": "rb200_lsrk54_step_host, one synchronous call per step: the whole state is copied in "
                     "from pinned host memory and back every step, so PCIe copies dominate",
         }
+        # the same entry point used as solve! is: one call for all the steps, the state copied
+        # in once and back once (informational; the per-step form above is the e2e figure)
+        qh[...] = q0
+        barrier()
+        t0 = time.perf_counter()
+        dg.lsrk54_steps_host(qh, 0.0, dt, args.steps)
+        solve_s = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([solve_s], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            solve_s = float(t.item())
+        e2e["one_call_solve"] = {
+            "value": world * nodes * ns * 5 * args.steps / solve_s,
+            "unit": UNIT,
+            "steps": args.steps,
+            "h2d_bytes_per_call": nodes * ns * 8,
+            "d2h_bytes_per_call": nodes * ns * 8,
+            "ms_per_call": solve_s * 1e3,
+            "note": "rb200_lsrk54_step_host(q, nsteps = steps): one synchronous call, the state copied in "
+                    "and back once, as a solve! over host arrays would use it",
+        }
 
     peak, peak_kind = measured_peaks()
     bytes_launch = stage_bytes_per_launch(w, nodes, ns)
