@@ -138,3 +138,22 @@ def test_snapshot_knows_directions_and_boundary_conditions(rb, cuda_ok):
     with pytest.raises(rb.RB200Error) as ei:
         rb.restore(plain, snap, q2, rb.LSRK54(plain, q2, 1.0))
     assert ei.value.status == 2
+
+
+@pytest.mark.parametrize("conds", [{1: "wall"}, {1: [1.1, 0.2, -0.1, 0.05, 2.8]}], ids=["wall", "state"])
+def test_boundary_conditions_fp32_bulk(rb, cuda_ok, conds):
+    og = O.Grid(3, 5, [2, 2, 2], [0.0] * 3, [1.0] * 3, [False] * 3)
+    g = wrap_oracle_grid(og)
+    law, form = product_scheme(rb, "eul_kg", 3)
+    dg = rb.DGSEM(law=law, grid=g, volume_form=form, surface_numericalflux=rb.RusanovFlux(),
+                  boundary_conditions=conds, precision="fp32_bulk")
+    c = conds[1]
+    og.set_boundary_condition(1, 2 if c == "wall" else 1, None if c == "wall" else c)
+    olaw = oracle_law("eul_kg", 3)
+    q = initial_state(og, olaw, "eul_kg", seed=64, amp=0.02)
+    ref = og.tendency(olaw, q)
+    qg = rb.GridArray.from_numpy(q)
+    dqg = rb.GridArray.from_numpy(np.zeros_like(q))
+    dg(dqg, qg, 0.0, increment=False)
+    for s in range(law.ns):
+        assert rel_err(dqg.numpy()[:, s], ref[:, s]) <= 5e-5, s
