@@ -113,6 +113,14 @@ rb200_status rb200_lsrk54_step(rb200_handle* h, double* q, double* dq, double ti
 rb200_status rb200_lsrk144_step(rb200_handle* h, double* q, double* dq, double time, double dt, int32_t nsteps,
                                 void* stream);
 
+/* nsteps of dostep!(q, LSRK(rhs!, rka, rkb, rkc, q, dt, t0))  (odesolvers.jl:32-61): any
+ * low-storage table of 1..32 stages (host arrays rka[nstages], rkb[nstages], copied;
+ * rka[i] == 0 skips reading the register in stage i).  The fused steps of
+ * rb200_lsrk54_step with the caller's coefficients; the captured step graph is reused
+ * while the table's values stay the same.  Arguments otherwise as for rb200_lsrk54_step. */
+rb200_status rb200_lsrk_step(rb200_handle* h, double* q, double* dq, const double* rka, const double* rkb,
+                             int32_t nstages, double time, double dt, int32_t nsteps, void* stream);
+
 /* Same as rb200_lsrk54_step for a state held in HOST memory: copies q in, runs the
  * steps, copies q back, synchronously.  The LSRK register lives on the device. */
 rb200_status rb200_lsrk54_step_host(rb200_handle* h, double* q_host, double time, double dt, int32_t nsteps,
@@ -133,6 +141,12 @@ rb200_status rb200_lsrk54_stage(rb200_handle* h, const double* q_in, double* q_o
 rb200_status rb200_lsrk54_stage_range(rb200_handle* h, const double* q_in, double* q_out, double* dq,
                                       int32_t stage, int64_t e_begin, int64_t e_end, double time, double dt,
                                       void* stream);
+
+/* One stage of any low-storage scheme (odesolvers.jl:51-60): dq = rka*dq + RHS(q_in);
+ * q_out = q_in + rkb*dt*dq on the active elements (rka == 0: the register is not read).
+ * The stage-by-stage form of rb200_lsrk_step, for stage callbacks. */
+rb200_status rb200_lsrk_stage(rb200_handle* h, const double* q_in, double* q_out, double* dq, double rka,
+                              double rkb, double time, double dt, void* stream);
 
 /* Ghost elements: only elements 0..num_active-1 are computed and summed by the
  * reductions; elements num_active..E-1 hold other ranks' data (Raven's GridArray ghost
@@ -187,6 +201,13 @@ rb200_status rb200_rlsrk54_step(rb200_handle* h, double* q, double* dq, double* 
  * rb200_rlsrk54_step over the 14 LSRK(14,4) stages.  Arguments as for rb200_rlsrk54_step. */
 rb200_status rb200_rlsrk144_step(rb200_handle* h, double* q, double* dq, double* gamma, double time, double dt,
                                  int32_t nsteps, void* stream);
+
+/* `nsteps` steps of RLSRK(rhs!, rka, rkb, rkc, q, dt, t0)  (odesolvers.jl:73-151) with
+ * any low-storage table of 1..32 stages (host arrays, copied).  Arguments otherwise as
+ * for rb200_rlsrk54_step. */
+rb200_status rb200_rlsrk_step(rb200_handle* h, double* q, double* dq, double* gamma, const double* rka,
+                              const double* rkb, int32_t nstages, double time, double dt, int32_t nsteps,
+                              void* stream);
 
 /* Snapshot / resume of the time-stepper state.  The reference keeps (q, dq, time, dt)
  * in its LSRK struct (odesolvers.jl:32-49; RLSRK adds gamma, :73-84) and has no

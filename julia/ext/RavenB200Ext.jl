@@ -20,9 +20,9 @@
 #   * dostep!(q, solver, f::Function) runs the five stages one by one (rb200_lsrk54_stage),
 #     writes each stage's result back into q and calls f(stagetime, q) after each, as the
 #     reference does; a callback that changes q in place is seen by the next stage;
-#   * LSRK144 has the fused step only, and RLSRK54 / RLSRK144 run their stages, entropy
-#     products and relaxation fused in the library; for these a stage callback raises an
-#     error instead of being ignored.
+#   * any LSRK table (LSRK54, LSRK144, LSRK(rhs!, rka, rkb, rkc, ...)) runs both ways;
+#     RLSRK runs its stages, entropy products and relaxation fused in the library, so for
+#     it a stage callback raises an error instead of being ignored.
 #
 # Not run in this repository: no Julia exists on its build or GPU machines.  The Python
 # binding (raven.jl_b200/_lib.py) drives the same entry points in the GPU tests.
@@ -150,16 +150,16 @@ end
 const B200LSRK = LSRK{FT,AT,NS,<:B200DGSEM} where {FT,AT,NS}
 const B200RLSRK = RLSRK{FT,AT,NS,<:B200DGSEM} where {FT,AT,NS}
 
-# the fused entry points, one per coefficient table of NS stages (ccall takes a constant
-# symbol, so the table is chosen by dispatch)
-const LSRKSig = (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, Float64, Float64, Int32, Ptr{Cvoid})
-const RLSRKSig = (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, Ref{Float64}, Float64, Float64, Int32, Ptr{Cvoid})
-fused_lsrk(::Val{5}, args...) = ccall((:rb200_lsrk54_step, lib), Cint, LSRKSig, args...)
-fused_lsrk(::Val{14}, args...) = ccall((:rb200_lsrk144_step, lib), Cint, LSRKSig, args...)
-fused_lsrk(::Val{NS}, args...) where {NS} = error("raven_b200: no fused LSRK scheme with ", NS, " stages")
-fused_rlsrk(::Val{5}, args...) = ccall((:rb200_rlsrk54_step, lib), Cint, RLSRKSig, args...)
-fused_rlsrk(::Val{14}, args...) = ccall((:rb200_rlsrk144_step, lib), Cint, RLSRKSig, args...)
-fused_rlsrk(::Val{NS}, args...) where {NS} = error("raven_b200: no fused RLSRK scheme with ", NS, " stages")
+# the fused steps take the solver's own coefficient table (any NS up to 32 stages), so
+# LSRK54, LSRK144 and LSRK(rhs!, rka, rkb, rkc, q, dt, t0) all run the same entry point
+fused_lsrk(h, q, dq, rka, rkb, time, dt) =
+    ccall((:rb200_lsrk_step, lib), Cint,
+          (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, Ptr{Float64}, Ptr{Float64}, Int32, Float64, Float64, Int32,
+           Ptr{Cvoid}), h, q, dq, rka, rkb, length(rka), time, dt, 1, stream())
+fused_rlsrk(h, q, dq, γ, rka, rkb, time, dt) =
+    ccall((:rb200_rlsrk_step, lib), Cint,
+          (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, Ref{Float64}, Ptr{Float64}, Ptr{Float64}, Int32, Float64,
+           Float64, Int32, Ptr{Cvoid}), h, q, dq, γ, rka, rkb, length(rka), time, dt, 1, stream())
 
 # solve! (odesolvers.jl:9-30) for the B200 solvers: the same loop, with `nothing` as the
 # default stage callback so that dostep! can run the fused step
@@ -180,28 +180,25 @@ function solve!(q, timeend, solver::Union{B200LSRK,B200RLSRK}; after_step::Funct
     end
 end
 
-# all stages fused on the device (rb200_lsrk54_step / rb200_lsrk144_step)
+# all stages fused on the device (rb200_lsrk_step with the solver's table)
 function dostep!(q, lsrk::LSRK{FT,AT,NS,<:B200DGSEM}, ::Nothing) where {FT,AT,NS}
-    st = fused_lsrk(Val(NS), lsrk.rhs!.handle, pointer(parent(q)), pointer(parent(lsrk.dq)), lsrk.time,
-                    lsrk.dt, 1, stream())
+    rka, rkb = Float64[lsrk.rka...], Float64[lsrk.rkb...]
+    st = fused_lsrk(lsrk.rhs!.handle, pointer(parent(q)), pointer(parent(lsrk.dq)), rka, rkb, lsrk.time, lsrk.dt)
     check(st, lsrk.rhs!.handle)
     lsrk.time += lsrk.dt
 end
 
-# LSRK(5,4) stage times c_i (odesolvers.jl:181-187)
-const RKC54 = (0 // 1, 1432997174477 // 9575080441755, 2526269341429 // 6820363962896,
-               2006345519317 // 3224310063776, 2802321613138 // 2924317926251)
-
-# stage by stage (rb200_lsrk54_stage), after_stage(stagetime, q) after each
-# (odesolvers.jl:51-60)
-function dostep!(q, lsrk::LSRK{FT,AT,5,<:B200DGSEM}, after_stage::Function) where {FT,AT}
+# stage by stage (rb200_lsrk_stage with the solver's a_i, b_i), after_stage(stagetime, q)
+# after each with stagetime = time + c_i dt (odesolvers.jl:51-60)
+function dostep!(q, lsrk::LSRK{FT,AT,NS,<:B200DGSEM}, after_stage::Function) where {FT,AT,NS}
     out = similar(parent(q))
-    for stage = 1:5
-        stagetime = lsrk.time + FT(RKC54[stage]) * lsrk.dt
-        st = ccall((:rb200_lsrk54_stage, lib), Cint,
-                   (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, CuPtr{Float64}, Int32, Float64, Float64, Ptr{Cvoid}),
-                   lsrk.rhs!.handle, pointer(parent(q)), pointer(out), pointer(parent(lsrk.dq)), stage - 1,
-                   stagetime, lsrk.dt, stream())
+    for stage = 1:NS
+        stagetime = lsrk.time + lsrk.rkc[stage] * lsrk.dt
+        st = ccall((:rb200_lsrk_stage, lib), Cint,
+                   (Ptr{Cvoid}, CuPtr{Float64}, CuPtr{Float64}, CuPtr{Float64}, Float64, Float64, Float64, Float64,
+                    Ptr{Cvoid}),
+                   lsrk.rhs!.handle, pointer(parent(q)), pointer(out), pointer(parent(lsrk.dq)),
+                   Float64(lsrk.rka[stage]), Float64(lsrk.rkb[stage]), stagetime, lsrk.dt, stream())
         check(st, lsrk.rhs!.handle)
         copyto!(parent(q), out)
         after_stage(stagetime, q)
@@ -210,15 +207,12 @@ function dostep!(q, lsrk::LSRK{FT,AT,5,<:B200DGSEM}, after_stage::Function) wher
     lsrk.time += lsrk.dt
 end
 
-dostep!(q, lsrk::LSRK{FT,AT,14,<:B200DGSEM}, ::Function) where {FT,AT} =
-    error("raven_b200: LSRK144 runs its stages fused on the device; after_stage is not supported")
-
 # RLSRK54 / RLSRK144 (odesolvers.jl:118-151): the stages, entropy products and the
 # relaxation solve run in the library; γ is read from and written back to the RLSRK struct
 function dostep!(q, r::RLSRK{FT,AT,NS,<:B200DGSEM}, ::Nothing) where {FT,AT,NS}
     γ = Ref(Float64(r.γ))
-    st = fused_rlsrk(Val(NS), r.rhs!.handle, pointer(parent(q)), pointer(parent(r.dq)), γ, r.time, r.dt, 1,
-                     stream())
+    rka, rkb = Float64[r.rka...], Float64[r.rkb...]
+    st = fused_rlsrk(r.rhs!.handle, pointer(parent(q)), pointer(parent(r.dq)), γ, rka, rkb, r.time, r.dt)
     check(st, r.rhs!.handle)
     r.γ = γ[]
     r.time += r.dt

@@ -76,6 +76,9 @@ def lib():
         L.og_grid_set_curved_mortars.argtypes = [P, ctypes.c_int]
         L.og_grid_set_directions.argtypes = [P, ctypes.c_int]
         L.og_grid_set_boundary_condition.argtypes = [P, ctypes.c_int, ctypes.c_int, P]
+        L.og_lsrk_step_coeffs.argtypes = [P, P, P, P, P, P, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        L.og_rlsrk_step_coeffs.argtypes = [P, P, P, P, P, P, P, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        L.og_rlsrk_step_coeffs.restype = ctypes.c_int
         for name in ("og_grid_sizes", "og_grid_points", "og_grid_vmet", "og_grid_smet", "og_grid_vmapM",
                      "og_grid_vmapP", "og_grid_boundary", "og_grid_tree_coords"):
             getattr(L, name).argtypes = [P, P]
@@ -268,6 +271,17 @@ class Grid:
         """One RLSRK(5,4) step in place; gamma is a 1-element float64 array carried
         between steps.  Returns the Newton iterations."""
         return lib().og_rlsrk54_step(self.h, ctypes.byref(law.c), _ptr(q), _ptr(dq), _ptr(gamma), time, dt)
+
+    def lsrk_step(self, law, q, dq, rka, rkb, time, dt):
+        """One LSRK step with the table (rka, rkb)."""
+        a, b = np.ascontiguousarray(rka, dtype=np.float64), np.ascontiguousarray(rkb, dtype=np.float64)
+        lib().og_lsrk_step_coeffs(self.h, ctypes.byref(law.c), _ptr(q), _ptr(dq), _ptr(a), _ptr(b), a.size, time, dt)
+
+    def rlsrk_step(self, law, q, dq, gamma, rka, rkb, time, dt):
+        """One RLSRK step with the table (rka, rkb) (see rlsrk54_step)."""
+        a, b = np.ascontiguousarray(rka, dtype=np.float64), np.ascontiguousarray(rkb, dtype=np.float64)
+        return lib().og_rlsrk_step_coeffs(self.h, ctypes.byref(law.c), _ptr(q), _ptr(dq), _ptr(gamma), _ptr(a),
+                                          _ptr(b), a.size, time, dt)
 
     def rlsrk144_step(self, law, q, dq, gamma, time, dt):
         """One RLSRK(14,4) step in place (see rlsrk54_step)."""

@@ -1474,7 +1474,7 @@ static int rlsrk_step(const og_grid* g, const og_law* law, const LsrkScheme& sc,
                       double* gamma, double time, double dt) {
     const int64_t n = (int64_t)g->np * num_states(g, law) * g->E;
     std::vector<double> q0(q, q + n), k(n);
-    double bf[14], sums[2];
+    double bf[32], sums[2];
     rkb_full(sc, bf);
     og_entropy_sums(g, law, q0.data(), nullptr, 0.0, nullptr, sums);
     const double eta0 = sums[0];
@@ -1509,6 +1509,18 @@ extern "C" int og_rlsrk54_step(const og_grid* g, const og_law* law, double* q, d
 extern "C" int og_rlsrk144_step(const og_grid* g, const og_law* law, double* q, double* dq, double* gamma,
                                 double time, double dt) {
     return rlsrk_step(g, law, kScheme144, q, dq, gamma, time, dt);
+}
+
+// LSRK(rhs!, rka, rkb, rkc, q, dt, t0) and RLSRK(...) with a caller's table
+// (odesolvers.jl:32-61, 73-151)
+extern "C" void og_lsrk_step_coeffs(const og_grid* g, const og_law* law, double* q, double* dq, const double* rka,
+                                    const double* rkb, int nstages, double time, double dt) {
+    lsrk_step(g, law, LsrkScheme{nstages, rka, rkb}, q, dq, time, dt);
+}
+
+extern "C" int og_rlsrk_step_coeffs(const og_grid* g, const og_law* law, double* q, double* dq, double* gamma,
+                                    const double* rka, const double* rkb, int nstages, double time, double dt) {
+    return rlsrk_step(g, law, LsrkScheme{nstages, rka, rkb}, q, dq, gamma, time, dt);
 }
 
 extern "C" int64_t og_solve_rlsrk(const og_grid* g, const og_law* law, double* q, double dt, double timeend,

@@ -79,6 +79,11 @@ void og_grid_set_directions(og_grid* g, int mask);
 /* boundarystate of the faces with boundary code `tag` (1..8): kind 0 q+ = q-, 1 q+ =
  * state (Ns doubles), 2 a reflecting wall (Euler). */
 void og_grid_set_boundary_condition(og_grid* g, int tag, int kind, const double* state);
+/* One step of LSRK / RLSRK with a caller's low-storage table (nstages <= 32). */
+void og_lsrk_step_coeffs(const og_grid* g, const og_law* law, double* q, double* dq, const double* rka,
+                         const double* rkb, int nstages, double time, double dt);
+int og_rlsrk_step_coeffs(const og_grid* g, const og_law* law, double* q, double* dq, double* gamma,
+                         const double* rka, const double* rkb, int nstages, double time, double dt);
 
 /* Standalone LGL operators for nq points (computed in __float128, rounded). */
 void og_lgl(int nq, double* r, double* w, double* D);

@@ -39,7 +39,7 @@ from .grids import Grid, brick_tree_order, jl_range, lobatto_operators
 __all__ = [
     "LobattoCell", "brick", "BrickGrid", "GridManager", "generate", "Grid", "AdvectionLaw", "EulerLaw",
     "RusanovFlux", "CentralFlux", "KennedyGruberFlux", "EntropyConservativeFlux", "RoeFlux", "MatrixFlux", "WeakForm",
-    "FluxDifferencingForm", "GridArray", "DGSEM", "LSRK54", "LSRK144", "RLSRK54", "RLSRK144", "solve",
+    "FluxDifferencingForm", "GridArray", "DGSEM", "LSRK", "LSRK54", "LSRK144", "RLSRK", "RLSRK54", "RLSRK144", "solve",
     "weightednorm", "integrals",
     "entropyintegral", "entropyproduct", "snapshot", "restore",
     "jl_range", "RB200Error", "brick_tree_order", "adapt", "AdaptRefine", "AdaptNone", "AdaptCoarsen",
@@ -560,15 +560,74 @@ class LSRK54:
             self.time += self.dt
 
 
-class LSRK144(LSRK54):
+class LSRK:
+    """LSRK(rhs!, rka, rkb, rkc, q, dt, t0) (src/balancelaws/odesolvers.jl:32-61): any
+    low-storage (2N) Runge-Kutta table of 1..32 stages on the fused stage kernels.
+    dostep(q, n) runs n fused steps (rb200_lsrk_step); with `after_stage` every stage is
+    its own kernel (rb200_lsrk_stage), written back into q before
+    after_stage(time + rkc_i dt, q) is called, as LSRK54.dostep does."""
+
+    def __init__(self, dg, rka, rkb, rkc, q, dt, t0=0.0):
+        self.dg = dg
+        self.rka = np.ascontiguousarray(rka, dtype=np.float64)
+        self.rkb = np.ascontiguousarray(rkb, dtype=np.float64)
+        self.rkc = np.ascontiguousarray(rkc, dtype=np.float64)
+        if not (self.rka.size == self.rkb.size == self.rkc.size) or not 1 <= self.rka.size <= 32:
+            raise ValueError("rka, rkb and rkc must have the same length, 1..32")
+        self.dt = float(dt)
+        self.time = float(t0)
+        self.dq = q.similar()  # fill!(dq, 0)
+        self._stage_out = None
+
+    def dostep(self, q, nsteps=1, after_stage=None):
+        """dostep!(q, lsrk, after_stage) (odesolvers.jl:51-61), `nsteps` times."""
+        L, h = _lib.lib(), self.dg._h
+        if after_stage is None:
+            dq = self.dq.ptr() if self.dg.precision == "fp64" else None
+            _lib.check(L.rb200_lsrk_step(h, q.ptr(), dq, self.rka.ctypes.data_as(ctypes.c_void_p),
+                                         self.rkb.ctypes.data_as(ctypes.c_void_p), int(self.rka.size), self.time,
+                                         self.dt, int(nsteps), _stream_ptr()), h)
+            for _ in range(nsteps):
+                self.time += self.dt
+            return
+        if self._stage_out is None or self._stage_out.data.shape != q.data.shape:
+            self._stage_out = q.similar()
+        out = self._stage_out
+        for _ in range(nsteps):
+            for i in range(self.rka.size):
+                stagetime = self.time + self.rkc[i] * self.dt
+                _lib.check(L.rb200_lsrk_stage(h, q.ptr(), out.ptr(), self.dq.ptr(), float(self.rka[i]),
+                                              float(self.rkb[i]), stagetime, self.dt, _stream_ptr()), h)
+                q.data.copy_(out.data)
+                after_stage(stagetime, q)
+            self.time += self.dt
+
+
+# LSRK(14,4) (odesolvers.jl:191-239, coefficients_lsrk144): the reference's Float64 literals
+LSRK144_RKA = (0.0, -0.7188012108672410, -0.7785331173421570, -0.0053282796654044, -0.8552979934029281,
+               -3.9564138245774565, -1.5780575380587385, -2.0837094552574054, -0.7483334182761610,
+               -0.7032861106563359, 0.0013917096117681, -0.0932075369637460, -0.9514200470875948,
+               -7.1151571693922548)
+LSRK144_RKB = (0.0367762454319673, 0.3136296607553959, 0.1531848691869027, 0.0030097086818182, 0.3326293790646110,
+               0.2440251405350864, 0.3718879239592277, 0.6204126221582444, 0.1524043173028741, 0.0760894927419266,
+               0.0077604214040978, 0.0024647284755382, 0.0780348340049386, 5.5059777270269628)
+LSRK144_RKC = (0.0, 0.0367762454319673, 0.1249685262725025, 0.2446177702277698, 0.2476149531070420,
+               0.2969311120382472, 0.3978149645802642, 0.5270854589440328, 0.6981269994175695, 0.8190890835352128,
+               0.8527059887098624, 0.8604711817462826, 0.8627060376969976, 0.8734213127600976)
+
+
+class LSRK144(LSRK):
     """LSRK144(rhs!, q, dt; t0 = 0) (src/balancelaws/odesolvers.jl:68-71, 191-239): the
-    14-stage fourth-order low-storage scheme on the same fused stage kernels.  Its stages
-    run fused only; a stage callback raises instead of being ignored."""
+    14-stage fourth-order low-storage scheme.  The fused steps use rb200_lsrk144_step;
+    stage callbacks run the stages one by one as LSRK does."""
+
+    def __init__(self, dg, q, dt, t0=0.0):
+        super().__init__(dg, LSRK144_RKA, LSRK144_RKB, LSRK144_RKC, q, dt, t0)
 
     def dostep(self, q, nsteps=1, after_stage=None):
         """dostep!(q, lsrk, after_stage) (odesolvers.jl:51-61), `nsteps` times."""
         if after_stage is not None:
-            raise NotImplementedError("LSRK144 runs its 14 stages fused on the device; after_stage is not supported")
+            return super().dostep(q, nsteps, after_stage)
         self.dg.lsrk144_steps(q, self.dq, self.time, self.dt, nsteps)
         for _ in range(nsteps):
             self.time += self.dt
@@ -603,6 +662,28 @@ class RLSRK54:
 
     def _entry(self):
         return _lib.lib().rb200_rlsrk54_step
+
+
+class RLSRK(RLSRK54):
+    """RLSRK(rhs!, rka, rkb, rkc, q, dt, t0) (src/balancelaws/odesolvers.jl:73-151): the
+    relaxation step over any low-storage table of 1..32 stages.  FP64 operators only."""
+
+    def __init__(self, dg, rka, rkb, rkc, q, dt, t0=0.0):
+        super().__init__(dg, q, dt, t0)
+        self.rka = np.ascontiguousarray(rka, dtype=np.float64)
+        self.rkb = np.ascontiguousarray(rkb, dtype=np.float64)
+        self.rkc = np.ascontiguousarray(rkc, dtype=np.float64)
+        if not (self.rka.size == self.rkb.size == self.rkc.size) or not 1 <= self.rka.size <= 32:
+            raise ValueError("rka, rkb and rkc must have the same length, 1..32")
+
+    def _entry(self):
+        L = _lib.lib()
+        rka, rkb, n = self.rka.ctypes.data_as(ctypes.c_void_p), self.rkb.ctypes.data_as(ctypes.c_void_p), self.rka.size
+
+        def call(h, q, dq, g, time, dt, nsteps, stream):
+            return L.rb200_rlsrk_step(h, q, dq, g, rka, rkb, int(n), time, dt, nsteps, stream)
+
+        return call
 
 
 class RLSRK144(RLSRK54):

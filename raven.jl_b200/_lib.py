@@ -56,6 +56,9 @@ EXPORTED = [
     "rb200_probe_fp64_rate",
     "rb200_set_directions",
     "rb200_set_boundary_condition",
+    "rb200_lsrk_step",
+    "rb200_lsrk_stage",
+    "rb200_rlsrk_step",
     "rb200_weighted_sums_noalloc",
     "rb200_server_create",
     "rb200_server_submit",
@@ -187,6 +190,9 @@ def lib():
     L.rb200_probe_fp64_rate.argtypes = [I64, P, P]
     L.rb200_set_directions.argtypes = [P, I32]
     L.rb200_set_boundary_condition.argtypes = [P, I32, I32, P]
+    L.rb200_lsrk_step.argtypes = [P, P, P, P, P, I32, D, D, I32, P]
+    L.rb200_lsrk_stage.argtypes = [P, P, P, P, D, D, D, D, P]
+    L.rb200_rlsrk_step.argtypes = [P, P, P, P, P, P, I32, D, D, I32, P]
     L.rb200_weighted_sums_noalloc.argtypes = [P, P, I32, I32, I64, P, P]
     L.rb200_last_error.argtypes = [P]
     L.rb200_last_error.restype = ctypes.c_char_p

@@ -67,7 +67,11 @@ struct rb200_handle {
     const double* graph_q = nullptr;
     const void* graph_dq = nullptr;
     double graph_dt = 0.0;
-    const double* graph_rka = nullptr;  // a coefficients of the captured graph's scheme
+    // the captured graph's scheme, by value (a caller's table may change between calls)
+    int graph_nst = 0;
+    double graph_rka[32] = {0}, graph_rkb[32] = {0};
+    // a caller's coefficient table (rb200_lsrk_step, rb200_rlsrk_step), copied per call
+    double user_rka[32] = {0}, user_rkb[32] = {0};
     int use_graphs = 1;
     int pipe_grid = 0;            // CTAs of the pipelined kernel (0: not eligible)
     int pipe_curved_grid = 0;     // CTAs of the curved-grid pipelined kernel, FP32 bulk or FP64 (0: not eligible)
@@ -120,7 +124,7 @@ struct Scheme {
     const double* rka;
     const double* rkb;
 };
-constexpr int kMaxStages = 14;
+constexpr int kMaxStages = 32;
 const Scheme kLSRK54{5, RKA, RKB};
 const Scheme kLSRK144{14, RKA144, RKB144};
 
@@ -330,8 +334,10 @@ rb200_status run_steps(rb200_handle* h, const Scheme& sc, double* q, void* dq, d
         // kernel attributes get configured outside the capture
         if ((rs = enqueue_steps(h, sc, q, dq, dt, 2, st, &cur)) != RB200_OK) return rs;
         done = 2;
-        if (!h->graph_exec || h->graph_q != q || h->graph_dq != dq || h->graph_dt != dt ||
-            h->graph_rka != sc.rka) {
+        const bool same_scheme = h->graph_nst == sc.stages &&
+                                 std::memcmp(h->graph_rka, sc.rka, sizeof(double) * sc.stages) == 0 &&
+                                 std::memcmp(h->graph_rkb, sc.rkb, sizeof(double) * sc.stages) == 0;
+        if (!h->graph_exec || h->graph_q != q || h->graph_dq != dq || h->graph_dt != dt || !same_scheme) {
             free_graph(h);
             cudaError_t e = cudaSuccess;
             if (!h->cap_stream) e = cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking);
@@ -355,7 +361,9 @@ rb200_status run_steps(rb200_handle* h, const Scheme& sc, double* q, void* dq, d
             h->graph_q = q;
             h->graph_dq = dq;
             h->graph_dt = dt;
-            h->graph_rka = sc.rka;
+            h->graph_nst = sc.stages;
+            std::memcpy(h->graph_rka, sc.rka, sizeof(double) * sc.stages);
+            std::memcpy(h->graph_rkb, sc.rkb, sizeof(double) * sc.stages);
         }
         for (; done + 2 <= nsteps; done += 2) {
             cudaError_t e = cudaGraphLaunch(h->graph_exec, st);
@@ -804,16 +812,39 @@ rb200_status rb200_lsrk144_step(rb200_handle* h, double* q, double* dq, double t
     return lsrk_steps(h, kLSRK144, q, dq, dt, nsteps, stream);
 }
 
+// A caller's low-storage table: finite, at most kMaxStages stages, copied into the handle.
+static rb200_status user_scheme(rb200_handle* h, const double* rka, const double* rkb, int32_t nstages, Scheme* sc) {
+    if (!rka || !rkb) return fail(h, RB200_ERR_BAD_ARG, "null coefficient table");
+    if (nstages < 1 || nstages > kMaxStages) return fail(h, RB200_ERR_BAD_ARG, "nstages must be in 1..32");
+    for (int i = 0; i < nstages; ++i)
+        if (!std::isfinite(rka[i]) || !std::isfinite(rkb[i])) return fail(h, RB200_ERR_BAD_ARG, "coefficients not finite");
+    std::memcpy(h->user_rka, rka, sizeof(double) * nstages);
+    std::memcpy(h->user_rkb, rkb, sizeof(double) * nstages);
+    *sc = Scheme{nstages, h->user_rka, h->user_rkb};
+    return RB200_OK;
+}
+
+rb200_status rb200_lsrk_step(rb200_handle* h, double* q, double* dq, const double* rka, const double* rkb,
+                             int32_t nstages, double time, double dt, int32_t nsteps, void* stream) {
+    (void)time;
+    if (!h) return RB200_ERR_BAD_ARG;
+    Scheme sc;
+    rb200_status st = user_scheme(h, rka, rkb, nstages, &sc);
+    if (st != RB200_OK) return st;
+    return lsrk_steps(h, sc, q, dq, dt, nsteps, stream);
+}
+
 // One stage of LSRK(5,4) (odesolvers.jl:163-189) from q_in to q_out on elements
 // e_begin..e_end-1: the building block of a step whose ghost elements are refreshed
 // between stages (the start!/finish! exchange of dgsem.jl:95-100 around every
 // right-hand side), with the interior elements computed while the exchange runs.
-static rb200_status stage_range(rb200_handle* h, const double* q_in, double* q_out, double* dq, int32_t stage,
-                                int64_t e_begin, int64_t e_end, double dt, cudaStream_t s) {
+static rb200_status stage_range(rb200_handle* h, const double* q_in, double* q_out, double* dq, double rka,
+                                double rkb, int64_t e_begin, int64_t e_end, double dt, cudaStream_t s) {
     if (!q_in || !q_out || (!dq && h->prec == RB200_PRECISION_FP64))
         return fail(h, RB200_ERR_BAD_ARG, "null state pointer");
     if (q_in == q_out) return fail(h, RB200_ERR_BAD_ARG, "q_in and q_out must be different buffers");
-    if (stage < 0 || stage > 4 || !std::isfinite(dt)) return fail(h, RB200_ERR_BAD_ARG, "bad stage or dt");
+    if (!std::isfinite(rka) || !std::isfinite(rkb) || !std::isfinite(dt))
+        return fail(h, RB200_ERR_BAD_ARG, "bad coefficients or dt");
     if (e_begin < 0 || e_begin > e_end || e_end > h->E_active)
         return fail(h, RB200_ERR_BAD_ARG, "element range outside the active elements");
     if (e_begin == e_end) return RB200_OK;
@@ -824,9 +855,9 @@ static rb200_status stage_range(rb200_handle* h, const double* q_in, double* q_o
     a.q_in = q_in;
     a.q_out = q_out;
     a.dq = h->prec == RB200_PRECISION_FP32_BULK ? static_cast<void*>(h->d_dq32) : static_cast<void*>(dq);
-    a.mode = RKA[stage] == 0.0 ? MODE_STAGE_FIRST : MODE_STAGE;
-    a.rka = RKA[stage];
-    a.rkb_dt = RKB[stage] * dt;
+    a.mode = rka == 0.0 ? MODE_STAGE_FIRST : MODE_STAGE;
+    a.rka = rka;
+    a.rkb_dt = rkb * dt;
     cudaError_t e = launch_any(h, a, s);
     if (e != cudaSuccess) return cuda_fail(h, e, "stage kernel launch");
     return RB200_OK;
@@ -836,7 +867,8 @@ rb200_status rb200_lsrk54_stage(rb200_handle* h, const double* q_in, double* q_o
                                 double time, double dt, void* stream) {
     (void)time;
     if (!h) return RB200_ERR_BAD_ARG;
-    return stage_range(h, q_in, q_out, dq, stage, 0, h->E_active, dt, (cudaStream_t)stream);
+    if (stage < 0 || stage > 4) return fail(h, RB200_ERR_BAD_ARG, "bad stage or dt");
+    return stage_range(h, q_in, q_out, dq, RKA[stage], RKB[stage], 0, h->E_active, dt, (cudaStream_t)stream);
 }
 
 rb200_status rb200_lsrk54_stage_range(rb200_handle* h, const double* q_in, double* q_out, double* dq,
@@ -844,7 +876,15 @@ rb200_status rb200_lsrk54_stage_range(rb200_handle* h, const double* q_in, doubl
                                       void* stream) {
     (void)time;
     if (!h) return RB200_ERR_BAD_ARG;
-    return stage_range(h, q_in, q_out, dq, stage, e_begin, e_end, dt, (cudaStream_t)stream);
+    if (stage < 0 || stage > 4) return fail(h, RB200_ERR_BAD_ARG, "bad stage or dt");
+    return stage_range(h, q_in, q_out, dq, RKA[stage], RKB[stage], e_begin, e_end, dt, (cudaStream_t)stream);
+}
+
+rb200_status rb200_lsrk_stage(rb200_handle* h, const double* q_in, double* q_out, double* dq, double rka,
+                              double rkb, double time, double dt, void* stream) {
+    (void)time;
+    if (!h) return RB200_ERR_BAD_ARG;
+    return stage_range(h, q_in, q_out, dq, rka, rkb, 0, h->E_active, dt, (cudaStream_t)stream);
 }
 
 rb200_status rb200_set_active_elements(rb200_handle* h, int64_t num_active) {
@@ -992,6 +1032,17 @@ rb200_status rb200_rlsrk144_step(rb200_handle* h, double* q, double* dq, double*
                                  int32_t nsteps, void* stream) {
     (void)time;
     return rlsrk_steps(h, kLSRK144, q, dq, gamma, dt, nsteps, stream);
+}
+
+rb200_status rb200_rlsrk_step(rb200_handle* h, double* q, double* dq, double* gamma, const double* rka,
+                              const double* rkb, int32_t nstages, double time, double dt, int32_t nsteps,
+                              void* stream) {
+    (void)time;
+    if (!h) return RB200_ERR_BAD_ARG;
+    Scheme sc;
+    rb200_status st = user_scheme(h, rka, rkb, nstages, &sc);
+    if (st != RB200_OK) return st;
+    return rlsrk_steps(h, sc, q, dq, gamma, dt, nsteps, stream);
 }
 
 // ---------------------------------------------------------------------------------

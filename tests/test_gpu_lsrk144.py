@@ -109,3 +109,81 @@ def test_lsrk144_after_stage_is_refused(rb, cuda_ok):
     q = rb.GridArray.from_numpy(initial_state(og, olaw, CASES[1][3]))
     with pytest.raises(NotImplementedError):
         rb.LSRK144(dg, q, 1e-3).dostep(q, 1, after_stage=lambda t, q: None)
+
+
+# Williamson's three-stage third-order low-storage scheme (J. Comput. Phys. 35 (1980), 48-56)
+RK3_A = (0.0, -5.0 / 9.0, -153.0 / 128.0)
+RK3_B = (1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0)
+RK3_C = (0.0, 1.0 / 3.0, 3.0 / 4.0)
+
+
+@pytest.mark.parametrize("case", CASES[:3], ids=[f"{c[0]}d-nq{c[1]}-{c[3]}-warp{c[4]}" for c in CASES[:3]])
+def test_lsrk_any_table(rb, cuda_ok, case):
+    """LSRK(rhs!, rka, rkb, rkc, q, dt, t0) with a table of the caller's (a three-stage
+    scheme) against the oracle, and then a different table on the same handle."""
+    og, dg, olaw, law = _build(rb, *case)
+    q = initial_state(og, olaw, case[3], seed=25, amp=0.01)
+    dt = 1e-3
+    qo, dqo = q.copy(order="F"), og.state(olaw)
+    for i in range(5):
+        og.lsrk_step(olaw, qo, dqo, RK3_A, RK3_B, i * dt, dt)
+    qg = rb.GridArray.from_numpy(q)
+    solver = rb.LSRK(dg, RK3_A, RK3_B, RK3_C, qg, dt)
+    solver.dostep(qg, 5)  # two eager steps, then the captured graph
+    dg.sync_status()
+    for s in range(law.ns):
+        assert rel_err(qg.numpy()[:, s], qo[:, s]) <= 1e-12, s
+    # another table of the same length on the same handle: the graph is recaptured
+    A2 = (0.0, -0.5, -1.0)
+    B2 = (0.25, 0.5, 0.4)
+    for i in range(5):
+        og.lsrk_step(olaw, qo, dqo, A2, B2, (5 + i) * dt, dt)
+    s2 = rb.LSRK(dg, A2, B2, RK3_C, qg, dt, t0=5 * dt)
+    s2.dq = solver.dq
+    s2.dostep(qg, 5)
+    dg.sync_status()
+    for s in range(law.ns):
+        assert rel_err(qg.numpy()[:, s], qo[:, s]) <= 1e-12, s
+
+
+def test_lsrk_generic_table_equals_lsrk54(rb, cuda_ok):
+    og, dg, olaw, law = _build(rb, *CASES[0])
+    q = initial_state(og, olaw, CASES[0][3], seed=26, amp=0.01)
+    a, b = rb.GridArray.from_numpy(q), rb.GridArray.from_numpy(q)
+    rb.LSRK54(dg, a, 1e-3).dostep(a, 6)
+    A = (0.0, -567301805773 / 1357537059087, -2404267990393 / 2016746695238, -3550918686646 / 2091501179385,
+         -1275806237668 / 842570457699)
+    B = (1432997174477 / 9575080441755, 5161836677717 / 13612068292357, 1720146321549 / 2090206949498,
+         3134564353537 / 4481467310338, 2277821191437 / 14882151754819)
+    rb.LSRK(dg, A, B, rb.LSRK54_RKC, b, 1e-3).dostep(b, 6)
+    assert np.array_equal(a.numpy(), b.numpy())
+
+
+def test_lsrk144_stage_callbacks(rb, cuda_ok):
+    """LSRK144 with after_stage: its 14 stages one by one, the callback at time + c_i dt,
+    and the same state as the fused steps, bit for bit."""
+    og, dg, olaw, law = _build(rb, *CASES[1])
+    q = initial_state(og, olaw, CASES[1][3], seed=27, amp=0.01)
+    a, b = rb.GridArray.from_numpy(q), rb.GridArray.from_numpy(q)
+    dt = 1e-3
+    rb.LSRK144(dg, a, dt).dostep(a, 2)
+    times = []
+    rb.LSRK144(dg, b, dt).dostep(b, 2, after_stage=lambda t, qq: times.append(t))
+    assert np.array_equal(a.numpy(), b.numpy())
+    want = [i * dt + c * dt for i in range(2) for c in rb.LSRK144_RKC]
+    assert times == pytest.approx(want, rel=0, abs=1e-15)
+
+
+def test_rlsrk_any_table(rb, cuda_ok):
+    og, dg, olaw, law = _build(rb, 2, 6, (3, 4), "eul_ec", O.WARP_NONE)
+    q = initial_state(og, olaw, "eul_ec", seed=28, amp=0.01)
+    dt = 2e-2
+    qo, dqo, gamma = q.copy(order="F"), og.state(olaw), np.ones(1)
+    for i in range(3):
+        og.rlsrk_step(olaw, qo, dqo, gamma, RK3_A, RK3_B, i * dt, dt)
+    qg = rb.GridArray.from_numpy(q)
+    solver = rb.RLSRK(dg, RK3_A, RK3_B, RK3_C, qg, dt)
+    solver.dostep(qg, 3)
+    for s in range(law.ns):
+        assert rel_err(qg.numpy()[:, s], qo[:, s]) <= 1e-12, s
+    assert abs(solver.gamma - gamma[0]) <= 1e-9

@@ -178,3 +178,16 @@ def test_oracle_walls_conserve_mass_and_energy():
     g.set_boundary_condition(1, 0)
     dq0 = g.tendency(law, q)
     assert abs((MJ * dq0[:, 0, :]).sum()) > 1e-10 * np.abs(MJ * dq0[:, 0, :]).sum()
+
+
+def test_oracle_generic_table_equals_lsrk54():
+    g, law, q, dt = _square_1d(5, 5, "euler")
+    q2, dq1, dq2 = q.copy(order="F"), g.state(law), g.state(law)
+    A = (0.0, -567301805773 / 1357537059087, -2404267990393 / 2016746695238, -3550918686646 / 2091501179385,
+         -1275806237668 / 842570457699)
+    B = (1432997174477 / 9575080441755, 5161836677717 / 13612068292357, 1720146321549 / 2090206949498,
+         3134564353537 / 4481467310338, 2277821191437 / 14882151754819)
+    for i in range(3):
+        g.lsrk54_step(law, q, dq1, i * dt, dt)
+        g.lsrk_step(law, q2, dq2, A, B, i * dt, dt)
+    assert np.array_equal(q, q2)
