@@ -104,11 +104,12 @@ def test_schemes_alternate_on_one_handle(rb, cuda_ok):
     assert np.array_equal(qa.numpy(), qb.numpy())
 
 
-def test_lsrk144_after_stage_is_refused(rb, cuda_ok):
-    og, dg, olaw, law = _build(rb, *CASES[1])
-    q = rb.GridArray.from_numpy(initial_state(og, olaw, CASES[1][3]))
+def test_rlsrk144_after_stage_is_refused(rb, cuda_ok):
+    """The relaxation step runs its stages fused: a stage callback raises."""
+    og, dg, olaw, law = _build(rb, 2, 6, (3, 4), "eul_ec", O.WARP_NONE)
+    q = rb.GridArray.from_numpy(initial_state(og, olaw, "eul_ec"))
     with pytest.raises(NotImplementedError):
-        rb.LSRK144(dg, q, 1e-3).dostep(q, 1, after_stage=lambda t, q: None)
+        rb.RLSRK144(dg, q, 1e-3).dostep(q, 1, after_stage=lambda t, q: None)
 
 
 # Williamson's three-stage third-order low-storage scheme (J. Comput. Phys. 35 (1980), 48-56)
