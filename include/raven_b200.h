@@ -148,6 +148,12 @@ rb200_status rb200_lsrk54_stage_range(rb200_handle* h, const double* q_in, doubl
 rb200_status rb200_lsrk_stage(rb200_handle* h, const double* q_in, double* q_out, double* dq, double rka,
                               double rkb, double time, double dt, void* stream);
 
+/* rb200_lsrk_stage on the active elements e_begin..e_end-1 only (the partitioned path's
+ * interior / partition-boundary split, as rb200_lsrk54_stage_range). */
+rb200_status rb200_lsrk_stage_range(rb200_handle* h, const double* q_in, double* q_out, double* dq, double rka,
+                                    double rkb, int64_t e_begin, int64_t e_end, double time, double dt,
+                                    void* stream);
+
 /* Ghost elements: only elements 0..num_active-1 are computed and summed by the
  * reductions; elements num_active..E-1 hold other ranks' data (Raven's GridArray ghost
  * cells, gridarrays.jl:26-40).  Their face maps point to themselves; the faces of active

@@ -495,6 +495,14 @@ class DGSEM:
                                                        int(e_begin), int(e_end), float(time), float(dt),
                                                        _stream_ptr()), self._h)
 
+    def lsrk_stage_range(self, q_in, q_out, dq, rka, rkb, e_begin, e_end, time, dt):
+        """One stage of any low-storage table (coefficients rka, rkb) on the active
+        elements e_begin..e_end-1."""
+        _lib.check(_lib.lib().rb200_lsrk_stage_range(self._h, q_in.ptr(), q_out.ptr(),
+                                                     dq.ptr() if dq is not None else None, float(rka), float(rkb),
+                                                     int(e_begin), int(e_end), float(time), float(dt),
+                                                     _stream_ptr()), self._h)
+
     def lsrk54_steps(self, q, dq, time, dt, nsteps):
         _lib.check(_lib.lib().rb200_lsrk54_step(self._h, q.ptr(), dq.ptr() if dq is not None else None,
                                                 float(time), float(dt), int(nsteps), _stream_ptr()), self._h)

@@ -58,6 +58,7 @@ EXPORTED = [
     "rb200_set_boundary_condition",
     "rb200_lsrk_step",
     "rb200_lsrk_stage",
+    "rb200_lsrk_stage_range",
     "rb200_rlsrk_step",
     "rb200_weighted_sums_noalloc",
     "rb200_server_create",
@@ -192,6 +193,7 @@ def lib():
     L.rb200_set_boundary_condition.argtypes = [P, I32, I32, P]
     L.rb200_lsrk_step.argtypes = [P, P, P, P, P, I32, D, D, I32, P]
     L.rb200_lsrk_stage.argtypes = [P, P, P, P, D, D, D, D, P]
+    L.rb200_lsrk_stage_range.argtypes = [P, P, P, P, D, D, I64, I64, D, D, P]
     L.rb200_rlsrk_step.argtypes = [P, P, P, P, P, P, I32, D, D, I32, P]
     L.rb200_weighted_sums_noalloc.argtypes = [P, P, I32, I32, I64, P, P]
     L.rb200_last_error.argtypes = [P]

@@ -887,6 +887,14 @@ rb200_status rb200_lsrk_stage(rb200_handle* h, const double* q_in, double* q_out
     return stage_range(h, q_in, q_out, dq, rka, rkb, 0, h->E_active, dt, (cudaStream_t)stream);
 }
 
+rb200_status rb200_lsrk_stage_range(rb200_handle* h, const double* q_in, double* q_out, double* dq, double rka,
+                                    double rkb, int64_t e_begin, int64_t e_end, double time, double dt,
+                                    void* stream) {
+    (void)time;
+    if (!h) return RB200_ERR_BAD_ARG;
+    return stage_range(h, q_in, q_out, dq, rka, rkb, e_begin, e_end, dt, (cudaStream_t)stream);
+}
+
 rb200_status rb200_set_active_elements(rb200_handle* h, int64_t num_active) {
     if (!h) return RB200_ERR_BAD_ARG;
     if (num_active < 0 || num_active > h->E) return fail(h, RB200_ERR_BAD_ARG, "active elements out of range");

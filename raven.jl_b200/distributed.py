@@ -248,8 +248,8 @@ class DistributedDGSEM:
     """DGSEM over the ranks of a process group: this rank's elements plus ghosts on its
     GPU, LSRK(5,4) stage by stage with a ghost exchange before every stage."""
 
-    def __init__(self, *, law, grid, surface_numericalflux, volume_form=None, precision="fp64", group=None,
-                 device=None):
+    def __init__(self, *, law, grid, surface_numericalflux, volume_form=None, directions=None,
+                 boundary_conditions=None, precision="fp64", group=None, device=None):
         import torch.distributed as dist
 
         from . import DGSEM
@@ -260,7 +260,8 @@ class DistributedDGSEM:
         self.local = LocalGrid(grid, self.parts, self.rank)
         self.law = law
         self.dg = DGSEM(law=law, grid=self.local.grid, surface_numericalflux=surface_numericalflux,
-                        volume_form=volume_form, precision=precision, device=device)
+                        volume_form=volume_form, directions=directions, boundary_conditions=boundary_conditions,
+                        precision=precision, device=device)
         self.dg.set_active_elements(self.local.num_local)
         self.pattern = node_comm_pattern(grid, self.parts, self.rank, law.ns)
         # NCCL addresses peers by global rank
@@ -295,6 +296,23 @@ class DistributedDGSEM:
                 self.dg.lsrk54_stage_range(cur, oth, dq, s, 0, n_int, t, dt)
                 self.halo.finish(cur.data.view(-1))
                 self.dg.lsrk54_stage_range(cur, oth, dq, s, n_int, n_loc, t, dt)
+                cur, oth = oth, cur
+        if cur is not q:
+            q.data.copy_(cur.data)
+
+    def lsrk_steps(self, q, dq, rka, rkb, rkc, time, dt, nsteps):
+        """nsteps of LSRK(rhs!, rka, rkb, rkc, ...) on this rank's elements, any table."""
+        if self._qtmp is None or self._qtmp.data.shape != q.data.shape:
+            self._qtmp = q.similar()
+        cur, oth = q, self._qtmp
+        n_int, n_loc = self.local.num_interior, self.local.num_local
+        for step in range(nsteps):
+            t = time + step * dt
+            for a, b, c in zip(rka, rkb, rkc):
+                self.halo.start(cur.data.view(-1))
+                self.dg.lsrk_stage_range(cur, oth, dq, a, b, 0, n_int, t + c * dt, dt)
+                self.halo.finish(cur.data.view(-1))
+                self.dg.lsrk_stage_range(cur, oth, dq, a, b, n_int, n_loc, t + c * dt, dt)
                 cur, oth = oth, cur
         if cur is not q:
             q.data.copy_(cur.data)

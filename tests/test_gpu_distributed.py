@@ -252,3 +252,58 @@ def test_bench_sharded_one_rank(rb, cuda_ok):
     assert line["n_gpus"] == 1 and line["scaling"] == "strong" and line["value"] > 0
     assert line["exchange"]["bytes_received_per_stage_all_ranks"] == 0
     assert line["exchange"]["ghost_elements_all_ranks"] == 0
+
+
+@pytest.mark.parametrize("nranks", [2, 3])
+def test_partitioned_any_table_walls_directions(rb, cuda_ok, nranks):
+    """The partitioned stages with the generic entry (rb200_lsrk_stage_range, the LSRK144
+    table), reflecting walls and a direction subset on every rank equal a single handle
+    with the same settings, bit for bit."""
+    import torch
+
+    from raven_b200 import distributed as D
+
+    og, g, law, form, q0 = _setup(rb, "eul_kg", 5, (5, 4, 3), (1, 0, 0), "fp64")
+    kw = dict(law=law, volume_form=form, surface_numericalflux=rb.RusanovFlux(), directions=(1, 3),
+              boundary_conditions={1: "wall"})
+    dt, nsteps = 1e-3, 2
+    ref_dg = rb.DGSEM(grid=g, **kw)
+    ref = rb.GridArray.from_numpy(q0)
+    rb.LSRK144(ref_dg, ref, dt).dostep(ref, nsteps)
+    ref_dg.sync_status()
+    q_ref = ref.numpy()
+    parts = D.partition(g.E, nranks)
+    locs = [D.LocalGrid(g, parts, r) for r in range(nranks)]
+    dgs, halos, cur, oth, dqs = [], [], [], [], []
+    for r, L in enumerate(locs):
+        dg = rb.DGSEM(grid=L.grid, **kw)
+        dg.set_active_elements(L.num_local)
+        s = L.local_state(q0)
+        s[:, :, L.num_local:] = 0.0
+        q = rb.GridArray.from_numpy(s)
+        dgs.append(dg)
+        halos.append(D.HaloExchange(D.node_comm_pattern(g, parts, r, law.ns), device="cuda"))
+        cur.append(q)
+        oth.append(q.similar())
+        dqs.append(q.similar())
+    for step in range(nsteps):
+        for a, b in zip(rb.LSRK144_RKA, rb.LSRK144_RKB):
+            for r in range(nranks):
+                halos[r].pack(cur[r].data.view(-1))
+                dgs[r].lsrk_stage_range(cur[r], oth[r], dqs[r], a, b, 0, locs[r].num_interior, step * dt, dt)
+            for r in range(nranks):
+                p = halos[r].pattern
+                for peer, (lo, hi) in zip(p.recvranks, p.recvrankindices):
+                    pp = halos[peer].pattern
+                    sa, sb = pp.sendrankindices[pp.sendranks.index(r)]
+                    halos[r].recvbuf[lo:hi].copy_(halos[peer].sendbuf[sa:sb])
+                halos[r].unpack(cur[r].data.view(-1))
+            for r in range(nranks):
+                L = locs[r]
+                dgs[r].lsrk_stage_range(cur[r], oth[r], dqs[r], a, b, L.num_interior, L.num_local, step * dt, dt)
+            cur, oth = oth, cur
+    torch.cuda.synchronize()
+    for r, L in enumerate(locs):
+        got = cur[r].numpy()[:, :, : L.num_local]
+        want = q_ref[:, :, L.global_elements[: L.num_local]]
+        assert np.array_equal(got, want), (r, np.abs(got - want).max())
