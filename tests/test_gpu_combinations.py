@@ -3,7 +3,8 @@ order, grid size, periodicity, warping, scheme, surface flux, direction subset a
 boundary conditions, drawn together so that the options are exercised jointly (each is
 also tested on its own elsewhere).
 
-Tolerance: FP64 tendency and two LSRK(5,4) steps 1e-12 relative per field (max norm).
+Tolerance: FP64 tendency and two LSRK(5,4) steps 1e-12 relative per field (max norm);
+FP32-bulk tendency 5e-5.
 """
 
 import numpy as np
@@ -90,3 +91,40 @@ def test_combination(rb, cuda_ok, seed):
     dg.sync_status()
     for s in range(law.ns):
         assert rel_err(qg.numpy()[:, s], qo[:, s]) <= 1e-12, (label, "steps", s)
+
+
+@pytest.mark.parametrize("seed", range(40, 60))
+def test_combination_fp32_bulk(rb, cuda_ok, seed):
+    """The same draws in FP32 bulk (Rusanov or central surface flux: the entropy-family
+    surface fluxes are FP64 only): tendency within 5e-5 of the oracle."""
+    dim, nq, K, per, scheme, warp, sflux, dirs, bc = _draw(seed)
+    if sflux not in ("rusanov", "central"):
+        sflux = "rusanov"
+    og = O.Grid(dim, nq, K, [0.0] * dim, [3.0] * dim, per, warp, 0.1 if warp == O.WARP_SINE else 0.0)
+    g = wrap_oracle_grid(og)
+    adv = [1.0, 0.5, 0.25][:dim]
+    law, form = product_scheme(rb, scheme, dim, adv)
+    sf = rb.RusanovFlux() if sflux == "rusanov" else rb.CentralFlux()
+    olaw = oracle_law(scheme, dim, adv)
+    olaw.c.surface_flux = O.FLUX_RUSANOV if sflux == "rusanov" else O.FLUX_CENTRAL
+    q = initial_state(og, olaw, scheme, seed=seed, amp=0.01)
+    conds = {}
+    for tag, kind in bc.items():
+        if kind == "wall":
+            conds[tag] = "wall"
+            og.set_boundary_condition(tag, 2)
+        else:
+            state = q[:, :, 0].mean(axis=0)
+            conds[tag] = state
+            og.set_boundary_condition(tag, 1, state)
+    if dirs is not None:
+        og.set_directions(dirs)
+    dg = rb.DGSEM(law=law, grid=g, volume_form=form, surface_numericalflux=sf, directions=dirs,
+                  boundary_conditions=conds, precision="fp32_bulk")
+    ref = og.tendency(olaw, q)
+    qg = rb.GridArray.from_numpy(q)
+    dqg = rb.GridArray.from_numpy(np.zeros_like(q))
+    dg(dqg, qg, 0.0, increment=False)
+    dg.sync_status()
+    for s in range(law.ns):
+        assert rel_err(dqg.numpy()[:, s], ref[:, s]) <= 5e-5, ((dim, nq, K, per, scheme, warp, sflux, dirs, bc), s)
