@@ -26,7 +26,14 @@
 
 #include "pipelined_kernel.cuh"
 
+// unroll factor of the curved kernels' pair loops over partners
+#ifndef RB200_CURVED_UNROLL
+#define RB200_CURVED_UNROLL 2
+#endif
+
 namespace rb200 {
+
+constexpr int kCurvedUnroll = RB200_CURVED_UNROLL;
 
 struct PipeCurvedArgs {
     const double* q_in;
@@ -203,7 +210,7 @@ __global__ void __launch_bounds__(256, 2) pipelined_curved_kernel(const __grid_c
             ac[3] += f1 * ub2 + pbar * G[2];
             ac[4] += un * (rb * eb + pbar);
         };
-#pragma unroll 2
+#pragma unroll kCurvedUnroll
         for (int a = 0; a < NQ; ++a) {
             const float Dax = sm.D[a][ii], Dxa = sm.D[ii][a];
             const float Day = sm.D[a][jj], Dya = sm.D[jj][a];

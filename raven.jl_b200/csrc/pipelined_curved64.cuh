@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(256, 2) pipelined_curved64_kernel(const __grid
                 lo[h][2] = sm.lgb[dir][PAD(n)];
             }
             const int id = dir == 0 ? ii : jj;
-#pragma unroll 2
+#pragma unroll kCurvedUnroll
             for (int a = 0; a < NQ; ++a) {
                 const double Dai = sm.D[a][id], Dia = sm.D[id][a];
 #pragma unroll
@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(256, 2) pipelined_curved64_kernel(const __grid
                 lo[h][1] = la.y;
                 lo[h][2] = sm.lgb[2][PAD(n)];
             }
-#pragma unroll 2
+#pragma unroll kCurvedUnroll
             for (int a = 0; a < NQ; ++a) {
                 const int nz = ii + 8 * (jj + 8 * a);
                 double pv[NAUX];
