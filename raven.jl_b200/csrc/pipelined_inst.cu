@@ -8,13 +8,9 @@
 
 namespace rb200 {
 
-#ifndef RB200_PIPE_NPT
-#define RB200_PIPE_NPT 2  // nodes per thread of the pipelined kernel
-#endif
-constexpr int kNPT = RB200_PIPE_NPT;
-
 template <int COMBO, typename T, bool BATCH, int Q>
 static cudaError_t launch_p(const PipeArgs& a, const PipeBatch& b, int grid, cudaStream_t s) {
+    constexpr int kNPT = pipe_npt<T, Q>();
     auto kern = pipelined_stage_kernel<COMBO, T, kNPT, BATCH, Q>;
     static std::atomic<uint64_t> configured{0};
     cudaError_t err = ensure_smem_limit(kern, (int)sizeof(pipe::Smem<T, Q>), configured);
@@ -78,6 +74,7 @@ cudaError_t launch_pipelined_batch(int nq, int combo, int fp32, const PipeArgs& 
 
 template <int COMBO, typename T, bool BATCH, int Q>
 static int occupancy_p() {
+    constexpr int kNPT = pipe_npt<T, Q>();
     auto kern = pipelined_stage_kernel<COMBO, T, kNPT, BATCH, Q>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(pipe::Smem<T, Q>)) !=
         cudaSuccess)

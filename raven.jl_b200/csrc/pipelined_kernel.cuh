@@ -1,8 +1,8 @@
 // Persistent, TMA-pipelined stage kernel for 3-D hexahedra on unwarped bricks (Nq = 4, 6
 // or 8), flux-differencing volume forms (Kennedy-Gruber, entropy conservative).
 //
-// Each CTA owns a strided set of elements (e = blockIdx.x + k*gridDim.x); two CTAs share
-// an SM in FP64, three in FP32 bulk.
+// Each CTA owns a strided set of elements (e = blockIdx.x + k*gridDim.x); three CTAs
+// share an SM (Nq = 8).
 // * The element's state q arrives by one 1-D bulk copy (cp.async.bulk, completion on an
 //   mbarrier) into shared memory.  It is only needed to build the per-node partner
 //   values, so right after the first barrier the copy of the CTA's next element is
@@ -13,8 +13,9 @@
 // * The element's own old q (and the FP64 register) are read with coalesced loads at
 //   the end, so that they hold no registers across the flux arithmetic.
 //
-// A thread owns NPT nodes of the element (same i, j), so the eight z-partners of its
-// line are loaded once for all of them.  The metric of an unwarped brick is folded into
+// A thread owns two nodes of one z line (their eight z-partners are loaded once for
+// both), or in FP64 at Nq = 8 four nodes on a 2 x 2 block of y and z lines (each y- and
+// z-partner is loaded once for two of them; a quarter of the partner loads saved).  The metric of an unwarped brick is folded into
 // a per-element table S_dir[a][id] = drdx_dir * (D[a,id] w_a / w_id - D[id,a]), which
 // equals MJI_id * (D[a,id] l_g[a] - D[id,a] l_g[id]) of esvolumeterm_dir!
 // (src/balancelaws/dgsem.jl:576-600); S_dir[id][id] = 0, so the z pair of a node with
@@ -279,9 +280,9 @@ __device__ __forceinline__ void fetch_part(const ElemRef& r, int t, double (&geo
 
 }  // namespace pipe
 
-// CTAs per SM the register allocation is sized for.  Nq = 8: 2 for FP64 (128 registers a
-// thread), 3 for FP32 bulk (80).  Smaller elements have fewer threads a CTA, so more CTAs
-// share an SM at about the same registers a thread.
+// CTAs per SM the register allocation is sized for.  Nq = 8: 3 for FP64 (128 threads of
+// 168 registers), 3 for FP32 bulk (256 threads of 80).  Smaller elements have fewer
+// threads a CTA, so more CTAs share an SM at about the same registers a thread.
 #ifndef RB200_PIPE_MIN6
 #define RB200_PIPE_MIN6 4, 6
 #endif
@@ -289,7 +290,7 @@ __device__ __forceinline__ void fetch_part(const ElemRef& r, int t, double (&geo
 #define RB200_PIPE_MIN4 14, 20
 #endif
 #ifndef RB200_PIPE_MIN8_FP64
-#define RB200_PIPE_MIN8_FP64 2
+#define RB200_PIPE_MIN8_FP64 3
 #endif
 #ifndef RB200_PIPE_MIN8_FP32
 #define RB200_PIPE_MIN8_FP32 3
@@ -304,20 +305,38 @@ constexpr int pipe_min_ctas() {
     return Q == 8 ? m8[sizeof(T) == 4] : Q == 6 ? m6[sizeof(T) == 4] : m4[sizeof(T) == 4];
 }
 
-// NPT nodes per thread: thread t owns nodes t + (Np/NPT)*h, h < NPT, which share i, j
-// (k = k0 + (Nq/NPT)*h), so their z-partners are loaded once.
+// Nodes per thread of the kernel: 4 (the 2 x 2 (y, z) block) in FP64 at Nq = 8, else 2.
+template <typename T, int Q>
+constexpr int pipe_npt() {
+    return (sizeof(T) == 8 && Q == 8) ? 4 : 2;
+}
+
+// NPT nodes per thread, with i = t mod Nq:
+// * NPT = 2: (i, j, k0) and (i, j, k0 + Nq/2), j = (t / Nq) mod Nq, k0 = t / Nq^2 — one z
+//   line, so their z-partners are loaded once;
+// * NPT = 4: (i, j0 + Nq/2 hj, k0 + Nq/2 hk), hj, hk in {0, 1}, j0 = (t / Nq) mod Nq/2,
+//   k0 = t / (Nq^2/2) — two y lines and two z lines, so each y- and z-partner serves two
+//   nodes.  A quarter-warp still spans an x line (x partners: one address a quarter), and
+//   k0 is the same across a warp (the z pair of a node with itself is skipped uniformly).
 template <int COMBO, typename T, int NPT, bool BATCH, int Q = 8>
 __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q>()))
     pipelined_stage_kernel(const __grid_constant__ PipeArgs A, const __grid_constant__ PipeBatch B) {
     using namespace pipe;
     using G = Geo<Q>;
     constexpr int NQ = Q, NP = G::NP, NFP = G::NFP, NSLOT = G::NSLOT;
-    static_assert(Q % NPT == 0, "a thread's nodes share (i, j)");
-    constexpr int NT = NP / NPT, KS = Q / NPT;
+    static_assert(NPT == 2 || NPT == 4, "a z pair or a 2 x 2 (y, z) block");
+    constexpr bool YZ = NPT == 4;
+    constexpr int NT = NP / NPT, H = Q / 2;
     extern __shared__ __align__(128) unsigned char pipe_smem_raw[];
     Smem<T, Q>& sm = *reinterpret_cast<Smem<T, Q>*>(pipe_smem_raw);
     const int t = threadIdx.x;
-    const int ii = t % Q, jj = (t / Q) % Q, k0 = t / (Q * Q);
+    const int ii = t % Q;
+    const int jj = YZ ? (t / Q) % H : (t / Q) % Q;
+    const int k0 = YZ ? t / (Q * H) : t / (Q * Q);
+    // coordinates and index of the thread's node h
+    auto jj_of = [&](int h) { return YZ ? jj + H * (h & 1) : jj; };
+    auto kk_of = [&](int h) { return YZ ? k0 + H * (h >> 1) : k0 + H * h; };
+    auto node_of = [&](int h) { return YZ ? ii + Q * (jj_of(h) + Q * kk_of(h)) : t + NT * h; };
     const bool stage = A.mode >= MODE_STAGE;
     const bool dq_is_f32 = stage && sizeof(T) == 4;
     constexpr bool kStageDq = sizeof(T) == 4;
@@ -375,7 +394,7 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q>()))
         T own[NPT][NAUX];
 #pragma unroll
         for (int h = 0; h < NPT; ++h) {
-            const int n = t + NT * h;
+            const int n = node_of(h);
             const T rho = (T)sm.q[0][n];
             const T rinv = T(1) / rho;
             const T m0 = (T)sm.q[1][n], m1 = (T)sm.q[2][n], m2 = (T)sm.q[3][n];
@@ -490,32 +509,62 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q>()))
         constexpr int kUnrA = RB200_PIPE_UNROLL_A < NQ ? RB200_PIPE_UNROLL_A : NQ;
 #pragma unroll kUnrA
         for (int a = 0; a < NQ; ++a) {
-            const T sx = sm.S[0][a][ii], sy = sm.S[1][a][jj];
+            const T sx = sm.S[0][a][ii];
+            if constexpr (YZ) {
 #pragma unroll
-            for (int h = 0; h < NPT; ++h) {
-                const int kk = k0 + KS * h;
+                for (int h = 0; h < NPT; ++h) {
+                    T pv[NAUX];
+                    load_aux(pv, a + Q * (jj_of(h) + Q * kk_of(h)));
+                    pair(acc[h], accu[h], own[h], pv, sx, 0);
+                }
+#pragma unroll
+                for (int hk = 0; hk < 2; ++hk) {  // y-partner (ii, a, kk): nodes 2hk, 2hk+1
+                    T pv[NAUX];
+                    load_aux(pv, ii + Q * (a + Q * kk_of(2 * hk)));
+#pragma unroll
+                    for (int hj = 0; hj < 2; ++hj) {
+                        const int h = 2 * hk + hj;
+                        pair(acc[h], accu[h], own[h], pv, sm.S[1][a][jj_of(h)], 1);
+                    }
+                }
+#pragma unroll
+                for (int hj = 0; hj < 2; ++hj) {  // z-partner (ii, jj, a): nodes hj, hj+2
+                    T pv[NAUX];
+                    load_aux(pv, ii + Q * (jj_of(hj) + Q * a));
+#pragma unroll
+                    for (int hk = 0; hk < 2; ++hk) {
+                        const int h = 2 * hk + hj;
+                        if (a != kk_of(h)) pair(acc[h], accu[h], own[h], pv, sm.S[2][a][kk_of(h)], 2);  // S_aa = 0
+                    }
+                }
+            } else {
+                const T sy = sm.S[1][a][jj];
+#pragma unroll
+                for (int h = 0; h < NPT; ++h) {
+                    const int kk = kk_of(h);
+                    T pv[NAUX];
+                    load_aux(pv, a + Q * (jj + Q * kk));
+                    pair(acc[h], accu[h], own[h], pv, sx, 0);
+                    load_aux(pv, ii + Q * (a + Q * kk));
+                    pair(acc[h], accu[h], own[h], pv, sy, 1);
+                }
                 T pv[NAUX];
-                load_aux(pv, a + Q * (jj + Q * kk));
-                pair(acc[h], accu[h], own[h], pv, sx, 0);
-                load_aux(pv, ii + Q * (a + Q * kk));
-                pair(acc[h], accu[h], own[h], pv, sy, 1);
-            }
-            T pv[NAUX];
-            load_aux(pv, ii + Q * (jj + Q * a));
+                load_aux(pv, ii + Q * (jj + Q * a));
 #pragma unroll
-            for (int h = 0; h < NPT; ++h)
-                if (a != k0 + KS * h) pair(acc[h], accu[h], own[h], pv, sm.S[2][a][k0 + KS * h], 2);  // S_aa = 0
+                for (int h = 0; h < NPT; ++h)
+                    if (a != kk_of(h)) pair(acc[h], accu[h], own[h], pv, sm.S[2][a][kk_of(h)], 2);  // S_aa = 0
+            }
         }
 
         if constexpr (COMBO == EUL_KG) {
 #pragma unroll
             for (int h = 0; h < NPT; ++h) {
-                const int kk = k0 + KS * h;
+                const int kk = kk_of(h), jh = jj_of(h);
                 if constexpr (sizeof(T) == 4) {
                     // FP32: e/2 and p/2 of the own node again from shared memory: they are not
                     // used in the pair loop and would hold registers across it (80 a thread)
                     T ov[NAUX];
-                    load_aux(ov, t + NT * h);
+                    load_aux(ov, node_of(h));
                     own[h][4] = ov[4];
                     own[h][5] = ov[5];
                 }
@@ -524,7 +573,7 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q>()))
                 acc[h][2] = fma(own[h][2], acc[h][0], acc[h][2]);
                 acc[h][3] = fma(own[h][3], acc[h][0], acc[h][3]);
                 acc[h][1] = fma(o5, sm.rs[0][ii], acc[h][1]);
-                acc[h][2] = fma(o5, sm.rs[1][jj], acc[h][2]);
+                acc[h][2] = fma(o5, sm.rs[1][jh], acc[h][2]);
                 acc[h][3] = fma(o5, sm.rs[2][kk], acc[h][3]);
                 acc[h][4] = fma(own[h][4], acc[h][0], fma(o5, accu[h], acc[h][4]));
             }
@@ -700,7 +749,7 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q>()))
         }
         __syncthreads();  // #2: face-slot contributions ready
         // ---- own old state and register, read now so that the loads overlap the faces
-        const size_t g0 = (size_t)e * NS * NP + t;
+        const size_t g0 = (size_t)e * NS * NP;
         double* const qout_e = BATCH ? sm.ref[buf].q_out : A.q_out;
         const double rkb_dt = BATCH ? sm.ref[buf].rkb_dt : A.rkb_dt;
         double qold[NPT][NS];
@@ -709,10 +758,10 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q>()))
         for (int h = 0; h < NPT; ++h)
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
-                const size_t g = g0 + NT * h + s * NP;
+                const size_t g = g0 + node_of(h) + s * NP;
                 qold[h][s] = stage ? __ldg(qin_e + g) : 0.0;
                 if (kStageDq && A.mode == MODE_STAGE)
-                    dqold[h][s] = sm.dqs[kStageDq ? s : 0][kStageDq ? t + NT * h : 0];
+                    dqold[h][s] = sm.dqs[kStageDq ? s : 0][kStageDq ? node_of(h) : 0];
                 else if (A.mode == MODE_STAGE || A.mode == MODE_TENDENCY_INC)
                     dqold[h][s] = dq_is_f32 ? (T)__ldg(reinterpret_cast<const float*>(dq_e) + g)
                                             : (T)__ldg(reinterpret_cast<const double*>(dq_e) + g);
@@ -723,14 +772,14 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q>()))
         // ---- own nodes: dq = rka*dq + volume - faces (x, y, z order); q_out = q + rkb*dt*dq
 #pragma unroll
         for (int h = 0; h < NPT; ++h) {
-            const int kk = k0 + KS * h;
+            const int kk = kk_of(h), jn = jj_of(h);
             int slots[3] = {-1, -1, -1};
-            if (ii == 0) slots[0] = jj + Q * kk;
-            else if (ii == NQ - 1) slots[0] = NFP + jj + Q * kk;
-            if (jj == 0) slots[1] = 2 * NFP + ii + Q * kk;
-            else if (jj == NQ - 1) slots[1] = 3 * NFP + ii + Q * kk;
-            if (kk == 0) slots[2] = 4 * NFP + ii + Q * jj;
-            else if (kk == NQ - 1) slots[2] = 5 * NFP + ii + Q * jj;
+            if (ii == 0) slots[0] = jn + Q * kk;
+            else if (ii == NQ - 1) slots[0] = NFP + jn + Q * kk;
+            if (jn == 0) slots[1] = 2 * NFP + ii + Q * kk;
+            else if (jn == NQ - 1) slots[1] = 3 * NFP + ii + Q * kk;
+            if (kk == 0) slots[2] = 4 * NFP + ii + Q * jn;
+            else if (kk == NQ - 1) slots[2] = 5 * NFP + ii + Q * jn;
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
                 T v = acc[h][s];
@@ -739,7 +788,7 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q>()))
 #pragma unroll
                 for (int d = 0; d < 3; ++d)
                     if (slots[d] >= 0) v = v - (T)sm.slot[s][slots[d]];
-                const size_t g = g0 + NT * h + s * NP;
+                const size_t g = g0 + node_of(h) + s * NP;
                 if (stage) {
                     if (dq_is_f32) reinterpret_cast<float*>(dq_e)[g] = (float)v;
                     else reinterpret_cast<double*>(dq_e)[g] = (double)v;

@@ -21,7 +21,7 @@ SCHEMES = ["eul_kg", "eul_ec"]
 
 
 # Nq and a grid with more elements than the kernel has CTAs at that Nq
-NQS = [(8, (8, 8, 7)), (6, (12, 12, 10)), (4, (20, 20, 16))]
+NQS = [(8, (9, 8, 7)), (6, (12, 12, 10)), (4, (20, 20, 16))]
 
 
 def _build(rb, scheme, K=(8, 8, 7), per=(1, 1, 0), precision="fp64", nq=8):
