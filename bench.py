@@ -282,10 +282,19 @@ def stage_bytes_per_launch(w, nodes, ns):
     return per_step / 5.0
 
 
+def timed_launches(dg, steps):
+    """Kernels of ours launched by one lsrk54_steps call of `steps` steps: one for the
+    cluster step kernel, else the stage (and mortar) kernels of each step."""
+    return 1 if getattr(dg, "cluster_ctas", 0) > 0 else int(dg.info[6]) * steps
+
+
 def kernel_name(w, dg):
     """The stage kernel the handle launches for this workload."""
     if w.get("serve"):
         return "batched_stage_kernel (all running solves of a class per launch)"
+    if getattr(dg, "cluster_ctas", 0) > 0:
+        return (f"cluster_adv_steps_kernel (one thread-block cluster of {dg.cluster_ctas} CTAs runs every stage "
+                "of the timed steps in one launch)")
     if dg.pipelined_ctas > 0:
         if dg.geometry == "curved":
             if w["precision"] == "fp64":
@@ -438,7 +447,7 @@ def other_configs_leg(rb, args, local, stream, barrier, dist, world):
         ms = timed_steps(dg, q, dq, args.warmup * dt, dt, n, stream, barrier, dist)
         sampler.stop()
         nodes, ns = grid.np * grid.E, law.ns
-        launches = int(dg.info[6]) * n  # stage kernels (and mortar kernels) per step
+        launches = timed_launches(dg, n)
         rec = {
             "label": label,
             "config": config_json(name, w, grid),
@@ -1042,7 +1051,7 @@ def main(argv=None):
     ms = timed_steps(dg, q, dq, args.warmup * dt, dt, args.steps, stream, barrier, dist)
     sampler.stop()
     value = world * nodes * ns * 5 * args.steps / (ms / 1e3)
-    launches = int(dg.info[6]) * args.steps  # stage kernels (and mortar kernels) per step
+    launches = timed_launches(dg, args.steps)
 
     # the FP32-bulk form of the same workload, timed the same way in the same process
     fp32_leg = None

@@ -304,7 +304,11 @@ rb200_status rb200_probe_fp64_rate(int64_t iters, double* tflops_out, void* stre
  * (0 affine brick, 1 curved), [5]=precision, [6]=kernel launches per LSRK step,
  * [7]=algorithmic HBM bytes per node per stage, [8]=CTAs of the pipelined kernel of the
  * handle's geometry (brick, or the FP32-bulk curved one; 0 when the configuration does
- * not use one). */
+ * not use one), [9]=CTAs of the cluster step kernel (small weak-form advection grids on
+ * unwarped bricks: one launch of one thread-block cluster runs all stages of all steps
+ * of an rb200_lsrk54_step / rb200_lsrk144_step / rb200_lsrk_step call, and [6] does not
+ * apply to those calls; 0 when the steps run as stage launches).  n <= 10 values are
+ * written. */
 rb200_status rb200_get_info(const rb200_handle* h, int64_t* info, int32_t n);
 
 /* Weighted sums without any device allocation (no counterpart in the reference).

@@ -422,11 +422,18 @@ class DGSEM:
                 L.rb200_destroy(h)
                 self._h = None
                 raise
-        info = (ctypes.c_int64 * 9)()
-        L.rb200_get_info(h, info, 9)
+        self._read_info()
+
+    def _read_info(self):
+        """rb200_get_info: `info` (10 values), `geometry`, `pipelined_ctas` and
+        `cluster_ctas` (CTAs of the one-launch cluster step kernel of small weak-form
+        advection bricks; 0 when the steps run as stage launches)."""
+        info = (ctypes.c_int64 * 10)()
+        _lib.check(_lib.lib().rb200_get_info(self._h, info, 10), self._h)
         self.info = list(info)
         self.geometry = "affine" if info[4] == 0 else "curved"
         self.pipelined_ctas = int(info[8])
+        self.cluster_ctas = int(info[9])
 
     def set_boundary_condition(self, tag, condition):
         """The exterior state of the faces with boundary code `tag` (1..8): a sequence of
@@ -445,15 +452,12 @@ class DGSEM:
         _lib.check(_lib.lib().rb200_set_boundary_condition(self._h, int(tag), kind,
                                                            None if st is None else st.ctypes.data_as(ctypes.c_void_p)),
                    self._h)
-        self.info = None  # the kernel choice may have changed; re-read below
-        info = (ctypes.c_int64 * 9)()
-        _lib.lib().rb200_get_info(self._h, info, 9)
-        self.info = list(info)
-        self.pipelined_ctas = int(info[8])
+        self._read_info()  # the kernel choice may have changed
 
     def set_kernel_path(self, path):
         """'auto' (pipelined kernel where eligible) or 'generic' (generic stage kernel only)."""
         _lib.check(_lib.lib().rb200_set_kernel_path(self._h, {"auto": 0, "generic": 1}[path]), self._h)
+        self._read_info()
 
     def sync_status(self):
         """Synchronizes and raises RB200Error(TIMEOUT) if a kernel gave up a bounded wait."""

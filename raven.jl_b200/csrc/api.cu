@@ -318,6 +318,22 @@ rb200_status enqueue_steps(rb200_handle* h, const Scheme& sc, double* q, void* d
     return RB200_OK;
 }
 
+// CTAs of the cluster step kernel for this handle, or 0 where the steps run as stage
+// launches: weak-form advection on an unwarped brick without mortars whose stages would
+// run the generic stage kernel (no pipelined kernel for its Nq), the automatic kernel
+// choice, and a grid whose elements kClusterCtas CTAs of kClusterNodes nodes hold.  The
+// cluster kernel then computes what the stage launches compute, bit for bit.
+int cluster_ctas(const rb200_handle* h) {
+    // (every neighbour an element of the cluster: no ghost elements beyond E_active)
+    if (h->kernel_path != 0 || h->combo != ADV_WEAK || h->geom != GEOM_AFFINE || h->nmortars > 0 ||
+        h->pipe_grid > 0 || h->E_active != h->E)
+        return 0;
+    const int64_t epb = cluster_elements_per_cta(h->np);
+    const int64_t groups = (h->E_active + epb - 1) / epb;
+    if (groups < 1 || groups > kClusterCtas) return 0;
+    return (int)groups;
+}
+
 rb200_status run_steps(rb200_handle* h, const Scheme& sc, double* q, void* dq, double dt, int32_t nsteps,
                        cudaStream_t st) {
     const size_t nstate = (size_t)h->np * h->ns * h->E;
@@ -329,7 +345,28 @@ rb200_status run_steps(rb200_handle* h, const Scheme& sc, double* q, void* dq, d
     double* cur = q;
     rb200_status rs;
     int32_t done = 0;
-    if (h->use_graphs && nsteps >= 4) {
+    const int cctas = cluster_ctas(h);
+    if (cctas > 0 && nsteps > 0 && sc.stages <= kClusterStages) {
+        // a small grid: all stages of all steps in one launch of one cluster
+        ClusterStepsArgs c;
+        std::memset(&c, 0, sizeof(c));
+        c.a = base_args(h);
+        c.a.dq = dq;
+        c.q = q;
+        c.nsteps = nsteps;
+        c.nstages = sc.stages;
+        for (int s = 0; s < sc.stages; ++s) {
+            c.rka[s] = sc.rka[s];
+            c.rkb_dt[s] = sc.rkb[s] * dt;
+        }
+        cudaError_t e = launch_cluster_steps(h->dim, h->nq, h->prec == RB200_PRECISION_FP32_BULK ? 1 : 0, c, cctas, st);
+        if (e == cudaSuccess) {
+            done = nsteps;  // the result is in q
+        } else if (e != cudaErrorNotSupported) {  // not supported: stage launches below
+            return cuda_fail(h, e, "cluster step kernel launch");
+        }
+    }
+    if (done < nsteps && h->use_graphs && nsteps >= 4) {
         // two steps (an even number of stages, so the state is back in q) run eagerly:
         // kernel attributes get configured outside the capture
         if ((rs = enqueue_steps(h, sc, q, dq, dt, 2, st, &cur)) != RB200_OK) return rs;
@@ -1329,9 +1366,10 @@ rb200_status rb200_get_info(const rb200_handle* h, int64_t* info, int32_t n) {
     int64_t per_node = h->ns * (2 * bytes_q + 2 * bytes_dq);
     if (h->geom == GEOM_CURVED)
         per_node += (h->dim * h->dim + 1) * 8 + (int64_t)h->nf * h->nfp * (h->dim + 1) * 8 / h->np;
-    const int64_t v[9] = {h->dim, h->nq, h->ns, h->E, h->geom, h->prec, h->nmortars > 0 ? 10 : 5, per_node,
-                          h->dir_mask || h->has_bc ? 0 : (h->geom == GEOM_CURVED ? h->pipe_curved_grid : h->pipe_grid)};
-    for (int i = 0; i < n && i < 9; ++i) info[i] = v[i];
+    const int64_t v[10] = {h->dim, h->nq, h->ns, h->E, h->geom, h->prec, h->nmortars > 0 ? 10 : 5, per_node,
+                           h->dir_mask || h->has_bc ? 0 : (h->geom == GEOM_CURVED ? h->pipe_curved_grid : h->pipe_grid),
+                           cluster_ctas(h)};
+    for (int i = 0; i < n && i < 10; ++i) info[i] = v[i];
     return RB200_OK;
 }
 

@@ -88,6 +88,34 @@ constexpr int kMaxBcTags = 8;
 constexpr int kBcBase = 16;
 enum { BC_DEFAULT = 0, BC_PRESCRIBED = 1, BC_WALL = 2 };
 
+// Small grids: all stages of `nsteps` LSRK steps in one launch of one thread-block
+// cluster (weak-form advection on unwarped bricks, stage_kernel.cuh).  The state q is
+// read at the start and written at the end; stage s of a step has rka[s] and rkb_dt[s];
+// the LSRK register is a.dq.
+// CTAs of the cluster at most: 16, the largest size B200 runs (above the portable 8, with
+// the kernel's opt-in), and nodes (threads) of a CTA at most.  On the 16^2, N=4 grid 13
+// CTAs of 500 threads take 5.3 us a step against 7.7 us for 7 CTAs of 1000 threads.
+#ifndef RB200_CLUSTER_CTAS
+#define RB200_CLUSTER_CTAS 16
+#endif
+#ifndef RB200_CLUSTER_NODES
+#define RB200_CLUSTER_NODES 512
+#endif
+constexpr int kClusterCtas = RB200_CLUSTER_CTAS;
+constexpr int kClusterNodes = RB200_CLUSTER_NODES;
+constexpr int kClusterStages = 32;   // stages of a step at most
+struct ClusterStepsArgs {
+    StageArgs a;                     // q_in, q_out, mode, rka and rkb_dt unused
+    double* q;
+    int32_t nsteps;
+    int32_t nstages;
+    double rka[kClusterStages];
+    double rkb_dt[kClusterStages];
+};
+// Elements per CTA of the cluster kernel: up to kClusterNodes nodes a CTA.
+inline int64_t cluster_elements_per_cta(int64_t np) { return np >= kClusterNodes ? 1 : kClusterNodes / np; }
+cudaError_t launch_cluster_steps(int dim, int nq, int fp32, const ClusterStepsArgs& c, int ctas, cudaStream_t s);
+
 // Mortars of an adapted grid (mortar.cu).
 struct MortarArgs {
     const double* q;          // q_in (Np, Ns, E)

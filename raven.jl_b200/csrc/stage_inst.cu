@@ -14,6 +14,7 @@
 #define RB_CAT(a, b, c, d) RB_CAT2(a, b, c, d)
 #define RB_LAUNCH_NAME RB_CAT(launch_stage_d, RB_DIM, _q, RB_NQ)
 #define RB_SMEM_NAME RB_CAT(smem_stage_d, RB_DIM, _q, RB_NQ)
+#define RB_CLUSTER_NAME RB_CAT(launch_cluster_d, RB_DIM, _q, RB_NQ)
 
 namespace rb200 {
 
@@ -53,6 +54,10 @@ static size_t smem_c(int geom, int fp32) {
                     : PersistentCfg<RB_DIM, RB_NQ, COMBO, GEOM_AFFINE, double>::smem;
     return fp32 ? PersistentCfg<RB_DIM, RB_NQ, COMBO, GEOM_CURVED, float>::smem
                 : PersistentCfg<RB_DIM, RB_NQ, COMBO, GEOM_CURVED, double>::smem;
+}
+
+cudaError_t RB_CLUSTER_NAME(int fp32, const ClusterStepsArgs& c, int ctas, cudaStream_t s) {
+    return fp32 ? launch_cluster_adv<RB_DIM, RB_NQ, float>(c, ctas, s) : launch_cluster_adv<RB_DIM, RB_NQ, double>(c, ctas, s);
 }
 
 size_t RB_SMEM_NAME(int combo, int geom, int fp32) {

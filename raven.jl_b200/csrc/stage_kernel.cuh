@@ -785,4 +785,187 @@ cudaError_t launch_one(const StageArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+// Small grids: every stage of every step of an LSRK call in one launch of one
+// thread-block cluster (weak-form advection on unwarped bricks).  On a grid that one pass
+// of a few CTAs covers (a 16^2, N=4 grid has 6400 nodes) a stage launch is mostly launch
+// latency and dependent trips to L2.  Here CTA r of the cluster owns elements
+// e_begin + r*EPB .. +EPB-1 (one node a thread, up to kClusterNodes a CTA) for the whole
+// call: a thread keeps its node's state and LSRK register in registers, the CTA keeps its
+// elements' state of the current stage in shared memory (two buffers by stage parity),
+// the volume term reads the element's own nodes there, and the surface term reads the
+// neighbour's trace from the shared memory of the CTA that owns it (distributed shared
+// memory).  One hardware cluster barrier a stage (arrive.release / wait.acquire) orders
+// a stage's shared-memory writes before the next stage's reads.  Global memory is read
+// at the start and written at the end only.  The arithmetic per node is that of
+// stage_element_adv_brick, expression for expression, so the results are bit for bit
+// those of the stage launches.
+template <int DIM, int NQ>
+struct ClusterShape {
+    static constexpr int NP = IPow<NQ, DIM>::v;
+    static constexpr int EPB = NP >= kClusterNodes ? 1 : kClusterNodes / NP;
+    using S = Shape<DIM, NQ, EPB>;
+    static constexpr size_t smem = (size_t)(2 * EPB * NP + NQ * NQ) * sizeof(double);
+};
+
+__device__ __forceinline__ void cluster_barrier() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// The address of `p` (this CTA's shared memory) in the shared memory of cluster CTA `rank`.
+template <typename T>
+__device__ __forceinline__ const T* cluster_peer(const T* p, unsigned rank) {
+    uint64_t out;
+    asm("mapa.u64 %0, %1, %2;" : "=l"(out) : "l"(reinterpret_cast<uint64_t>(p)), "r"(rank));
+    return reinterpret_cast<const T*>(out);
+}
+
+template <int DIM, int NQ, typename T>
+__global__ void __launch_bounds__(ClusterShape<DIM, NQ>::S::THREADS, 1)
+    cluster_adv_steps_kernel(const __grid_constant__ ClusterStepsArgs C) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using CS = ClusterShape<DIM, NQ>;
+    constexpr int NP = CS::NP, EPB = CS::EPB, NF = 2 * DIM, TH = CS::S::THREADS;
+    T* sq = reinterpret_cast<T*>(smem_raw);  // [2][EPB * NP]: the CTA's elements, by stage parity
+    T* sW = sq + 2 * EPB * NP;               // W[a + NQ i]
+    const StageArgs& A = C.a;
+    const int tid = threadIdx.x;
+    const int el = tid / NP;
+    const int n = tid - el * NP;
+    const int64_t e = A.e_begin + (int64_t)blockIdx.x * EPB + el;
+    const bool active = e < A.E;
+    int id[3];
+    id[0] = n % NQ;
+    id[1] = DIM > 1 ? (n / NQ) % NQ : 0;
+    id[2] = DIM > 2 ? n / (NQ * NQ) : 0;
+    for (int i = tid; i < NQ * NQ; i += TH) {
+        const int a = i % NQ, ii = i / NQ;
+        sW[i] = (T)(A.D[a + NQ * ii] * (A.w[a] / A.w[ii]));
+    }
+    const int dmask = A.dir_mask ? A.dir_mask : 7;
+    const size_t node0 = (size_t)e * NP + n;
+    double qd = 0.0, drdx[3] = {0.0, 0.0, 0.0};
+    T dqv = T(0);
+    int32_t nb[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) nb[f] = -1;
+    if (active) {
+        qd = C.q[node0];
+        if (C.rka[0] != 0.0) {  // a table whose first stage reads the register
+            if (sizeof(T) == 4) dqv = (T) reinterpret_cast<const float*>(A.dq)[node0];
+            else dqv = (T) reinterpret_cast<const double*>(A.dq)[node0];
+        }
+        const double* eg = A.elem_geo + 4 * e;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) drdx[d] = __ldg(eg + d);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) nb[f] = __ldg(A.nbr + (size_t)NF * e + f);
+        sq[el * NP + n] = (T)qd;
+    }
+    cluster_barrier();  // every CTA's first-stage state is in its shared memory
+    int b = 0;
+    for (int32_t step = 0; step < C.nsteps; ++step) {
+        for (int stg = 0; stg < C.nstages; ++stg) {
+            const T* cur = sq + b * EPB * NP;
+            if (active) {
+                const T q0 = (T)qd;
+                const T* qe = cur + el * NP;
+                // ---- volume term
+                T acc = T(0);
+#pragma unroll
+                for (int dir = 0; dir < DIM; ++dir) {
+                    if (!((dmask >> dir) & 1)) continue;
+                    const int stride = dir == 0 ? 1 : (dir == 1 ? NQ : NQ * NQ);
+                    const int idd = id[dir];
+                    const int base = n - idd * stride;
+                    T sum = T(0);
+#pragma unroll
+                    for (int a = 0; a < NQ; ++a) sum += sW[a + NQ * idd] * qe[base + a * stride];
+                    acc += ((T)drdx[dir] * (T)A.adv[dir]) * sum;
+                }
+                // ---- combine with dq
+                const double rka = C.rka[stg];
+                T v = acc;
+                if (rka != 0.0) v = (T)rka * dqv + v;
+                // ---- surface term, faces in the order x-, x+, y-, y+, z-, z+ (dgsem.jl:756-782)
+#pragma unroll
+                for (int dir = 0; dir < DIM; ++dir) {
+                    const int idd = id[dir];
+                    if (idd != 0 && idd != NQ - 1) continue;
+                    if (!((dmask >> dir) & 1)) continue;
+                    const int side = idd == 0 ? 0 : 1;
+                    const int stride = dir == 0 ? 1 : (dir == 1 ? NQ : NQ * NQ);
+                    const int ne = side == 0 ? nb[2 * dir] : nb[2 * dir + 1];  // registers, not a stack array
+                    T qp = q0;  // default boundarystate (balancelaw.jl:77)
+                    if (ne >= 0) {
+                        const int nn = n + (side == 0 ? (NQ - 1) * stride : -(NQ - 1) * stride);
+                        const int64_t rel = ne - A.e_begin;
+                        const T* peer = cluster_peer(cur, (unsigned)(rel / EPB));
+                        qp = peer[(rel % EPB) * NP + nn];
+                    } else if (ne <= -kBcBase && A.bc_kind[-ne - kBcBase] == BC_PRESCRIBED) {
+                        qp = (T)A.bc_state[-ne - kBcBase][0];
+                    }
+                    const T an = (T)A.adv[dir] * (side == 0 ? T(-1) : T(1));
+                    const T fc = (an * q0 + an * qp) * T(0.5);
+                    const T nf = A.surface_rusanov ? fc - (fabs(an) * (qp - q0)) * T(0.5) : fc;
+                    v = v - nf * (T)(fabs(drdx[dir]) / A.w[0]);
+                }
+                dqv = v;
+                qd = qd + C.rkb_dt[stg] * (double)v;
+                sq[(b ^ 1) * EPB * NP + el * NP + n] = (T)qd;
+            }
+            cluster_barrier();  // this stage's reads done and the next stage's state written
+            b ^= 1;
+        }
+    }
+    if (active) {
+        C.q[node0] = qd;
+        if (sizeof(T) == 4) reinterpret_cast<float*>(A.dq)[node0] = (float)dqv;
+        else reinterpret_cast<double*>(A.dq)[node0] = (double)dqv;
+    }
+}
+
+// One cluster of `ctas` CTAs (1..kClusterCtas) runs c.nsteps steps of c.nstages stages.
+template <int DIM, int NQ, typename T>
+cudaError_t launch_cluster_adv(const ClusterStepsArgs& c, int ctas, cudaStream_t st) {
+    using CS = ClusterShape<DIM, NQ>;
+    if (ctas < 1 || ctas > kClusterCtas) return cudaErrorInvalidValue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)ctas, 1, 1);
+    cfg.blockDim = dim3(CS::S::THREADS, 1, 1);
+    cfg.dynamicSmemBytes = CS::smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)ctas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    auto kern = cluster_adv_steps_kernel<DIM, NQ, T>;
+    if (kClusterCtas > 8) {  // sizes above the portable 8 need the kernel's opt-in
+        static std::atomic<bool> opted{false};
+        if (!opted.load(std::memory_order_relaxed)) {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            if (e != cudaSuccess) return e;
+            opted.store(true, std::memory_order_relaxed);
+        }
+    }
+    // whether a cluster of this size fits the device at all, asked once per size;
+    // cudaErrorNotSupported tells the caller to run the steps as stage launches
+    static std::atomic<int> fits[kClusterCtas + 1];  // 0 unknown, 1 yes, 2 no
+    int f = fits[ctas].load(std::memory_order_relaxed);
+    if (f == 0) {
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            n = 0;
+        }
+        f = n > 0 ? 1 : 2;
+        fits[ctas].store(f, std::memory_order_relaxed);
+    }
+    if (f != 1) return cudaErrorNotSupported;
+    cudaError_t err = cudaLaunchKernelEx(&cfg, kern, c);
+    return err != cudaSuccess ? err : cudaGetLastError();
+}
+
 }  // namespace rb200
