@@ -164,6 +164,7 @@ __global__ void __launch_bounds__((DIM == 3 ? 4 : 2) * Pow<NQ, DIM - 1>::v)
     const int t = threadIdx.x;
     const int k = t / NFP, j = t - k * NFP;
     const int j1 = j % NQ, j2 = j / NQ;
+    grid_dependency_wait();  // the stage that wrote A.q, and read A.ncflux, has completed
     for (int64_t m = blockIdx.x; m < A.M; m += gridDim.x) {
         const int64_t* col = A.mortars + (size_t)MCOLS * m;
         const int64_t eC = col[0];
@@ -254,9 +255,8 @@ cudaError_t launch_t(int fp32, const MortarArgs& a, cudaStream_t s) {
     constexpr int threads = (DIM == 3 ? 4 : 2) * Pow<NQ, DIM - 1>::v;
     const int grid = (int)std::min<int64_t>(a.M, 148 * 16);
     if (grid <= 0) return cudaSuccess;
-    if (fp32) mortar_kernel<DIM, NQ, EULER, float><<<grid, threads, 0, s>>>(a);
-    else mortar_kernel<DIM, NQ, EULER, double><<<grid, threads, 0, s>>>(a);
-    return cudaGetLastError();
+    if (fp32) return launch_pdl(mortar_kernel<DIM, NQ, EULER, float>, grid, threads, 0, s, a);
+    return launch_pdl(mortar_kernel<DIM, NQ, EULER, double>, grid, threads, 0, s, a);
 }
 
 template <int DIM, bool EULER>

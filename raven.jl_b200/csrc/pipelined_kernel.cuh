@@ -353,8 +353,11 @@ __global__ void __launch_bounds__(Q * Q * Q / NPT, (pipe_min_ctas<T, Q>()))
         r.e = -1;
         if (cur.start(A, B)) cur.resolve(A, B, r);
         if (t == 0) sm.ref[0] = r;
-        if (r.e >= 0) fetch_part(r, t, sm.geo[0], sm.nb[0]);
+        if (r.e >= 0) fetch_part(r, t, sm.geo[0], sm.nb[0]);  // geometry: written by no kernel
     }
+    // the previous kernel of the stream (the last stage, or this stage's mortar fluxes)
+    // has completed before any state, register or mortar flux is read or written
+    grid_dependency_wait();
     cp_async_commit();
     cp_async_wait_all();
     __syncthreads();

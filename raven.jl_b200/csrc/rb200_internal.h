@@ -84,6 +84,34 @@ struct StageArgs {
     double w[kMaxNq];
 };
 
+// Programmatic dependent launch between the kernels of a step: a kernel launched with it
+// may start while the previous kernel of the stream drains; it touches no global memory
+// that kernel writes or reads before grid_dependency_wait() (griddepcontrol.wait: the
+// previous grid has completed and its writes are visible; a no-op in a kernel launched
+// without it).  RB200_PDL=0 launches the kernels in plain stream order.
+#ifndef RB200_PDL
+#define RB200_PDL 1
+#endif
+#ifdef __CUDACC__
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+#endif
+// Launches kern<<<grid, block, smem, s>>>(args) with programmatic stream serialization.
+template <typename Kern, typename Arg>
+cudaError_t launch_pdl(Kern kern, int grid, int block, size_t smem, cudaStream_t s, const Arg& arg) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid, 1, 1);
+    cfg.blockDim = dim3((unsigned)block, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = RB200_PDL;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, kern, arg);
+    return e != cudaSuccess ? e : cudaGetLastError();
+}
+
 constexpr int kMaxBcTags = 8;
 constexpr int kBcBase = 16;
 enum { BC_DEFAULT = 0, BC_PRESCRIBED = 1, BC_WALL = 2 };
