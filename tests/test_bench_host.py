@@ -44,3 +44,18 @@ def test_reference_arm_times_the_workload_grid(capsys, monkeypatch):
     assert line["timed_steps"] == 3 and line["steps"] == 3
     assert line["cpu_baseline"]["value"] == line["value"]
     assert "16^2-element" in line["cpu_baseline"]["sample"]
+
+
+def test_launch_count_of_the_cluster_step_kernel():
+    """One lsrk54_steps call is one launch on the cluster step kernel, and the stage (and
+    mortar) kernels of every step otherwise (rb200_get_info: info[6] a step, info[9] the
+    cluster's CTAs)."""
+    import types
+
+    cluster = types.SimpleNamespace(cluster_ctas=13, pipelined_ctas=0, info=[2, 5, 1, 256, 0, 0, 5, 32, 0, 13])
+    stages = types.SimpleNamespace(cluster_ctas=0, pipelined_ctas=444, info=[3, 8, 5, 32768, 0, 0, 5, 152, 444, 0])
+    assert bench.timed_launches(cluster, 100) == 1
+    assert bench.timed_launches(stages, 20) == 100
+    w = bench.WORKLOADS["adv2d_weak_n4_16_fp64"]
+    assert bench.kernel_name(w, cluster).startswith("cluster_adv_steps_kernel")
+    assert bench.kernel_name(bench.WORKLOADS["euler3d_kg_n7_32_fp64"], stages).startswith("pipelined_stage_kernel")
