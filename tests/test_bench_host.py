@@ -52,8 +52,8 @@ def test_launch_count_of_the_cluster_step_kernel():
     cluster's CTAs)."""
     import types
 
-    cluster = types.SimpleNamespace(cluster_ctas=13, pipelined_ctas=0, info=[2, 5, 1, 256, 0, 0, 5, 32, 0, 13])
-    stages = types.SimpleNamespace(cluster_ctas=0, pipelined_ctas=444, info=[3, 8, 5, 32768, 0, 0, 5, 152, 444, 0])
+    cluster = types.SimpleNamespace(cluster_ctas=13, pipelined_ctas=0, geometry="affine", info=[2, 5, 1, 256, 0, 0, 5, 32, 0, 13])
+    stages = types.SimpleNamespace(cluster_ctas=0, pipelined_ctas=444, geometry="affine", info=[3, 8, 5, 32768, 0, 0, 5, 152, 444, 0])
     assert bench.timed_launches(cluster, 100) == 1
     assert bench.timed_launches(stages, 20) == 100
     w = bench.WORKLOADS["adv2d_weak_n4_16_fp64"]
