@@ -115,3 +115,25 @@ def test_large_pipelined_and_euler_grids_keep_stage_launches(rb, cuda_ok):
     law, form = product_scheme(rb, "eul_kg", 2)
     dg = rb.DGSEM(law=law, grid=wrap_oracle_grid(og), volume_form=form, surface_numericalflux=rb.RusanovFlux())
     assert dg.cluster_ctas == 0
+
+
+@pytest.mark.parametrize("case", [(2, 8, (1, 1)), (2, 5, (16, 20)), (3, 2, (4, 4, 4)), (1, 2, (1,))],
+                         ids=["one-element", "16-ctas", "3d-nq2", "1d-one-element"])
+def test_cluster_edges(rb, cuda_ok, case):
+    """One periodic element (every face meets the element itself, in its own CTA), a grid
+    that fills all 16 CTAs (320 elements of 25 nodes), Nq = 2."""
+    dim, nq, K = case
+    og, dg = _build(rb, dim, nq, K)
+    assert dg.cluster_ctas > 0
+    if K == (16, 20):
+        assert dg.cluster_ctas == 16
+    q = initial_state(og, oracle_law("adv_weak", dim, ADV[:dim]), "adv_weak", seed=9)
+    dt = 0.1 / (nq * max(K))
+    got = _steps(rb, dg, q, dt, 9, "auto")
+    ref = _steps(rb, dg, q, dt, 9, "generic")
+    assert np.array_equal(got, ref)
+
+
+def test_one_group_too_many_keeps_stage_launches(rb, cuda_ok):
+    _, dg = _build(rb, 2, 5, (17, 20))  # 340 elements: 17 groups of 20
+    assert dg.cluster_ctas == 0
