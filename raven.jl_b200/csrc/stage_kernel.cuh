@@ -942,18 +942,23 @@ cudaError_t launch_cluster_adv(const ClusterStepsArgs& c, int ctas, cudaStream_t
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     auto kern = cluster_adv_steps_kernel<DIM, NQ, T>;
-    if (kClusterCtas > 8) {  // sizes above the portable 8 need the kernel's opt-in
-        static std::atomic<bool> opted{false};
-        if (!opted.load(std::memory_order_relaxed)) {
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-            if (e != cudaSuccess) return e;
-            opted.store(true, std::memory_order_relaxed);
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    if (dev < 0 || dev >= 64) return cudaErrorNotSupported;  // the caches below hold 64 devices
+    if (kClusterCtas > 8) {  // sizes above the portable 8 need the kernel's opt-in, per device
+        static std::atomic<uint64_t> opted{0};
+        const uint64_t bit = uint64_t{1} << dev;
+        if (!(opted.load(std::memory_order_acquire) & bit)) {
+            err = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            if (err != cudaSuccess) return err;
+            opted.fetch_or(bit, std::memory_order_acq_rel);
         }
     }
-    // whether a cluster of this size fits the device at all, asked once per size;
-    // cudaErrorNotSupported tells the caller to run the steps as stage launches
-    static std::atomic<int> fits[kClusterCtas + 1];  // 0 unknown, 1 yes, 2 no
-    int f = fits[ctas].load(std::memory_order_relaxed);
+    // whether a cluster of this size fits the device at all, asked once per device and
+    // size; cudaErrorNotSupported tells the caller to run the steps as stage launches
+    static std::atomic<uint8_t> fits[64][kClusterCtas + 1];  // 0 unknown, 1 yes, 2 no
+    int f = fits[dev][ctas].load(std::memory_order_relaxed);
     if (f == 0) {
         int n = 0;
         if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess) {
@@ -961,10 +966,10 @@ cudaError_t launch_cluster_adv(const ClusterStepsArgs& c, int ctas, cudaStream_t
             n = 0;
         }
         f = n > 0 ? 1 : 2;
-        fits[ctas].store(f, std::memory_order_relaxed);
+        fits[dev][ctas].store((uint8_t)f, std::memory_order_relaxed);
     }
     if (f != 1) return cudaErrorNotSupported;
-    cudaError_t err = cudaLaunchKernelEx(&cfg, kern, c);
+    err = cudaLaunchKernelEx(&cfg, kern, c);
     return err != cudaSuccess ? err : cudaGetLastError();
 }
 
