@@ -15,20 +15,8 @@ static cudaError_t launch_p(const PipeArgs& a, const PipeBatch& b, int grid, cud
     static std::atomic<uint64_t> configured{0};
     cudaError_t err = ensure_smem_limit(kern, (int)sizeof(pipe::Smem<T, Q>), configured);
     if (err != cudaSuccess) return err;
-    if constexpr (!BATCH) {  // serving ticks follow host-written chunk tables: plain order
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)grid, 1, 1);
-        cfg.blockDim = dim3(Q * Q * Q / kNPT, 1, 1);
-        cfg.dynamicSmemBytes = sizeof(pipe::Smem<T, Q>);
-        cfg.stream = s;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        attr[0].val.programmaticStreamSerializationAllowed = RB200_PDL;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        err = cudaLaunchKernelEx(&cfg, kern, a, b);
-        return err != cudaSuccess ? err : cudaGetLastError();
-    }
+    if constexpr (!BATCH)  // serving ticks follow host-written chunk tables: plain order
+        return launch_pdl(kern, grid, Q * Q * Q / kNPT, sizeof(pipe::Smem<T, Q>), s, a, b);
     kern<<<grid, Q * Q * Q / kNPT, sizeof(pipe::Smem<T, Q>), s>>>(a, b);
     return cudaGetLastError();
 }

@@ -95,9 +95,9 @@ struct StageArgs {
 #ifdef __CUDACC__
 __device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 #endif
-// Launches kern<<<grid, block, smem, s>>>(args) with programmatic stream serialization.
-template <typename Kern, typename Arg>
-cudaError_t launch_pdl(Kern kern, int grid, int block, size_t smem, cudaStream_t s, const Arg& arg) {
+// Launches kern<<<grid, block, smem, s>>>(args...) with programmatic stream serialization.
+template <typename Kern, typename... Args>
+cudaError_t launch_pdl(Kern kern, int grid, int block, size_t smem, cudaStream_t s, const Args&... args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)grid, 1, 1);
     cfg.blockDim = dim3((unsigned)block, 1, 1);
@@ -108,7 +108,7 @@ cudaError_t launch_pdl(Kern kern, int grid, int block, size_t smem, cudaStream_t
     attr[0].val.programmaticStreamSerializationAllowed = RB200_PDL;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaError_t e = cudaLaunchKernelEx(&cfg, kern, arg);
+    cudaError_t e = cudaLaunchKernelEx(&cfg, kern, args...);
     return e != cudaSuccess ? e : cudaGetLastError();
 }
 
